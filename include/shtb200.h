@@ -1,0 +1,160 @@
+/*
+ * shtb200.h — C ABI of the B200-native spherical harmonic transform library.
+ *
+ * Every entry point takes plain pointers, sizes and an opaque plan; no C++ or
+ * torch types cross this boundary. Device pointers are CUDA device addresses
+ * on the plan's device; the stream is a cudaStream_t passed as void* (NULL =
+ * legacy default stream). Calls are asynchronous on that stream.
+ *
+ * Layouts are the reference's Julia column-major ones:
+ *   grid         f[i, j, k]   at i + nlat*j + nlat*nlon*k   (latitude north->south fastest)
+ *   coefficients a[l, m, k]   at l + (lmax+1)*m + (lmax+1)*(mmax+1)*k, complex = (re, im) pair
+ * Entries with l < m are ignored on input and written as zero on output.
+ *
+ * Reference interfaces replaced (SHTnsKit.jl v3.0.0, paths within that project):
+ *   shtb_plan_create        per-config device tables built by `_cuda_scalar_tables` /
+ *                           `_cuda_vector_tables` (ext/SHTnsKitGPUExt.jl:495-557) from an
+ *                           `SHTConfig` (src/config.jl:170-206, create_gauss_config :633-655)
+ *   shtb_synthesis          `_gpu_adapter_synthesis(::CUDAAdapter, cfg, alm; real_output=true)`
+ *                           (ext/SHTnsKitGPUExt.jl:788-836); CPU semantics src/core_transforms.jl:271-344
+ *   shtb_analysis           `_gpu_adapter_analysis` (ext/SHTnsKitGPUExt.jl:750-786, :828-831);
+ *                           CPU semantics src/core_transforms.jl:169-207
+ *   shtb_synthesis_sphtor   `_gpu_adapter_synthesis_sphtor` (ext/SHTnsKitGPUExt.jl:927-992);
+ *                           CPU semantics src/sphtor_transforms.jl:162-241
+ *   shtb_analysis_sphtor    `_gpu_adapter_analysis_sphtor` (ext/SHTnsKitGPUExt.jl:859-910, :987-989);
+ *                           CPU semantics src/sphtor_transforms.jl:252-289
+ *   batched calls (nfields > 1) replace `analysis_batch(::GPU, ...)` / `synthesis_batch`
+ *                           (ext/SHTnsKitGPUExt.jl:1845-1975; src/batch_transforms.jl:312-660)
+ *   *_adjoint               the pullbacks of the ChainRules rrules
+ *                           (ext/SHTnsKitAdvancedADExt.jl:55-91, :198-246) which call
+ *                           `_adjoint_synthesis` (src/core_transforms.jl:477-519),
+ *                           `_adjoint_analysis` (:611-652), `_adjoint_synthesis_sphtor` (:537-597),
+ *                           `_adjoint_analysis_sphtor` (src/sphtor_transforms.jl:385-452)
+ *   shtb_gauss_nodes        `gausslegendre` (src/legendre.jl:956-1003) with the north-first
+ *                           reversal of create_gauss_config (src/config.jl:639)
+ */
+#ifndef SHTB200_H
+#define SHTB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (every entry point returns one) ---- */
+#define SHTB_OK               0
+#define SHTB_ERR_BAD_ARG     -1   /* invalid scalar argument (maps to ArgumentError)        */
+#define SHTB_ERR_BAD_SHAPE   -2   /* size/layout mismatch (maps to DimensionMismatch)        */
+#define SHTB_ERR_ALIGN       -3   /* pointer not 16-byte aligned                             */
+#define SHTB_ERR_OOM         -4   /* device allocation for plan tables failed                */
+#define SHTB_ERR_CUDA        -5   /* CUDA runtime error (maps to BackendUnavailableError)    */
+#define SHTB_ERR_TIMEOUT     -6   /* a bounded device wait gave up                           */
+#define SHTB_ERR_UNSUPPORTED -7   /* valid request this build does not implement             */
+#define SHTB_ERR_WORKSPACE   -8   /* workspace pointer NULL or smaller than required         */
+
+/* ---- element types of the caller's buffers ---- */
+#define SHTB_F64 0   /* grids double, coefficients complex double */
+#define SHTB_F32 1   /* grids float,  coefficients complex float  */
+
+/* ---- arithmetic paths ---- */
+#define SHTB_PREC_FP64  0   /* plain FP64 drop-in (relative L2 <= 1e-12 vs the FP64 CPU result) */
+#define SHTB_PREC_MIXED 1   /* Legendre contraction on tensor cores, split BF16x3 products with
+                               FP32 accumulation; nodes, weights, seeds and recurrence in FP64   */
+
+/* ---- operation ids for shtb_workspace_bytes ---- */
+#define SHTB_OP_SYNTHESIS        0
+#define SHTB_OP_ANALYSIS         1
+#define SHTB_OP_SYNTHESIS_SPHTOR 2
+#define SHTB_OP_ANALYSIS_SPHTOR  3
+
+typedef struct shtb_plan shtb_plan;
+
+/* Library version (major*10000 + minor*100 + patch). */
+int shtb_version(void);
+
+/* Message of the last failing call on this host thread ("" if none). */
+const char* shtb_last_error(void);
+
+/* Gauss-Legendre nodes x (descending, north pole first) and weights w, n > 0. Host memory. */
+int shtb_gauss_nodes(int n, double* x, double* w);
+
+/*
+ * Build a plan on the current CUDA device.
+ *   x, w          host arrays of nlat Gauss nodes/weights, north pole first
+ *   coeff_scale   host (lmax+1)*(mmax+1) column-major array s[l,m] with
+ *                 a_canonical = s * a_configured (src/normalization.jl:142-147), or NULL
+ *                 for the canonical orthonormal + Condon-Shortley convention
+ *   phi_inv_scale       synthesis bin scale (nlon under phi_scale=:dft, src/SHTnsKit.jl:141-159)
+ *   analysis_phi_scale  analysis factor (2*pi/nlon under :dft, src/SHTnsKit.jl:177)
+ *   robert_form   nonzero: vector fields carry the sin(theta) factor
+ * Validation mirrors `_validate_spectral_layout` (src/config.jl:465-481).
+ */
+int shtb_plan_create(shtb_plan** plan, int lmax, int mmax, int mres, int nlat, int nlon,
+                     const double* x, const double* w, const double* coeff_scale,
+                     double phi_inv_scale, double analysis_phi_scale, int robert_form);
+int shtb_plan_destroy(shtb_plan* plan);
+
+/* Device bytes held by the plan's tables. */
+size_t shtb_plan_table_bytes(const shtb_plan* plan);
+
+/* Workspace bytes a call needs for nfields fields (caller allocates, >= 256-byte aligned). */
+size_t shtb_workspace_bytes(const shtb_plan* plan, int op, int nfields, int dtype, int precision);
+
+/*
+ * Scalar synthesis, real output: f = Re(ifft(Hermitian-filled bins)) for nfields fields.
+ * ltr truncates degrees (ltr < 0 means lmax).
+ */
+int shtb_synthesis(const shtb_plan* plan, const void* alm, void* f, int nfields, int ltr,
+                   int dtype, int precision, void* work, size_t work_bytes, void* stream);
+
+/* Scalar analysis of real grids. */
+int shtb_analysis(const shtb_plan* plan, const void* f, void* alm, int nfields, int ltr,
+                  int dtype, int precision, void* work, size_t work_bytes, void* stream);
+
+/* Spheroidal/toroidal synthesis to (Vt, Vp), real output. */
+int shtb_synthesis_sphtor(const shtb_plan* plan, const void* S, const void* T, void* Vt, void* Vp,
+                          int nfields, int ltr, int dtype, int precision,
+                          void* work, size_t work_bytes, void* stream);
+
+/* Spheroidal/toroidal analysis of real (Vt, Vp). */
+int shtb_analysis_sphtor(const shtb_plan* plan, const void* Vt, const void* Vp, void* S, void* T,
+                         int nfields, int ltr, int dtype, int precision,
+                         void* work, size_t work_bytes, void* stream);
+
+/*
+ * Adjoints (Zygote convention g = 2 dL/d(conj a)), FP64 only, real spatial cotangents.
+ *   shtb_synthesis_adjoint:        ybar (grid)  -> abar (coefficients)
+ *   shtb_analysis_adjoint:         abar         -> fbar (grid, real projection)
+ *   shtb_synthesis_sphtor_adjoint: (Vtbar, Vpbar) -> (Sbar, Tbar)
+ *   shtb_analysis_sphtor_adjoint:  (Sbar, Tbar)   -> (Vtbar, Vpbar) (real projection)
+ * Workspace: same as the forward operation of the same shape.
+ */
+int shtb_synthesis_adjoint(const shtb_plan* plan, const void* ybar, void* abar, int nfields,
+                           void* work, size_t work_bytes, void* stream);
+int shtb_analysis_adjoint(const shtb_plan* plan, const void* abar, void* fbar, int nfields,
+                          void* work, size_t work_bytes, void* stream);
+int shtb_synthesis_sphtor_adjoint(const shtb_plan* plan, const void* Vtbar, const void* Vpbar,
+                                  void* Sbar, void* Tbar, int nfields,
+                                  void* work, size_t work_bytes, void* stream);
+int shtb_analysis_sphtor_adjoint(const shtb_plan* plan, const void* Sbar, const void* Tbar,
+                                 void* Vtbar, void* Vpbar, int nfields,
+                                 void* work, size_t work_bytes, void* stream);
+
+/* Number of kernels the library launched on this host thread since the last reset. */
+uint64_t shtb_launch_count(int reset);
+
+/*
+ * Per-kernel timing: while enabled, every launch on this host thread is bracketed
+ * by CUDA events on its stream. shtb_profile_read synchronizes the recorded events
+ * and returns the number of distinct kernel names (names: max*64 bytes).
+ * Enabling clears earlier records.
+ */
+int shtb_profile_enable(int on);
+int shtb_profile_read(int max, char* names, double* total_ms, int* count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SHTB200_H */

@@ -1,0 +1,213 @@
+// fft.cuh — shared-memory Stockham FFT along longitude.
+//
+// Each CTA transforms H latitude pairs (north row i, south row nlat-1-i) of one
+// field. A pair is packed into ONE complex sequence z = f_north + i f_south of
+// length nlon, so a complex FFT of nlon points yields both real transforms.
+// The pair packing is also the equatorial fold: the analysis side writes
+// E = w (X_N + X_S) and O = w (X_N - X_S) directly, and the synthesis side reads
+// E/O and forms X_N = E + O, X_S = E - O.
+//
+// Sign conventions follow FFTW/Julia (src/fftutils.jl:280-305): forward
+// F_k = sum_j f_j exp(-2 pi i j k / N), inverse without the 1/N (the caller's
+// per-row factor carries it).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "internal.cuh"
+
+namespace shtb {
+
+template <typename T> struct V2;
+template <> struct V2<double> { using type = double2; };
+template <> struct V2<float> { using type = float2; };
+
+template <typename V> __device__ __forceinline__ V cadd(V a, V b) { a.x += b.x; a.y += b.y; return a; }
+template <typename V> __device__ __forceinline__ V csub(V a, V b) { a.x -= b.x; a.y -= b.y; return a; }
+template <typename V> __device__ __forceinline__ V cmul(V a, V b) {
+  V r;
+  r.x = a.x * b.x - a.y * b.y;
+  r.y = a.x * b.y + a.y * b.x;
+  return r;
+}
+template <typename V, typename T> __device__ __forceinline__ V cscale(V a, T s) { a.x *= s; a.y *= s; return a; }
+// multiply by (dir * i): dir = -1 forward, +1 inverse
+template <typename V> __device__ __forceinline__ V crot(V a, int dir) {
+  V r;
+  if (dir > 0) { r.x = -a.y; r.y = a.x; } else { r.x = a.y; r.y = -a.x; }
+  return r;
+}
+
+// In-register DFT of RADIX points, direction dir (twiddles for generic radices from
+// the table tw[t] = exp(-2 pi i t / N), N/RADIX = twstep).
+template <typename T, typename V, int RADIX>
+__device__ __forceinline__ void dft_small(V* u, int dir, const V* __restrict__ tw, int twstep, int radix_rt) {
+  if constexpr (RADIX == 2) {
+    V a = u[0], b = u[1];
+    u[0] = cadd(a, b);
+    u[1] = csub(a, b);
+  } else if constexpr (RADIX == 3) {
+    const T h = (T)0.86602540378443864676;
+    V t = cadd(u[1], u[2]);
+    V s = cscale(crot(csub(u[1], u[2]), dir), h);
+    V a = u[0];
+    u[0] = cadd(a, t);
+    V b = csub(a, cscale(t, (T)0.5));
+    u[1] = cadd(b, s);
+    u[2] = csub(b, s);
+  } else if constexpr (RADIX == 4) {
+    V t0 = cadd(u[0], u[2]), t1 = csub(u[0], u[2]);
+    V t2 = cadd(u[1], u[3]), t3 = crot(csub(u[1], u[3]), dir);
+    u[0] = cadd(t0, t2);
+    u[2] = csub(t0, t2);
+    u[1] = cadd(t1, t3);
+    u[3] = csub(t1, t3);
+  } else if constexpr (RADIX == 5) {
+    const T c1 = (T)0.30901699437494742410, c2 = (T)-0.80901699437494742410;
+    const T s1 = (T)0.95105651629515357212, s2 = (T)0.58778525229247312917;
+    V a1 = cadd(u[1], u[4]), a2 = cadd(u[2], u[3]);
+    V b1 = csub(u[1], u[4]), b2 = csub(u[2], u[3]);
+    V x0 = u[0];
+    u[0] = cadd(x0, cadd(a1, a2));
+    V p1 = cadd(x0, cadd(cscale(a1, c1), cscale(a2, c2)));
+    V p2 = cadd(x0, cadd(cscale(a1, c2), cscale(a2, c1)));
+    // forward: X1 = p1 - i(s1 b1 + s2 b2), X2 = p2 - i(s2 b1 - s1 b2)
+    V q1 = crot(cadd(cscale(b1, s1), cscale(b2, s2)), dir);
+    V q2 = crot(csub(cscale(b1, s2), cscale(b2, s1)), dir);
+    u[1] = cadd(p1, q1);
+    u[4] = csub(p1, q1);
+    u[2] = cadd(p2, q2);
+    u[3] = csub(p2, q2);
+  } else if constexpr (RADIX == 8) {
+    V e[4] = {u[0], u[2], u[4], u[6]}, o[4] = {u[1], u[3], u[5], u[7]};
+    dft_small<T, V, 4>(e, dir, tw, twstep, 4);
+    dft_small<T, V, 4>(o, dir, tw, twstep, 4);
+    const T r = (T)0.70710678118654752440;
+    // w8^k = exp(dir * 2 pi i k / 8)
+    V w1, w3;
+    w1.x = r; w1.y = dir > 0 ? r : -r;
+    w3.x = -r; w3.y = dir > 0 ? r : -r;
+    V o1 = cmul(o[1], w1), o2 = crot(o[2], dir), o3 = cmul(o[3], w3);
+    u[0] = cadd(e[0], o[0]); u[4] = csub(e[0], o[0]);
+    u[1] = cadd(e[1], o1);   u[5] = csub(e[1], o1);
+    u[2] = cadd(e[2], o2);   u[6] = csub(e[2], o2);
+    u[3] = cadd(e[3], o3);   u[7] = csub(e[3], o3);
+  } else {
+    // generic odd radix <= RADIX (runtime radix_rt), O(r^2) with table twiddles
+    V out[RADIX];
+#pragma unroll
+    for (int a = 0; a < RADIX; ++a) {
+      V acc;
+      acc.x = 0; acc.y = 0;
+      if (a < radix_rt) {
+#pragma unroll
+        for (int q = 0; q < RADIX; ++q) {
+          if (q < radix_rt) {
+            V wv = tw[((a * q) % radix_rt) * twstep];
+            if (dir > 0) wv.y = -wv.y;
+            acc = cadd(acc, cmul(u[q], wv));
+          }
+        }
+      }
+      out[a] = acc;
+    }
+#pragma unroll
+    for (int a = 0; a < RADIX; ++a) u[a] = out[a];
+  }
+}
+
+// One Stockham pass of radix RADIX over F sequences of length N stored with row
+// stride S in shared memory. p = product of the radices already applied.
+// Register staging: all threads load their butterflies, barrier, compute, store.
+template <typename T, typename V, int RADIX, int EMAX>
+__device__ __forceinline__ void fft_pass(V* X, int F, int N, int S, int p, int radix_rt, const V* __restrict__ tw, int dir) {
+  // butterflies per thread: the launcher guarantees F*N <= EMAX*blockDim, and the
+  // generic template serves every odd radix from 7 up to RADIX
+  constexpr int RMIN = (RADIX >= 7) ? 7 : RADIX;
+  constexpr int NB = (EMAX + RMIN - 1) / RMIN;
+  const int r = (RADIX >= 7) ? radix_rt : RADIX;
+  const int stride = N / r;
+  const int nbt = F * stride;
+  V u[NB][RADIX];
+#pragma unroll
+  for (int e = 0; e < NB; ++e) {
+    const int b = threadIdx.x + e * blockDim.x;
+    if (b < nbt) {
+      const int f = b / stride, i = b - f * stride;
+#pragma unroll
+      for (int q = 0; q < RADIX; ++q)
+        if (q < r) u[e][q] = X[f * S + i + q * stride];
+    }
+  }
+  __syncthreads();
+  const int tws = N / (p * r);
+#pragma unroll
+  for (int e = 0; e < NB; ++e) {
+    const int b = threadIdx.x + e * blockDim.x;
+    if (b < nbt) {
+      const int f = b / stride, i = b - f * stride;
+      const int k = i % p;
+      if (k != 0) {
+#pragma unroll
+        for (int q = 1; q < RADIX; ++q) {
+          if (q < r) {
+            V wv = tw[q * k * tws];
+            if (dir > 0) wv.y = -wv.y;
+            u[e][q] = cmul(u[e][q], wv);
+          }
+        }
+      }
+      dft_small<T, V, RADIX>(u[e], dir, tw, N / r, r);
+      const int j = (i / p) * p * r + k;
+#pragma unroll
+      for (int q = 0; q < RADIX; ++q)
+        if (q < r) X[f * S + j + q * p] = u[e][q];
+    }
+  }
+  __syncthreads();
+}
+
+// Full FFT of F rows in X (stride S) in direction dir. `scratch` is a second
+// buffer of the same size, used only when nlon has a prime factor above 13.
+template <typename T, typename V, int EMAX>
+__device__ void fft_rows(V* X, V* scratch, int F, int S, const FFTDesc& fd, const V* __restrict__ tw, int dir) {
+  const int N = fd.n;
+  if (fd.direct) {
+    for (int idx = threadIdx.x; idx < F * N; idx += blockDim.x) {
+      const int f = idx / N, k = idx - f * N;
+      V acc;
+      acc.x = 0; acc.y = 0;
+      long long t = 0;
+      for (int n = 0; n < N; ++n) {
+        V wv = tw[t];
+        if (dir > 0) wv.y = -wv.y;
+        acc = cadd(acc, cmul(X[f * S + n], wv));
+        t += k;
+        if (t >= N) t -= N;
+      }
+      scratch[f * S + k] = acc;
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < F * N; idx += blockDim.x) {
+      const int f = idx / N, k = idx - f * N;
+      X[f * S + k] = scratch[f * S + k];
+    }
+    __syncthreads();
+    return;
+  }
+  int p = 1;
+  for (int s = 0; s < fd.nrad; ++s) {
+    const int r = fd.rad[s];
+    switch (r) {
+      case 2: fft_pass<T, V, 2, EMAX>(X, F, N, S, p, 2, tw, dir); break;
+      case 3: fft_pass<T, V, 3, EMAX>(X, F, N, S, p, 3, tw, dir); break;
+      case 4: fft_pass<T, V, 4, EMAX>(X, F, N, S, p, 4, tw, dir); break;
+      case 5: fft_pass<T, V, 5, EMAX>(X, F, N, S, p, 5, tw, dir); break;
+      case 8: fft_pass<T, V, 8, EMAX>(X, F, N, S, p, 8, tw, dir); break;
+      default: fft_pass<T, V, 13, EMAX>(X, F, N, S, p, r, tw, dir); break;
+    }
+    p *= r;
+  }
+}
+
+}  // namespace shtb

@@ -1,0 +1,89 @@
+// internal.cuh — plan layout, error plumbing and small device helpers shared by
+// the translation units of libshtb200.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/shtb200.h"
+
+namespace shtb {
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+int set_error(int code, const std::string& msg);   // records msg, returns code
+int check_cuda(cudaError_t e, const char* what);    // SHTB_OK or SHTB_ERR_CUDA
+void count_launch(int n = 1);
+// Per-kernel CUDA-event timing on the launching stream (off unless enabled by
+// shtb_profile_enable); prof_begin/prof_end bracket one launch.
+void prof_begin(cudaStream_t st);
+void prof_end(const char* name, cudaStream_t st);
+
+#define SHTB_TRY_CUDA(expr, what)                                   \
+  do {                                                              \
+    int _rc = ::shtb::check_cuda((expr), (what));                   \
+    if (_rc != SHTB_OK) return _rc;                                 \
+  } while (0)
+
+#define SHTB_LAUNCHED(what)                                         \
+  do {                                                              \
+    ::shtb::prof_end((what), st);                                   \
+    ::shtb::count_launch();                                         \
+    int _rc = ::shtb::check_cuda(cudaGetLastError(), (what));       \
+    if (_rc != SHTB_OK) return _rc;                                 \
+  } while (0)
+
+// Rows of one analysis tile (degree range sharing one recurrence checkpoint).
+constexpr int kTileRows = 64;
+
+// ---------------------------------------------------------------------------
+// device view of a plan (passed by value to kernels)
+// ---------------------------------------------------------------------------
+struct PlanDev {
+  int lmax, mmax, mres, nlat, nlon, nm, npair, lrec;  // lrec = lmax + 1
+  const double* x;         // [nlat] north first
+  const double* w;         // [nlat]
+  const double* sint;      // [nlat]
+  const long long* off;    // [nm+1] packed (im, l) offsets, l in [m, lrec]
+  const double* alpha;     // packed: r_l = alpha_l x r_{l-1} - r_{l-2}
+  const double* cfac;      // packed: P_l = c_l r_l
+  const int* l0;           // [nm*npair] first significant degree per (im, pair)
+  const double2* r01;      // [nm*npair] (r_{l0}, r_{l0+1})
+  const double2* ckpt;     // [ntiles*npair] state (r_{t0-1}, r_{t0-2}) before tile row t0
+  const int2* tiles;       // [ntiles] (im, t0)
+  int ntiles;
+};
+
+// FFT description for nlon
+struct FFTDesc {
+  int n;
+  int nrad;
+  int rad[24];
+  bool direct;             // a prime factor above the largest register radix: O(N^2) DFT
+};
+
+}  // namespace shtb
+
+struct shtb_plan {
+  int lmax, mmax, mres, nlat, nlon, nm, npair, lrec;
+  int robert;
+  int device;
+  double phi_inv_scale, ana_scale;
+  bool canonical;
+  std::vector<double> hx, hw, hsint;
+  std::vector<double> hscale;             // (lmax+1)*(mmax+1), empty if canonical
+  std::vector<long long> hoff;            // [nm+1]
+  shtb::FFTDesc fft;
+  // device memory
+  void* dmem = nullptr;                   // one allocation for every small table
+  size_t dbytes = 0;
+  shtb::PlanDev dev{};
+  const double* d_scale = nullptr;        // s_lm table (device) or null
+  const double2* d_tw64 = nullptr;        // exp(-2 pi i t / nlon)
+  const float2* d_tw32 = nullptr;
+  const double* d_dcoef = nullptr;        // packed d(l,m) = sqrt((l^2-m^2)/(4l^2-1)), l in [m, lrec]
+  std::vector<int2> htiles;
+};

@@ -1,0 +1,52 @@
+// kernels.cuh — launchers shared between translation units.
+#pragma once
+
+#include <algorithm>
+#include <type_traits>
+
+#include "internal.cuh"
+
+namespace shtb {
+
+// Coefficient-side operands of the Legendre stage. Element (l, im, k) lives at
+//   ptr[k * ld_k + base(im) + l],  base(im) = packed ? off[im] - m : m * ld_m.
+struct CoefSrc {
+  const double2* ptr;
+  long long ld_k, ld_m;
+  int packed;
+};
+struct CoefSink {
+  double2* ptr;
+  long long ld_k, ld_m;
+  int packed;
+};
+
+// Per-(l, m) multipliers applied where coefficients enter (synthesis) or leave
+// (analysis) the Legendre stage: fac (packed, e.g. c_l) * sc[l,m]^(+1|-1) * mf(m).
+struct Factors {
+  const double* fac;   // packed over (im, l), or null
+  const double* sc;    // dense (lmax+1)x(mmax+1) normalization scale, or null
+  int sc_mode;         // 0 none, 1 multiply, 2 divide
+  double mf0, mf1;     // factor for m == 0 and for m > 0
+};
+
+template <typename T, typename GT>
+int launch_fft_syn(const shtb_plan* p, const void* W, GT* out0, GT* out1, int ncomp, int nfw, int mlim,
+                   double gscale, int use_w, int spow, cudaStream_t st);
+template <typename T, typename GT>
+int launch_fft_ana(const shtb_plan* p, const GT* in0, const GT* in1, int ncomp, void* W, int nfw, int mlim,
+                   double wscale, int use_w, int spow, cudaStream_t st);
+
+int launch_leg_syn64(const shtb_plan* p, const CoefSrc& src, const Factors& F, void* W, int nf, int row_end,
+                     int mlim, cudaStream_t st);
+int launch_leg_ana64(const shtb_plan* p, const void* W, int nf, int row_end, int mlim, const CoefSink& dst,
+                     const Factors& F, int zero_fill, cudaStream_t st);
+
+// Vector coefficient transforms around the scalar Legendre stage.
+int launch_sphtor_pre64(const shtb_plan* p, const double2* S, const double2* T, double2* U, int nf, int ltr,
+                        const Factors& F, int div_ll, cudaStream_t st);
+int launch_sphtor_post64(const shtb_plan* p, const double2* V, double2* S, double2* T, int nf, int ltr,
+                         const Factors& F, int div_ll, cudaStream_t st);
+int launch_zero_columns64(const shtb_plan* p, double2* a, int nf, int mlim, cudaStream_t st);
+
+}  // namespace shtb
