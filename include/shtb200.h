@@ -99,6 +99,12 @@ int shtb_plan_destroy(shtb_plan* plan);
 /* Device bytes held by the plan's tables. */
 size_t shtb_plan_table_bytes(const shtb_plan* plan);
 
+/*
+ * Synchronizes the device; returns SHTB_ERR_TIMEOUT if a kernel of this plan gave
+ * up a bounded device wait since the last call (and clears the condition), else SHTB_OK.
+ */
+int shtb_plan_status(const shtb_plan* plan);
+
 /* Workspace bytes a call needs for nfields fields (caller allocates, >= 256-byte aligned). */
 size_t shtb_workspace_bytes(const shtb_plan* plan, int op, int nfields, int dtype, int precision);
 

@@ -18,14 +18,15 @@ __device__ __forceinline__ T pair_factor(const PlanDev& P, int pair, double scal
   return (T)g;
 }
 
-template <typename T, typename GT, int EMAX>
-__global__ void __launch_bounds__(1024) fft_syn_kernel(PlanDev P, FFTDesc fd, const typename V2<T>::type* __restrict__ W,
+template <typename T, typename GT, bool GENERIC>
+__global__ void __launch_bounds__(256) fft_syn_kernel(PlanDev P, FFTDesc fd, const int* __restrict__ rev,
+                                                      const typename V2<T>::type* __restrict__ W,
                                                        GT* __restrict__ out0, GT* __restrict__ out1, int ncomp,
                                                        int mlim, int H, double gscale, int use_w, int spow,
                                                        const typename V2<T>::type* __restrict__ tw) {
   using V = typename V2<T>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int N = fd.n, S = N + 1;
+  const int N = fd.n, S = fft_row_stride(N);
   V* Z = reinterpret_cast<V*>(smem_raw);
   V* scratch = Z + H * S;
   T* gfac = reinterpret_cast<T*>(Z + (fd.direct ? 2 : 1) * H * S);
@@ -41,34 +42,53 @@ __global__ void __launch_bounds__(1024) fft_syn_kernel(PlanDev P, FFTDesc fd, co
     gfac[h] = (p0 + h < npair) ? pair_factor<T>(P, p0 + h, gscale, use_w, spow) : (T)0;
   __syncthreads();
   const int nmu = mlim / P.mres + 1;
-  for (int idx = threadIdx.x; idx < nmu * H; idx += blockDim.x) {
-    const int im = idx / H, h = idx - im * H, pair = p0 + h;
-    if (pair >= npair) continue;
-    const int m = im * P.mres;
-    const size_t base = ((size_t)k * P.nm + im) * 2 * npair + pair;
-    const V E = W[base], O = W[base + npair];
-    V XN = cadd(E, O), XS = csub(E, O);
-    if (m == 0) {
-      V z;
-      z.x = XN.x; z.y = XS.x;
-      Z[h * S] = z;
-    } else {
-      V a, b;
-      a.x = XN.x - XS.y; a.y = XN.y + XS.x;
-      b.x = XN.x + XS.y; b.y = XS.x - XN.y;
-      Z[h * S + m] = a;
-      Z[h * S + N - m] = b;
+  // batched loads (U items in flight per thread) for memory-level parallelism
+  constexpr int U = 4;
+  for (int base0 = threadIdx.x; base0 < nmu * H; base0 += blockDim.x * U) {
+    V Ev[U], Ov[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int idx = base0 + u * blockDim.x;
+      Ev[u].x = Ev[u].y = Ov[u].x = Ov[u].y = 0;
+      if (idx < nmu * H) {
+        const int im = idx / H, h = idx - im * H, pair = p0 + h;
+        if (pair < npair) {
+          const size_t base = ((size_t)k * P.nm + im) * 2 * npair + pair;
+          Ev[u] = W[base];
+          Ov[u] = W[base + npair];
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int idx = base0 + u * blockDim.x;
+      if (idx >= nmu * H) continue;
+      const int im = idx / H, h = idx - im * H, pair = p0 + h;
+      if (pair >= npair) continue;
+      const int m = im * P.mres;
+      const V XN = cadd(Ev[u], Ov[u]), XS = csub(Ev[u], Ov[u]);
+      if (m == 0) {
+        V z;
+        z.x = XN.x; z.y = XS.x;
+        Z[h * S] = z;
+      } else {
+        V a, b;
+        a.x = XN.x - XS.y; a.y = XN.y + XS.x;
+        b.x = XN.x + XS.y; b.y = XS.x - XN.y;
+        Z[h * S + fft_pad(m)] = a;
+        Z[h * S + fft_pad(N - m)] = b;
+      }
     }
   }
   __syncthreads();
-  fft_rows<T, V, EMAX>(Z, scratch, H, S, fd, tw, +1);
+  fft_rows<T, V, GENERIC>(Z, scratch, H, S, fd, tw, +1);
   GT* out = (ncomp == 2 && (k & 1)) ? out1 : out0;
   const size_t kk = (ncomp == 2) ? (size_t)(k >> 1) : (size_t)k;
   const size_t fbase = kk * (size_t)nlat * N;
   for (int idx = threadIdx.x; idx < N * H; idx += blockDim.x) {
     const int j = idx / H, h = idx - j * H, pair = p0 + h;
     if (pair >= npair) continue;
-    const V z = Z[h * S + j];
+    const V z = Z[h * S + fft_pad(rev[j])];
     const T g = gfac[h];
     out[fbase + (size_t)j * nlat + pair] = (GT)(z.x * g);
     const int south = nlat - 1 - pair;
@@ -76,15 +96,16 @@ __global__ void __launch_bounds__(1024) fft_syn_kernel(PlanDev P, FFTDesc fd, co
   }
 }
 
-template <typename T, typename GT, int EMAX>
-__global__ void __launch_bounds__(1024) fft_ana_kernel(PlanDev P, FFTDesc fd, const GT* __restrict__ in0,
+template <typename T, typename GT, bool GENERIC>
+__global__ void __launch_bounds__(256) fft_ana_kernel(PlanDev P, FFTDesc fd, const int* __restrict__ rev,
+                                                      const GT* __restrict__ in0,
                                                        const GT* __restrict__ in1, int ncomp,
                                                        typename V2<T>::type* __restrict__ W, int mlim, int H,
                                                        double wscale, int use_w, int spow,
                                                        const typename V2<T>::type* __restrict__ tw) {
   using V = typename V2<T>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int N = fd.n, S = N + 1;
+  const int N = fd.n, S = fft_row_stride(N);
   V* Z = reinterpret_cast<V*>(smem_raw);
   V* scratch = Z + H * S;
   T* wfac = reinterpret_cast<T*>(Z + (fd.direct ? 2 : 1) * H * S);
@@ -96,26 +117,43 @@ __global__ void __launch_bounds__(1024) fft_ana_kernel(PlanDev P, FFTDesc fd, co
   const size_t fbase = kk * (size_t)nlat * N;
   for (int h = threadIdx.x; h < H; h += blockDim.x)
     wfac[h] = (p0 + h < npair) ? pair_factor<T>(P, p0 + h, wscale, use_w, spow) : (T)0;
-  for (int idx = threadIdx.x; idx < N * H; idx += blockDim.x) {
-    const int j = idx / H, h = idx - j * H, pair = p0 + h;
-    V z;
-    z.x = 0; z.y = 0;
-    if (pair < npair) {
-      z.x = (T)in[fbase + (size_t)j * nlat + pair];
-      const int south = nlat - 1 - pair;
-      if (south != pair) z.y = (T)in[fbase + (size_t)j * nlat + south];
+  constexpr int U = 8;
+  for (int base0 = threadIdx.x; base0 < N * H; base0 += blockDim.x * U) {
+    T vn[U], vs[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int idx = base0 + u * blockDim.x;
+      vn[u] = vs[u] = (T)0;
+      if (idx < N * H) {
+        const int j = idx / H, h = idx - j * H, pair = p0 + h;
+        if (pair < npair) {
+          vn[u] = (T)in[fbase + (size_t)j * nlat + pair];
+          const int south = nlat - 1 - pair;
+          if (south != pair) vs[u] = (T)in[fbase + (size_t)j * nlat + south];
+        }
+      }
     }
-    Z[h * S + j] = z;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int idx = base0 + u * blockDim.x;
+      if (idx < N * H) {
+        const int j = idx / H, h = idx - j * H;
+        V z;
+        z.x = vn[u];
+        z.y = vs[u];
+        Z[h * S + fft_pad(j)] = z;
+      }
+    }
   }
   __syncthreads();
-  fft_rows<T, V, EMAX>(Z, scratch, H, S, fd, tw, -1);
+  fft_rows<T, V, GENERIC>(Z, scratch, H, S, fd, tw, -1);
   const int nmu = mlim / P.mres + 1;
   for (int idx = threadIdx.x; idx < nmu * H; idx += blockDim.x) {
     const int im = idx / H, h = idx - im * H, pair = p0 + h;
     if (pair >= npair) continue;
     const int m = im * P.mres;
-    const V Zm = Z[h * S + m];
-    V Zc = Z[h * S + (m == 0 ? 0 : N - m)];
+    const V Zm = Z[h * S + fft_pad(rev[m])];
+    V Zc = Z[h * S + fft_pad(rev[m == 0 ? 0 : N - m])];
     Zc.y = -Zc.y;
     const V sum = cadd(Zm, Zc), d = csub(Zm, Zc);
     V XN, XS;
@@ -130,17 +168,15 @@ __global__ void __launch_bounds__(1024) fft_ana_kernel(PlanDev P, FFTDesc fd, co
 
 static int fft_config(const FFTDesc& fd, size_t celem, int npair, int* H, int* threads, size_t* smem) {
   const int N = fd.n;
-  constexpr int EMAX = 16;
-  int h = std::max(1, std::min(16, 4096 / N));
-  h = std::min(h, npair);
-  const int S = N + 1;
+  const int S = fft_row_stride(N);
+  // enough latitude pairs for 32-byte (FP64) / 32-byte (FP32) row segments, up to 16
+  int h = std::min(16, std::max(celem == 16 ? 2 : 4, 4096 / std::max(N, 1)));
+  h = std::max(1, std::min(h, npair));
   auto need = [&](int hh) { return (size_t)hh * S * celem * (fd.direct ? 2 : 1) + (size_t)hh * 8 + 16; };
-  while (h > 1 && need(h) > 96 * 1024) --h;
-  int t = (int)std::min<long long>(1024, std::max<long long>(256, ((long long)h * N + EMAX - 1) / EMAX));
-  t = (t + 31) / 32 * 32;
-  if ((long long)h * N > (long long)EMAX * t) return set_error(SHTB_ERR_UNSUPPORTED, "nlon too large for the FFT kernel");
+  while (h > 1 && need(h) > 100 * 1024) --h;
+  if (need(h) > 220 * 1024) return set_error(SHTB_ERR_UNSUPPORTED, "nlon too large for the shared-memory FFT");
   *H = h;
-  *threads = t;
+  *threads = 256;
   *smem = need(h);
   return SHTB_OK;
 }
@@ -153,12 +189,17 @@ int launch_fft_syn(const shtb_plan* p, const void* W, GT* out0, GT* out1, int nc
   size_t smem;
   int rc = fft_config(p->fft, sizeof(V), p->npair, &H, &threads, &smem);
   if (rc) return rc;
-  auto kern = fft_syn_kernel<T, GT, 16>;
+  bool generic = p->fft.direct;
+  for (int i = 0; i < p->fft.nrad; ++i) {
+    const int r = p->fft.rad[i];
+    generic = generic || !(r == 2 || r == 3 || r == 4 || r == 5 || r == 8);
+  }
+  auto kern = generic ? fft_syn_kernel<T, GT, true> : fft_syn_kernel<T, GT, false>;
   SHTB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "fft smem attr");
   dim3 grid((p->npair + H - 1) / H, nfw);
   const V* tw = std::is_same<T, double>::value ? (const V*)p->d_tw64 : (const V*)p->d_tw32;
   prof_begin(st);
-  kern<<<grid, threads, smem, st>>>(p->dev, p->fft, (const V*)W, out0, out1, ncomp, mlim, H, gscale, use_w, spow, tw);
+  kern<<<grid, threads, smem, st>>>(p->dev, p->fft, p->d_rev, (const V*)W, out0, out1, ncomp, mlim, H, gscale, use_w, spow, tw);
   SHTB_LAUNCHED("fft synthesis kernel");
   return SHTB_OK;
 }
@@ -171,12 +212,17 @@ int launch_fft_ana(const shtb_plan* p, const GT* in0, const GT* in1, int ncomp, 
   size_t smem;
   int rc = fft_config(p->fft, sizeof(V), p->npair, &H, &threads, &smem);
   if (rc) return rc;
-  auto kern = fft_ana_kernel<T, GT, 16>;
+  bool generic = p->fft.direct;
+  for (int i = 0; i < p->fft.nrad; ++i) {
+    const int r = p->fft.rad[i];
+    generic = generic || !(r == 2 || r == 3 || r == 4 || r == 5 || r == 8);
+  }
+  auto kern = generic ? fft_ana_kernel<T, GT, true> : fft_ana_kernel<T, GT, false>;
   SHTB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "fft smem attr");
   dim3 grid((p->npair + H - 1) / H, nfw);
   const V* tw = std::is_same<T, double>::value ? (const V*)p->d_tw64 : (const V*)p->d_tw32;
   prof_begin(st);
-  kern<<<grid, threads, smem, st>>>(p->dev, p->fft, in0, in1, ncomp, (V*)W, mlim, H, wscale, use_w, spow, tw);
+  kern<<<grid, threads, smem, st>>>(p->dev, p->fft, p->d_rev, in0, in1, ncomp, (V*)W, mlim, H, wscale, use_w, spow, tw);
   SHTB_LAUNCHED("fft analysis kernel");
   return SHTB_OK;
 }

@@ -1,4 +1,4 @@
-// fft.cuh — shared-memory Stockham FFT along longitude.
+// fft.cuh — shared-memory mixed-radix FFT along longitude.
 //
 // Each CTA transforms H latitude pairs (north row i, south row nlat-1-i) of one
 // field. A pair is packed into ONE complex sequence z = f_north + i f_south of
@@ -6,6 +6,14 @@
 // The pair packing is also the equatorial fold: the analysis side writes
 // E = w (X_N + X_S) and O = w (X_N - X_S) directly, and the synthesis side reads
 // E/O and forms X_N = E + O, X_S = E - O.
+//
+// The transform is an in-place decimation-in-frequency mixed-radix FFT
+// (radices 8, 4, 2, 3, 5 and generic odd radices up to 13): every pass updates
+// disjoint groups of r elements where they lie, so one shared buffer and one
+// barrier per pass suffice for any thread count. The result comes out in
+// mixed-radix digit-reversed order; callers read bin k at position rev[k]
+// (a plan table). Indices are skewed by pad(n) = n + n/8 to spread the strided
+// accesses of the late passes over the shared-memory banks.
 //
 // Sign conventions follow FFTW/Julia (src/fftutils.jl:280-305): forward
 // F_k = sum_j f_j exp(-2 pi i j k / N), inverse without the 1/N (the caller's
@@ -38,8 +46,11 @@ template <typename V> __device__ __forceinline__ V crot(V a, int dir) {
   return r;
 }
 
-// In-register DFT of RADIX points, direction dir (twiddles for generic radices from
-// the table tw[t] = exp(-2 pi i t / N), N/RADIX = twstep).
+__device__ __forceinline__ int fft_pad(int n) { return n + (n >> 3); }
+__host__ __device__ inline int fft_row_stride(int n) { return n + (n >> 3) + 1; }
+
+// In-register DFT of RADIX points in direction dir. Generic odd radices use the
+// twiddle table tw[t] = exp(-2 pi i t / N) with step twstep = N / radix.
 template <typename T, typename V, int RADIX>
 __device__ __forceinline__ void dft_small(V* u, int dir, const V* __restrict__ tw, int twstep, int radix_rt) {
   if constexpr (RADIX == 2) {
@@ -93,7 +104,6 @@ __device__ __forceinline__ void dft_small(V* u, int dir, const V* __restrict__ t
     u[2] = cadd(e[2], o2);   u[6] = csub(e[2], o2);
     u[3] = cadd(e[3], o3);   u[7] = csub(e[3], o3);
   } else {
-    // generic odd radix <= RADIX (runtime radix_rt), O(r^2) with table twiddles
     V out[RADIX];
 #pragma unroll
     for (int a = 0; a < RADIX; ++a) {
@@ -116,97 +126,86 @@ __device__ __forceinline__ void dft_small(V* u, int dir, const V* __restrict__ t
   }
 }
 
-// One Stockham pass of radix RADIX over F sequences of length N stored with row
-// stride S in shared memory. p = product of the radices already applied.
-// Register staging: all threads load their butterflies, barrier, compute, store.
-template <typename T, typename V, int RADIX, int EMAX>
-__device__ __forceinline__ void fft_pass(V* X, int F, int N, int S, int p, int radix_rt, const V* __restrict__ tw, int dir) {
-  // butterflies per thread: the launcher guarantees F*N <= EMAX*blockDim, and the
-  // generic template serves every odd radix from 7 up to RADIX
-  constexpr int RMIN = (RADIX >= 7) ? 7 : RADIX;
-  constexpr int NB = (EMAX + RMIN - 1) / RMIN;
+// One DIF pass of radix r on sub-transforms of length Ns (all F rows, stride S):
+// for j < Ns/r, element group {base + j + q*Ns/r}: DFT_r, then twiddle
+// W_Ns^(j*q) on output q.
+template <typename T, typename V, int RADIX>
+__device__ __forceinline__ void dif_pass(V* X, int F, int N, int S, int Ns, int radix_rt, const V* __restrict__ tw,
+                                         int dir) {
   const int r = (RADIX >= 7) ? radix_rt : RADIX;
-  const int stride = N / r;
-  const int nbt = F * stride;
-  V u[NB][RADIX];
+  const int span = Ns / r;            // distance between group members
+  const int per_row = N / r;          // groups per row
+  const int twmul = N / Ns;           // table step for W_Ns
+  for (int b = threadIdx.x; b < F * per_row; b += blockDim.x) {
+    const int f = b / per_row, t = b - f * per_row;
+    const int blk = t / span, j = t - blk * span;
+    const int base = blk * Ns + j;
+    V* row = X + (size_t)f * S;
+    V u[RADIX];
 #pragma unroll
-  for (int e = 0; e < NB; ++e) {
-    const int b = threadIdx.x + e * blockDim.x;
-    if (b < nbt) {
-      const int f = b / stride, i = b - f * stride;
+    for (int q = 0; q < RADIX; ++q)
+      if (q < r) u[q] = row[fft_pad(base + q * span)];
+    dft_small<T, V, RADIX>(u, dir, tw, N / r, r);
+    if (j != 0) {
 #pragma unroll
-      for (int q = 0; q < RADIX; ++q)
-        if (q < r) u[e][q] = X[f * S + i + q * stride];
-    }
-  }
-  __syncthreads();
-  const int tws = N / (p * r);
-#pragma unroll
-  for (int e = 0; e < NB; ++e) {
-    const int b = threadIdx.x + e * blockDim.x;
-    if (b < nbt) {
-      const int f = b / stride, i = b - f * stride;
-      const int k = i % p;
-      if (k != 0) {
-#pragma unroll
-        for (int q = 1; q < RADIX; ++q) {
-          if (q < r) {
-            V wv = tw[q * k * tws];
-            if (dir > 0) wv.y = -wv.y;
-            u[e][q] = cmul(u[e][q], wv);
-          }
+      for (int q = 1; q < RADIX; ++q) {
+        if (q < r) {
+          V wv = tw[j * q * twmul];
+          if (dir > 0) wv.y = -wv.y;
+          u[q] = cmul(u[q], wv);
         }
       }
-      dft_small<T, V, RADIX>(u[e], dir, tw, N / r, r);
-      const int j = (i / p) * p * r + k;
-#pragma unroll
-      for (int q = 0; q < RADIX; ++q)
-        if (q < r) X[f * S + j + q * p] = u[e][q];
     }
+#pragma unroll
+    for (int q = 0; q < RADIX; ++q)
+      if (q < r) row[fft_pad(base + q * span)] = u[q];
   }
   __syncthreads();
 }
 
-// Full FFT of F rows in X (stride S) in direction dir. `scratch` is a second
-// buffer of the same size, used only when nlon has a prime factor above 13.
-template <typename T, typename V, int EMAX>
+// Full in-place FFT of F rows (natural-order input; output bin k at rev[k]).
+// `scratch` (same size as X) is used only in direct mode (a prime factor above 13).
+template <typename T, typename V, bool GENERIC>
 __device__ void fft_rows(V* X, V* scratch, int F, int S, const FFTDesc& fd, const V* __restrict__ tw, int dir) {
   const int N = fd.n;
-  if (fd.direct) {
+  if (GENERIC && fd.direct) {
+    // O(N^2) DFT into scratch, written at natural positions (rev = identity in direct mode)
     for (int idx = threadIdx.x; idx < F * N; idx += blockDim.x) {
       const int f = idx / N, k = idx - f * N;
       V acc;
       acc.x = 0; acc.y = 0;
-      long long t = 0;
+      int t = 0;
       for (int n = 0; n < N; ++n) {
         V wv = tw[t];
         if (dir > 0) wv.y = -wv.y;
-        acc = cadd(acc, cmul(X[f * S + n], wv));
+        acc = cadd(acc, cmul(X[(size_t)f * S + fft_pad(n)], wv));
         t += k;
         if (t >= N) t -= N;
       }
-      scratch[f * S + k] = acc;
+      scratch[(size_t)f * S + fft_pad(k)] = acc;
     }
     __syncthreads();
     for (int idx = threadIdx.x; idx < F * N; idx += blockDim.x) {
       const int f = idx / N, k = idx - f * N;
-      X[f * S + k] = scratch[f * S + k];
+      X[(size_t)f * S + fft_pad(k)] = scratch[(size_t)f * S + fft_pad(k)];
     }
     __syncthreads();
     return;
   }
-  int p = 1;
+  int Ns = N;
   for (int s = 0; s < fd.nrad; ++s) {
     const int r = fd.rad[s];
     switch (r) {
-      case 2: fft_pass<T, V, 2, EMAX>(X, F, N, S, p, 2, tw, dir); break;
-      case 3: fft_pass<T, V, 3, EMAX>(X, F, N, S, p, 3, tw, dir); break;
-      case 4: fft_pass<T, V, 4, EMAX>(X, F, N, S, p, 4, tw, dir); break;
-      case 5: fft_pass<T, V, 5, EMAX>(X, F, N, S, p, 5, tw, dir); break;
-      case 8: fft_pass<T, V, 8, EMAX>(X, F, N, S, p, 8, tw, dir); break;
-      default: fft_pass<T, V, 13, EMAX>(X, F, N, S, p, r, tw, dir); break;
+      case 2: dif_pass<T, V, 2>(X, F, N, S, Ns, 2, tw, dir); break;
+      case 3: dif_pass<T, V, 3>(X, F, N, S, Ns, 3, tw, dir); break;
+      case 4: dif_pass<T, V, 4>(X, F, N, S, Ns, 4, tw, dir); break;
+      case 5: dif_pass<T, V, 5>(X, F, N, S, Ns, 5, tw, dir); break;
+      case 8: dif_pass<T, V, 8>(X, F, N, S, Ns, 8, tw, dir); break;
+      default:
+        if constexpr (GENERIC) dif_pass<T, V, 13>(X, F, N, S, Ns, r, tw, dir);
+        break;
     }
-    p *= r;
+    Ns /= r;
   }
 }
 

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -84,6 +85,18 @@ struct shtb_plan {
   const double* d_scale = nullptr;        // s_lm table (device) or null
   const double2* d_tw64 = nullptr;        // exp(-2 pi i t / nlon)
   const float2* d_tw32 = nullptr;
+  const int* d_rev = nullptr;             // FFT output position of bin k (digit reversal)
   const double* d_dcoef = nullptr;        // packed d(l,m) = sqrt((l^2-m^2)/(4l^2-1)), l in [m, lrec]
   std::vector<int2> htiles;
+  int* d_err = nullptr;                   // device status word (bounded waits that gave up)
+  // mixed-precision path: FP32 table of P_l^m grouped by (m, parity), built on first use
+  std::mutex tab_mu;
+  float* d_tab = nullptr;
+  const long long* d_tab_seg = nullptr;
+  size_t tab_bytes = 0;
+  int npp = 0;
+  std::vector<long long> htab_seg;
+  std::vector<int2> hmx_tiles;
+  int mx_tiles_key = -1;
+  int2* d_mx_tiles = nullptr;
 };

@@ -177,7 +177,7 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 constexpr int kKC = 32;       // latitude pairs per K chunk
-constexpr int kRS = 66;       // Rs row stride (doubles): [E rows 32][O rows 32] + pad
+constexpr int kRS = 82;       // Rs row stride (doubles): 64 rows, 2 pad doubles after every 8 rows, +2
 
 template <int CT>
 __host__ __device__ constexpr int ana_bs() { return CT + 2; }
@@ -236,15 +236,29 @@ __global__ void __launch_bounds__(256, 1) leg_ana64_kernel(PlanDev P, const doub
       r1 = v.y;
     }
     double* R = Rs + (size_t)(buf * kKC + lane) * kRS;
-#pragma unroll 8
-    for (int rr = 0; rr < 64; ++rr) {
-      const int l = t0 + rr;
-      double r = fma(alph[rr] * x, ra, -rb);
-      r = (l == l0) ? r0 : r;
-      r = (l == l0 + 1) ? r1 : r;
-      rb = ra;
-      ra = r;
-      R[(rr & 1) * 32 + (rr >> 1)] = r;
+#pragma unroll 4
+    for (int rr = 0; rr < 64; rr += 2) {
+      double re, ro;
+      {
+        const int l = t0 + rr;
+        double r = fma(alph[rr] * x, ra, -rb);
+        r = (l == l0) ? r0 : r;
+        r = (l == l0 + 1) ? r1 : r;
+        rb = ra;
+        ra = r;
+        re = r;
+      }
+      {
+        const int l = t0 + rr + 1;
+        double r = fma(alph[rr + 1] * x, ra, -rb);
+        r = (l == l0) ? r0 : r;
+        r = (l == l0 + 1) ? r1 : r;
+        rb = ra;
+        ra = r;
+        ro = r;
+      }
+      // rows (rr, rr+1) = (E row rr/2, O row rr/2) side by side; 16 bytes of padding per 8 rows
+      *reinterpret_cast<double2*>(R + rr + 2 * (rr >> 3)) = make_double2(re, ro);
     }
   };
   auto loadB = [&](int c, int buf) {
@@ -287,11 +301,10 @@ __global__ void __launch_bounds__(256, 1) leg_ana64_kernel(PlanDev P, const doub
       const int k = ks * KPT + kk;
       double rE[TRP], rO[TRP], bE[TC], bO[TC];
 #pragma unroll
-      for (int i = 0; i < TRP; i += 2) {
-        const double2 e = *reinterpret_cast<const double2*>(R + k * kRS + rg * TRP + i);
-        const double2 o = *reinterpret_cast<const double2*>(R + k * kRS + 32 + rg * TRP + i);
-        rE[i] = e.x; rE[i + 1] = e.y;
-        rO[i] = o.x; rO[i + 1] = o.y;
+      for (int i = 0; i < TRP; ++i) {
+        const double2 eo = *reinterpret_cast<const double2*>(R + k * kRS + 10 * rg + 2 * i);
+        rE[i] = eo.x;
+        rO[i] = eo.y;
       }
 #pragma unroll
       for (int q = 0; q < TC; q += 2) {

@@ -223,7 +223,7 @@ extern "C" int shtb_plan_create(shtb_plan** out, int lmax, int mmax, int mres, i
                                            " to resolve every azimuthal order, got nlon=" +
                                            std::to_string(nlon));
   if (!x || !w) return set_error(SHTB_ERR_BAD_ARG, "x and w must be host arrays of nlat values");
-  if (nlon > 16384) return set_error(SHTB_ERR_UNSUPPORTED, "nlon above 16384 is not supported");
+  if (nlon > 8192) return set_error(SHTB_ERR_UNSUPPORTED, "nlon above 8192 is not supported");
   for (int i = 0; i < nlat; ++i) {
     if (!(x[i] >= -1.0 && x[i] <= 1.0)) return set_error(SHTB_ERR_BAD_ARG, "x must lie in [-1, 1]");
     if (i > 0 && !(x[i] < x[i - 1])) return set_error(SHTB_ERR_BAD_ARG, "x must be strictly decreasing (north first)");
@@ -294,6 +294,19 @@ extern "C" int shtb_plan_create(shtb_plan** out, int lmax, int mmax, int mres, i
     const double ang = -2.0 * (double)t / (double)nlon;  // in units of pi
     tw[t] = make_double2(std::cos(M_PI * ang), std::sin(M_PI * ang));
   }
+  std::vector<int> rev(nlon);
+  for (int k = 0; k < nlon; ++k) {
+    if (p->fft.direct) { rev[k] = k; continue; }
+    int pos = 0, kk = k, Ns = nlon;
+    for (int s = 0; s < p->fft.nrad; ++s) {
+      const int r = p->fft.rad[s];
+      const int d = kk % r;
+      kk /= r;
+      Ns /= r;
+      pos += d * Ns;
+    }
+    rev[k] = pos;
+  }
   std::vector<float2> tw32(nlon);
   for (int t = 0; t < nlon; ++t) tw32[t] = make_float2((float)tw[t].x, (float)tw[t].y);
 
@@ -306,7 +319,8 @@ extern "C" int shtb_plan_create(shtb_plan** out, int lmax, int mmax, int mres, i
   const size_t o_ck = take((size_t)ntiles * npair * 16), o_tiles = take((size_t)ntiles * 8);
   const size_t o_scale = coeff_scale ? take((size_t)(lmax + 1) * (mmax + 1) * 8) : 0;
   const size_t o_tw = take((size_t)nlon * 16), o_tw32 = take((size_t)nlon * 8);
-  const size_t o_seed = take((mmax + 2) * 8), o_tb = take(nm * 4);
+  const size_t o_seed = take((mmax + 2) * 8), o_tb = take(nm * 4), o_rev = take((size_t)nlon * 4);
+  const size_t o_err = take(16);
   p->dbytes = o;
   cudaError_t ce = cudaMalloc(&p->dmem, o);
   if (ce != cudaSuccess) {
@@ -331,6 +345,7 @@ extern "C" int shtb_plan_create(shtb_plan** out, int lmax, int mmax, int mres, i
   if (ce == cudaSuccess) ce = up(o_tw32, tw32.data(), (size_t)nlon * 8);
   if (ce == cudaSuccess) ce = up(o_seed, seedfac.data(), (mmax + 2) * 8);
   if (ce == cudaSuccess) ce = up(o_tb, tile_base.data(), nm * 4);
+  if (ce == cudaSuccess) ce = up(o_rev, rev.data(), (size_t)nlon * 4);
   if (ce != cudaSuccess) {
     cudaFree(p->dmem);
     delete p;
@@ -354,6 +369,9 @@ extern "C" int shtb_plan_create(shtb_plan** out, int lmax, int mmax, int mres, i
   p->d_tw64 = (const double2*)(D + o_tw);
   p->d_tw32 = (const float2*)(D + o_tw32);
   p->d_dcoef = (const double*)(D + o_d);
+  p->d_rev = (const int*)(D + o_rev);
+  p->d_err = (int*)(D + o_err);
+  if (ce == cudaSuccess) ce = cudaMemset(D + o_err, 0, 16);
 
   dim3 grid((npair + 127) / 128, nm);
   plan_setup_kernel<<<grid, 128>>>(dv, (const double*)(D + o_seed), (const int*)(D + o_tb), (int*)(D + o_l0),
@@ -376,12 +394,28 @@ extern "C" int shtb_plan_destroy(shtb_plan* p) {
   cudaGetDevice(&dev);
   if (dev != p->device) cudaSetDevice(p->device);
   cudaError_t e = cudaFree(p->dmem);
+  if (p->d_tab) cudaFree(p->d_tab);
+  if (p->d_mx_tiles) cudaFree(p->d_mx_tiles);
   if (dev >= 0 && dev != p->device) cudaSetDevice(dev);
   delete p;
   return check_cuda(e, "plan destroy");
 }
 
-extern "C" size_t shtb_plan_table_bytes(const shtb_plan* p) { return p ? p->dbytes : 0; }
+extern "C" size_t shtb_plan_table_bytes(const shtb_plan* p) { return p ? p->dbytes + p->tab_bytes : 0; }
+
+// Synchronizes the device and reports whether any kernel of this plan gave up a
+// bounded wait since the last call (the status word is cleared).
+extern "C" int shtb_plan_status(const shtb_plan* p) {
+  if (!p) return set_error(SHTB_ERR_BAD_ARG, "plan is NULL");
+  int h = 0;
+  cudaError_t e = cudaMemcpy(&h, p->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return set_error(SHTB_ERR_CUDA, std::string("plan status: ") + cudaGetErrorString(e));
+  if (h) {
+    cudaMemset(p->d_err, 0, sizeof(int));
+    return set_error(SHTB_ERR_TIMEOUT, "a device wait exceeded its time limit; results of the affected call are invalid");
+  }
+  return SHTB_OK;
+}
 
 // ---------------------------------------------------------------------------
 // per-kernel event timing

@@ -179,6 +179,8 @@ static int check_common(const shtb_plan* p, int nf, int* ltr, int dtype, int pre
   if (dtype != SHTB_F64 && dtype != SHTB_F32) return set_error(SHTB_ERR_BAD_ARG, "unknown dtype");
   if (precision == SHTB_PREC_FP64 && dtype != SHTB_F64)
     return set_error(SHTB_ERR_UNSUPPORTED, "the FP64 path takes double buffers (dtype SHTB_F64)");
+  if (precision == SHTB_PREC_MIXED && dtype != SHTB_F32)
+    return set_error(SHTB_ERR_UNSUPPORTED, "the mixed-precision path takes float buffers (dtype SHTB_F32)");
   const size_t need = shtb_workspace_bytes(p, op, nf, dtype, precision);
   if (!work || wb < need)
     return set_error(SHTB_ERR_WORKSPACE, "workspace of " + std::to_string(need) + " bytes required, got " +

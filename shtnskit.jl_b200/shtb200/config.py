@@ -175,6 +175,13 @@ class Plan:
     def table_bytes(self) -> int:
         return int(_lib.load().shtb_plan_table_bytes(self.handle))
 
+    def status(self) -> None:
+        """Raise BackendUnavailableError if a kernel of this plan gave up a bounded device wait."""
+        import torch
+
+        with torch.cuda.device(self.device_index):
+            _lib.check(_lib.load().shtb_plan_status(self.handle), "plan_status")
+
     def destroy(self) -> None:
         if getattr(self, "_alive", False):
             self._alive = False

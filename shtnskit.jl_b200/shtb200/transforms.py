@@ -374,7 +374,10 @@ def _synthesis_impl(cfg, alm, batched, real_output, use_rfft, fft_scratch, lcap,
             synthesis_device(cfg, a3.detach(), tmp, ltr, prec)
             out.copy_(tmp.reshape(out.shape))
             return out
-        synthesis_device(cfg, a3.detach(), f if out is None else f.reshape(cfg.nlat, cfg.nlon, nf), ltr, prec)
+        if out is not None:
+            synthesis_device(cfg, a3.detach(), out.reshape(cfg.nlat, cfg.nlon, nf), ltr, prec)
+            return out
+        synthesis_device(cfg, a3.detach(), f, ltr, prec)
     return f if batched else f[:, :, 0]
 
 

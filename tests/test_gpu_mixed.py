@@ -1,0 +1,80 @@
+"""GPU parity of the mixed-precision (tensor-core 3xTF32) path.
+
+Inputs are rounded to FP32 (the path's I/O type); the FP64 oracle runs on the same
+rounded inputs. Bar: relative L2 <= 1e-6 against the FP64 result.
+"""
+import numpy as np
+import pytest
+import torch
+
+import shtb200 as sht
+from oracle import sht_oracle as so
+
+from _util import rand_alm, rel_l2
+
+pytestmark = pytest.mark.gpu
+TOLMX = 1e-6
+
+CASES = [
+    dict(lmax=15, nlat=16, nlon=32),
+    dict(lmax=31, nlat=33, nlon=64),
+    dict(lmax=63, nlat=64, nlon=128),
+    dict(lmax=40, nlat=44, nlon=90, mmax=30),
+    dict(lmax=30, nlat=32, nlon=64, mres=3, mmax=30),
+    dict(lmax=127, nlat=128, nlon=256),
+    dict(lmax=20, nlat=22, nlon=42, norm="schmidt", cs_phase=False),
+]
+
+
+def host(t):
+    torch.cuda.synchronize()
+    return sht.to_host(t)
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: "-".join(f"{k}{v}" for k, v in c.items()))
+@pytest.mark.parametrize("nf", [1, 9, 20, 64])
+def test_mixed_vs_fp64_oracle(case, nf):
+    c = dict(case)
+    lmax, nlat = c.pop("lmax"), c.pop("nlat")
+    cfg = sht.create_gauss_config(lmax, nlat, **c)
+    ocfg = so.create_gauss_config(lmax, nlat, **c)
+    a = rand_alm(lmax, cfg.mmax, nf, seed=3, mres=cfg.mres).astype(np.complex64).astype(np.complex128)
+    f = sht.synthesis_batch(cfg, a.astype(np.complex64), precision="mixed")
+    fh = host(f)
+    assert fh.dtype == np.float32
+    f_ref = so.synthesis_batch(ocfg, a)
+    assert rel_l2(fh, f_ref) <= TOLMX
+    g = np.random.default_rng(4).standard_normal((nlat, cfg.nlon, nf)).astype(np.float32)
+    b = host(sht.analysis_batch(cfg, g, precision="mixed"))
+    b_ref = so.analysis_batch(ocfg, g.astype(np.float64))
+    assert rel_l2(b, b_ref) <= TOLMX
+    cfg.plan(0).status()
+
+
+def test_mixed_lcap():
+    cfg = sht.create_gauss_config(40, 42, nlon=81)
+    ocfg = so.create_gauss_config(40, 42, nlon=81)
+    a = rand_alm(40, 40, 3, seed=5).astype(np.complex64).astype(np.complex128)
+    for ltr in (3, 17, 40):
+        f = host(sht.synthesis_batch(cfg, a.astype(np.complex64), lcap=ltr, precision="mixed"))
+        ref = np.stack([so.synthesis(ocfg, a[:, :, k], ltr=ltr) for k in range(3)], axis=2)
+        assert rel_l2(f, ref) <= TOLMX
+        g = np.random.default_rng(6).standard_normal((42, 81, 3)).astype(np.float32)
+        b = host(sht.analysis_batch(cfg, g, lcap=ltr, precision="mixed"))
+        bref = np.stack([so.analysis(ocfg, g[:, :, k].astype(np.float64), ltr=ltr) for k in range(3)], axis=2)
+        assert rel_l2(b, bref) <= TOLMX
+
+
+def test_mixed_config3_size():
+    """lmax=1023, 1024x2048, 64 fields: mixed roundtrip against the FP64 GPU path at <= 1e-6."""
+    cfg = sht.create_gauss_config(1023, 1024, nlon=2048)
+    a = rand_alm(1023, 1023, 64, seed=7).astype(np.complex64)
+    a64 = a.astype(np.complex128)
+    f32 = sht.synthesis_batch(cfg, a, precision="mixed")
+    f64 = sht.synthesis_batch(cfg, a64)
+    assert rel_l2(host(f32), host(f64)) <= TOLMX
+    b32 = sht.analysis_batch(cfg, f32, precision="mixed")
+    b64 = sht.analysis_batch(cfg, f64)
+    assert rel_l2(host(b32), host(b64)) <= TOLMX
+    assert rel_l2(host(b32), a64) <= TOLMX
+    cfg.plan(0).status()
