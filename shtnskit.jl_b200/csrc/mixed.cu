@@ -12,11 +12,16 @@
 // mixed_table_kernel from the FP64 recurrence (extended-range seeds and FP64
 // recurrence coefficients), so every P value is the FP64 result rounded once.
 //
-// CTA organisation (288 threads): warps 0-7 are two producer groups of 128
-// threads that load operands, split them into hi/lo and store K-major tiles
-// (no swizzle) into a 6-stage shared-memory ring, alternating stages; warp 8
-// allocates TMEM and one of its threads issues the MMAs and tcgen05.commit
-// releases each stage. Warps 0-3 then read the accumulators with tcgen05.ld.
+// CTA organisation (544 threads, one parity class per CTA): warps 0-7 are two
+// producer groups of 128 threads that load operands, split them into hi/lo and
+// store K-major tiles (no swizzle) into an 8-stage shared-memory ring,
+// alternating stages; warp 8 allocates TMEM and one of its threads issues the
+// MMAs (tcgen05.commit releases each stage). The tensor core accumulates only
+// kChunk K-steps into one of two TMEM buffers (hi*hi and the small cross terms
+// in separate accumulators); warps 9-16 drain each finished chunk with
+// tcgen05.ld into round-to-nearest FP32 register sums. Long accumulation chains
+// inside the tensor core round toward zero and would bias sums of many terms;
+// short chunks keep that bias below 1e-6 relative at any lmax.
 // Every mbarrier wait is bounded (2 s of %globaltimer); a timeout sets the
 // plan's error word and the CTA drains and exits.
 #include <climits>
@@ -28,8 +33,9 @@ namespace mx {
 
 constexpr int kM = 128;          // UMMA M
 constexpr int kK = 8;            // TF32 K per instruction
-constexpr int kStages = 6;
-constexpr int kThreads = 288;
+constexpr int kStages = 8;
+constexpr int kChunk = 4;          // K-steps accumulated in TMEM before promotion
+constexpr int kThreads = 544;       // 8 producer warps, 1 MMA warp, 8 promotion warps
 constexpr int kTileBytesA = kM * kK * 4;  // 4 KB
 constexpr unsigned long long kWaitNs = 2000000000ull;
 
@@ -166,125 +172,132 @@ __device__ __forceinline__ float coef_factor(const Args& a, int l, int m) {
 template <int N>
 struct Smem {
   static constexpr int kTileB = N * kK * 4;
-  // per stage: A_E_hi, A_E_lo, A_O_hi, A_O_lo, B_E_hi, B_E_lo, B_O_hi, B_O_lo
-  static constexpr int kStage = 4 * kTileBytesA + 4 * kTileB;
+  // per stage: A_hi, A_lo, B_hi, B_lo (one parity class per CTA)
+  static constexpr int kStage = 2 * kTileBytesA + 2 * kTileB;
   static constexpr int kBar = kStages * kStage;
-  static constexpr int kBytes = kBar + (2 * kStages + 1) * 8 + 16;
+  static constexpr int kBytes = kBar + (2 * kStages + 4) * 8 + 16;
 };
 
+__device__ __forceinline__ void store_split4(unsigned char* hi, unsigned char* lo, int row, int khalf, const float* v) {
+  float4 h, l;
+  h.x = tf32_rn(v[0]); h.y = tf32_rn(v[1]); h.z = tf32_rn(v[2]); h.w = tf32_rn(v[3]);
+  l.x = tf32_rn(v[0] - h.x); l.y = tf32_rn(v[1] - h.y); l.z = tf32_rn(v[2] - h.z); l.w = tf32_rn(v[3] - h.w);
+  *reinterpret_cast<float4*>(hi + tile_off(row, khalf)) = h;
+  *reinterpret_cast<float4*>(lo + tile_off(row, khalf)) = l;
+}
+
 // MODE 0: synthesis, MODE 1: analysis. N = columns per CTA (2 x fields).
+// blockIdx.x = 2 * tile + parity; one CTA accumulates one parity class.
 template <int MODE, int N>
 __global__ void __launch_bounds__(kThreads, 1) mixed_gemm_kernel(const __grid_constant__ Args a) {
   using S = Smem<N>;
   extern __shared__ __align__(1024) unsigned char sm[];
   unsigned long long* full = reinterpret_cast<unsigned long long*>(sm + S::kBar);
   unsigned long long* empty = full + kStages;
-  unsigned long long* done = empty + kStages;
-  unsigned* tmem_slot = reinterpret_cast<unsigned*>(done + 1);
+  unsigned long long* accf = empty + kStages;   // [2] chunk accumulated in TMEM buffer b
+  unsigned long long* acce = accf + 2;          // [2] TMEM buffer b drained by the promotion warps
+  unsigned* tmem_slot = reinterpret_cast<unsigned*>(acce + 2);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
-  const int tid = threadIdx.x, warp = tid >> 5;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const PlanDev& P = a.P;
   const int npair = P.npair;
+  const int par = blockIdx.x & 1, tile = blockIdx.x >> 1;
   int im, p0 = 0, j0 = 0;
   if (MODE == 0) {
     im = blockIdx.y;
-    p0 = blockIdx.x * kM;
+    p0 = tile * kM;
   } else {
-    const int2 t = a.tiles[blockIdx.x];
+    const int2 t = a.tiles[tile];
     im = t.x;
     j0 = t.y;
   }
   const int m = im * P.mres;
   const int kb = blockIdx.z * (N / 2);
-  // degrees of each parity class present in [m, lend]
-  const int JE = (a.lend >= m) ? (a.lend - m) / 2 + 1 : 0;
-  const int JO = (a.lend >= m + 1) ? (a.lend - m - 1) / 2 + 1 : 0;
-  const long long segE = a.seg[2 * im], segO = a.seg[2 * im + 1];
-  const long long lenE = a.seg[2 * im + 1] - segE, lenO = a.seg[2 * im + 2] - segO;
-  const int nks = (MODE == 0) ? (JE + kK - 1) / kK : (npair + kK - 1) / kK;
+  // degrees of this parity class in [m, lend]
+  const int J = (a.lend >= m + par) ? (a.lend - m - par) / 2 + 1 : 0;
+  const long long sg = a.seg[2 * im + par];
+  const long long ln = a.seg[2 * im + par + 1] - sg;
+  const int nks = (MODE == 0) ? (J + kK - 1) / kK : (npair + kK - 1) / kK;
+  const int nch = (nks + kChunk - 1) / kChunk;
 
   if (tid == 0) {
     for (int s = 0; s < kStages; ++s) {
       mbar_init(&full[s], 128);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(done, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&accf[b], 1);
+      mbar_init(&acce[b], 256);
+    }
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 8) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(2 * N));
+                 "r"(4 * N));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const unsigned tmem = *tmem_slot;
+  // TMEM: buffer b holds the hi*hi chunk sum at column 2bN and the cross terms at 2bN + N
 
   if (warp < 8) {
     // ------------------------------------------------------------- producers
     const int g = warp >> 2, t = tid & 127;
-    float va[2][kK], vb[2][kK];   // [parity][k] for A row t; B: [re|im][k] of (field t/2, parity t%2)
-    const int bf = t >> 1, bpar = t & 1;
+    const int bf = t >> 1, bh = t & 1;           // B: field bf, K half bh (4 values)
     const bool bact = bf < N / 2;
+    float va[kK], vb[2][4];
     auto load = [&](int ks) {
-      // A operand row t
+      if (MODE == 0) {
+        const int pr = p0 + t;
 #pragma unroll
-      for (int par = 0; par < 2; ++par) {
-        const long long sg = par ? segO : segE, ln = par ? lenO : lenE;
-        if (MODE == 0) {
-          const int pr = p0 + t;
-#pragma unroll
-          for (int k = 0; k < kK; ++k) {
-            const int j = ks * kK + k;
-            va[par][k] = (j < ln) ? a.tab[(sg + j) * a.npp + pr] : 0.f;
-          }
+        for (int k = 0; k < kK; ++k) {
+          const int j = ks * kK + k;
+          va[k] = (j < ln) ? a.tab[(sg + j) * a.npp + pr] : 0.f;
+        }
+      } else {
+        const int j = j0 + t;
+        if (j < ln) {
+          const float4* q = reinterpret_cast<const float4*>(a.tab + (sg + j) * a.npp + ks * kK);
+          const float4 x0 = q[0], x1 = q[1];
+          va[0] = x0.x; va[1] = x0.y; va[2] = x0.z; va[3] = x0.w;
+          va[4] = x1.x; va[5] = x1.y; va[6] = x1.z; va[7] = x1.w;
         } else {
-          const int j = j0 + t;
-          if (j < ln) {
-            const float4* q = reinterpret_cast<const float4*>(a.tab + (sg + j) * a.npp + ks * kK);
-            const float4 x0 = q[0], x1 = q[1];
-            va[par][0] = x0.x; va[par][1] = x0.y; va[par][2] = x0.z; va[par][3] = x0.w;
-            va[par][4] = x1.x; va[par][5] = x1.y; va[par][6] = x1.z; va[par][7] = x1.w;
-          } else {
 #pragma unroll
-            for (int k = 0; k < kK; ++k) va[par][k] = 0.f;
-          }
+          for (int k = 0; k < kK; ++k) va[k] = 0.f;
         }
       }
-      // B operand rows (2 bf, 2 bf + 1) of parity bpar
       const int kf = kb + bf;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) vb[0][k] = vb[1][k] = 0.f;
       if (bact && kf < a.nf) {
         if (MODE == 0) {
           const float2* c = a.cin + (long long)kf * a.ld_k + (long long)m * (P.lmax + 1);
 #pragma unroll
-          for (int k = 0; k < kK; ++k) {
-            const int l = m + 2 * (ks * kK + k) + bpar;
-            float2 v = make_float2(0.f, 0.f);
+          for (int k = 0; k < 4; ++k) {
+            const int l = m + 2 * (ks * kK + 4 * bh + k) + par;
             if (l <= a.lend) {
-              v = c[l];
+              float2 v = c[l];
               const float s = coef_factor(a, l, m);
-              v.x *= s;
-              v.y *= s;
+              vb[0][k] = v.x * s;
+              vb[1][k] = v.y * s;
             }
-            vb[0][k] = v.x;
-            vb[1][k] = v.y;
           }
         } else {
-          const float2* w = a.Win + (((long long)kf * P.nm + im) * 2 + bpar) * npair;
+          const float2* w = a.Win + (((long long)kf * P.nm + im) * 2 + par) * npair;
 #pragma unroll
-          for (int k = 0; k < kK; ++k) {
-            const int pr = ks * kK + k;
-            const float2 v = (pr < npair) ? w[pr] : make_float2(0.f, 0.f);
-            vb[0][k] = v.x;
-            vb[1][k] = v.y;
+          for (int k = 0; k < 4; ++k) {
+            const int pr = ks * kK + 4 * bh + k;
+            if (pr < npair) {
+              const float2 v = w[pr];
+              vb[0][k] = v.x;
+              vb[1][k] = v.y;
+            }
           }
         }
-      } else {
-#pragma unroll
-        for (int k = 0; k < kK; ++k) vb[0][k] = vb[1][k] = 0.f;
       }
     };
     if (g < nks) load(g);
@@ -293,103 +306,88 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_gemm_kernel(const __grid_co
       if (ks >= kStages)
         if (!mbar_wait(&empty[b], ((ks / kStages) - 1) & 1, abort_flag, a.err)) break;
       unsigned char* st = sm + (size_t)b * S::kStage;
-      unsigned char* AEh = st;
-      unsigned char* AEl = st + kTileBytesA;
-      unsigned char* AOh = st + 2 * kTileBytesA;
-      unsigned char* AOl = st + 3 * kTileBytesA;
-      unsigned char* BEh = st + 4 * kTileBytesA;
-      unsigned char* BEl = BEh + S::kTileB;
-      unsigned char* BOh = BEh + 2 * S::kTileB;
-      unsigned char* BOl = BEh + 3 * S::kTileB;
-      store_split8(AEh, AEl, t, va[0]);
-      store_split8(AOh, AOl, t, va[1]);
+      store_split8(st, st + kTileBytesA, t, va);
       if (bact) {
-        unsigned char* bh = bpar ? BOh : BEh;
-        unsigned char* bl = bpar ? BOl : BEl;
-        store_split8(bh, bl, 2 * bf, vb[0]);
-        store_split8(bh, bl, 2 * bf + 1, vb[1]);
+        unsigned char* bh_ = st + 2 * kTileBytesA;
+        unsigned char* bl_ = bh_ + S::kTileB;
+        store_split4(bh_, bl_, 2 * bf, bh, vb[0]);
+        store_split4(bh_, bl_, 2 * bf + 1, bh, vb[1]);
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive(&full[b]);
       if (ks + 2 < nks) load(ks + 2);
     }
-  } else if (tid == 8 * 32) {
+  } else if (warp == 8) {
     // ------------------------------------------------------------- MMA issuer
-    constexpr unsigned id = 0;
-    const unsigned idesc = idesc_tf32<N>();
-    (void)id;
-    const unsigned dE = tmem, dO = tmem + N;
-    const int nE = (MODE == 0) ? (JE + kK - 1) / kK : nks;
-    const int nO = (MODE == 0) ? (JO + kK - 1) / kK : (JO > 0 ? nks : 0);
-    bool ok = true;
-    for (int ks = 0; ks < nks; ++ks) {
-      const int b = ks % kStages;
-      if (!mbar_wait(&full[b], (ks / kStages) & 1, abort_flag, a.err)) {
-        ok = false;
-        break;
+    if (lane == 0) {
+      const unsigned idesc = idesc_tf32<N>();
+      bool ok = true;
+      for (int c = 0; c < nch && ok; ++c) {
+        const int bb = c & 1;
+        if (c >= 2 && !mbar_wait(&acce[bb], ((c >> 1) - 1) & 1, abort_flag, a.err)) break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const unsigned dH = tmem + 2 * bb * N, dX = dH + N;
+        const int k1 = min(nks, (c + 1) * kChunk);
+        for (int ks = c * kChunk; ks < k1; ++ks) {
+          const int b = ks % kStages;
+          if (!mbar_wait(&full[b], (ks / kStages) & 1, abort_flag, a.err)) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          unsigned char* st = sm + (size_t)b * S::kStage;
+          const unsigned long long ah = sdesc(st), al = sdesc(st + kTileBytesA);
+          const unsigned long long bh_ = sdesc(st + 2 * kTileBytesA), bl_ = sdesc(st + 2 * kTileBytesA + S::kTileB);
+          const unsigned acc = (ks == c * kChunk) ? 0u : 1u;
+          mma_tf32(dH, ah, bh_, idesc, acc);
+          mma_tf32(dX, ah, bl_, idesc, acc);
+          mma_tf32(dX, al, bh_, idesc, 1u);
+          mma_commit(&empty[b]);
+        }
+        mma_commit(&accf[bb]);
       }
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      unsigned char* st = sm + (size_t)b * S::kStage;
-      const unsigned long long aEh = sdesc(st), aEl = sdesc(st + kTileBytesA);
-      const unsigned long long aOh = sdesc(st + 2 * kTileBytesA), aOl = sdesc(st + 3 * kTileBytesA);
-      unsigned char* bB = st + 4 * kTileBytesA;
-      const unsigned long long bEh = sdesc(bB), bEl = sdesc(bB + S::kTileB);
-      const unsigned long long bOh = sdesc(bB + 2 * S::kTileB), bOl = sdesc(bB + 3 * S::kTileB);
-      if (ks < nE) {
-        mma_tf32(dE, aEh, bEh, idesc, ks > 0 ? 1u : 0u);
-        mma_tf32(dE, aEh, bEl, idesc, 1u);
-        mma_tf32(dE, aEl, bEh, idesc, 1u);
-      }
-      if (ks < nO) {
-        mma_tf32(dO, aOh, bOh, idesc, ks > 0 ? 1u : 0u);
-        mma_tf32(dO, aOh, bOl, idesc, 1u);
-        mma_tf32(dO, aOl, bOh, idesc, 1u);
-      }
-      mma_commit(&empty[b]);
     }
-    mma_commit(done);
-    (void)ok;
-  }
-
-  // ------------------------------------------------------------- epilogue (warps 0-3)
-  if (warp < 4) {
-    const bool ok = mbar_wait(done, 0, abort_flag, a.err);
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const int t = tid;
-    const unsigned lane_base = (unsigned)(warp * 32) << 16;
-    const bool haveO = JO > 0;
-    __syncwarp();
-#pragma unroll 1
-    for (int c0 = 0; c0 < N; c0 += 16) {
-      float e[16], o[16];
-      tmem_ld16(tmem + lane_base + c0, e);
-      tmem_ld16(tmem + lane_base + N + c0, o);
-      if (!ok) continue;
-      if (!haveO) {
+  } else {
+    // ------------------------------------------------------------- promotion warps (9..16)
+    const int q = warp & 3;                        // TMEM lane quadrant this warp may access
+    const int h = (warp - 9) >> 2;                 // column half
+    const int row = 32 * q + lane;
+    const unsigned lane_base = (unsigned)(32 * q) << 16;
+    float acc[N / 2];
 #pragma unroll
-        for (int i = 0; i < 16; ++i) o[i] = 0.f;
+    for (int i = 0; i < N / 2; ++i) acc[i] = 0.f;
+    bool ok = true;
+    for (int c = 0; c < nch; ++c) {
+      const int bb = c & 1;
+      if (ok) ok = mbar_wait(&accf[bb], (c >> 1) & 1, abort_flag, a.err);
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      __syncwarp();
+      const unsigned dH = tmem + lane_base + 2 * bb * N + h * (N / 2), dX = dH + N;
+#pragma unroll
+      for (int i = 0; i < N / 2; i += 16) {
+        float vh[16], vx[16];
+        tmem_ld16(dH + i, vh);
+        tmem_ld16(dX + i, vx);
+#pragma unroll
+        for (int u = 0; u < 16; ++u) acc[i + u] += vh[u] + vx[u];
       }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      mbar_arrive(&acce[bb]);
+      if (!ok) break;
+    }
+    if (ok) {
 #pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const int kf = kb + (c0 >> 1) + q;
+      for (int qq = 0; qq < N / 4; ++qq) {
+        const int kf = kb + h * (N / 4) + qq;
         if (kf >= a.nf) continue;
         if (MODE == 0) {
-          const int pr = p0 + t;
-          if (pr < npair) {
-            const size_t base = (((size_t)kf * P.nm + im) * 2) * npair + pr;
-            a.Wout[base] = make_float2(e[2 * q], e[2 * q + 1]);
-            a.Wout[base + npair] = make_float2(o[2 * q], o[2 * q + 1]);
-          }
+          const int pr = p0 + row;
+          if (pr < npair) a.Wout[(((size_t)kf * P.nm + im) * 2 + par) * npair + pr] = make_float2(acc[2 * qq], acc[2 * qq + 1]);
         } else {
-          const int lE = m + 2 * (j0 + t), lO = lE + 1;
-          float2* c = a.cout + (long long)kf * a.ld_k + (long long)m * (P.lmax + 1);
-          if (lE <= a.lcap) {
-            const float s = coef_factor(a, lE, m);
-            c[lE] = make_float2(e[2 * q] * s, e[2 * q + 1] * s);
-          }
-          if (lO <= a.lcap) {
-            const float s = coef_factor(a, lO, m);
-            c[lO] = make_float2(o[2 * q] * s, o[2 * q + 1] * s);
+          const int l = m + 2 * (j0 + row) + par;
+          if (l <= a.lcap) {
+            const float s = coef_factor(a, l, m);
+            a.cout[(long long)kf * a.ld_k + (long long)m * (P.lmax + 1) + l] = make_float2(acc[2 * qq] * s, acc[2 * qq + 1] * s);
           }
         }
       }
@@ -399,7 +397,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_gemm_kernel(const __grid_co
   __syncthreads();
   if (warp == 8) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * N));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(4 * N));
   }
 }
 
@@ -529,7 +527,7 @@ int mixed_synthesis(const shtb_plan* p, const void* alm, void* f, int nf, int lt
   a.nf = nf;
   a.lend = ltr;
   a.lcap = ltr;
-  dim3 g((p->npair + kM - 1) / kM, mlim / p->mres + 1);
+  dim3 g(2 * ((p->npair + kM - 1) / kM), mlim / p->mres + 1);
   if ((rc = dispatch_gemm<0>(p, a, nf, g, st))) return rc;
   return launch_fft_syn<float, float>(p, work, (float*)f, nullptr, 1, nf, mlim, p->phi_inv_scale / p->nlon, 0, 0, st);
 }
@@ -566,7 +564,7 @@ int mixed_analysis(const shtb_plan* p, const void* f, void* alm, int nf, int ltr
   a.lend = ltr;
   a.lcap = ltr;
   a.tiles = p->d_mx_tiles;
-  dim3 g((unsigned)tl.size(), 1);
+  dim3 g(2 * (unsigned)tl.size(), 1);
   if ((rc = dispatch_gemm<1>(p, a, nf, g, st))) return rc;
   dim3 zg((p->lmax + 1 + 127) / 128, p->mmax + 1, nf);
   prof_begin(st);
