@@ -208,7 +208,8 @@ def sectoral_seed(s: np.ndarray, m: int) -> tuple[np.ndarray, np.ndarray]:
             small = (np.abs(pmm) < TINY) & (pmm != 0)
             if not small.any():
                 break
-            pmm = np.where(small, pmm * up, pmm)
+            with np.errstate(over="ignore"):
+                pmm = np.where(small, pmm * up, pmm)
             e = np.where(small, e - SHIFT, e)
         k = kend + 1
     return pmm, e
