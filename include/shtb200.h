@@ -148,6 +148,21 @@ int shtb_analysis_sphtor_adjoint(const shtb_plan* plan, const void* Sbar, const 
                                  void* Vtbar, void* Vpbar, int nfields,
                                  void* work, size_t work_bytes, void* stream);
 
+/*
+ * Scalar FP64 synthesis that allocates no device memory and takes no workspace.
+ * No counterpart in the reference: it exists for hosts that must not call cudaMalloc
+ * between transforms (code running inside another runtime's memory pool, or long runs
+ * where an allocation could synchronize the device or fail). Same inputs, outputs and
+ * results as shtb_synthesis with dtype SHTB_F64 and precision SHTB_PREC_FP64.
+ * Scratch: a 32 MiB array owned by the library on every GPU that loads it (until process
+ * exit); calls needing more (nfields * (mmax/mres+1) * 2 * ceil(nlat/2) * 16 bytes) return
+ * SHTB_ERR_WORKSPACE. The first call on each device looks up the array's device address
+ * (make that first call before any stream capture). All calls share the array: calls that
+ * overlap on the GPU (other streams or other host threads) race and must be serialized.
+ */
+int shtb_synthesis_noalloc(const shtb_plan* plan, const void* alm, void* f, int nfields, int ltr,
+                           void* stream);
+
 /* Number of kernels the library launched on this host thread since the last reset. */
 uint64_t shtb_launch_count(int reset);
 
