@@ -1,7 +1,15 @@
 // fft.cu — longitude FFT kernels fused with the equatorial fold/unfold.
 //
-// Synthesis (shtb_fft_syn): W[k][im][E|O][pair] -> grid rows north/south.
-// Analysis  (shtb_fft_ana): grid rows north/south -> W[k][im][E|O][pair], weighted.
+// Synthesis (fft_syn_kernel): W[k][im][E|O][pair] -> grid rows north/south.
+// Analysis  (fft_ana_kernel): grid rows north/south -> W[k][im][E|O][pair], weighted.
+//
+// A CTA owns H consecutive latitude pairs of one field (H templated so the per-pair
+// values live in registers). Global traffic moves in whole segments: a longitude row
+// j of the grid contributes H north values (contiguous) and H south values
+// (contiguous, reversed order), loaded/stored as 16-byte vectors when the grid's
+// latitude count allows; W is read/written per order m as H contiguous complex values.
+// The FFT itself (fft.cuh) leaves bins in digit-reversed positions, so the synthesis
+// output loop walks shared memory in storage order q and writes longitude rinv[q].
 #include "fft.cuh"
 #include "kernels.cuh"
 
@@ -18,31 +26,61 @@ __device__ __forceinline__ T pair_factor(const PlanDev& P, int pair, double scal
   return (T)g;
 }
 
-template <typename T, typename GT, bool GENERIC>
-__global__ void __launch_bounds__(256) fft_syn_kernel(PlanDev P, FFTDesc fd, const int* __restrict__ rev,
-                                                      const typename V2<T>::type* __restrict__ W,
-                                                       GT* __restrict__ out0, GT* __restrict__ out1, int ncomp,
-                                                       int mlim, int H, double gscale, int use_w, int spow,
-                                                       const typename V2<T>::type* __restrict__ tw) {
+// 16-byte vector of grid values
+template <typename T> struct Vec16;
+template <> struct Vec16<float> { using type = float4; static constexpr int n = 4; };
+template <> struct Vec16<double> { using type = double2; static constexpr int n = 2; };
+
+template <typename T, int NV>
+__device__ __forceinline__ void load_seg(const T* __restrict__ src, T* v) {
+  using VT = typename Vec16<T>::type;
+  constexpr int L = Vec16<T>::n;
+#pragma unroll
+  for (int c = 0; c < NV / L; ++c) {
+    const VT x = *reinterpret_cast<const VT*>(src + c * L);
+    const T* xs = reinterpret_cast<const T*>(&x);
+#pragma unroll
+    for (int u = 0; u < L; ++u) v[c * L + u] = xs[u];
+  }
+}
+template <typename T, int NV>
+__device__ __forceinline__ void store_seg(T* __restrict__ dst, const T* v) {
+  using VT = typename Vec16<T>::type;
+  constexpr int L = Vec16<T>::n;
+#pragma unroll
+  for (int c = 0; c < NV / L; ++c) {
+    VT x;
+    T* xs = reinterpret_cast<T*>(&x);
+#pragma unroll
+    for (int u = 0; u < L; ++u) xs[u] = v[c * L + u];
+    *reinterpret_cast<VT*>(dst + c * L) = x;
+  }
+}
+
+template <typename T, int H, bool GENERIC>
+__global__ void __launch_bounds__(512) fft_syn_kernel(PlanDev P, FFTDesc fd, const int* __restrict__ rinv,
+                                                      const typename V2<T>::type* __restrict__ W, T* __restrict__ out0,
+                                                      T* __restrict__ out1, int ncomp, int mlim, double gscale,
+                                                      int use_w, int spow, const typename V2<T>::type* __restrict__ tw) {
   using V = typename V2<T>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int N = fd.n, S = fft_row_stride(N);
   V* Z = reinterpret_cast<V*>(smem_raw);
   V* scratch = Z + H * S;
-  T* gfac = reinterpret_cast<T*>(Z + (fd.direct ? 2 : 1) * H * S);
+  T* gfac = reinterpret_cast<T*>(Z + ((GENERIC && fd.direct) ? 2 : 1) * H * S);
   const int p0 = blockIdx.x * H;
   const int k = blockIdx.y;
   const int npair = P.npair, nlat = P.nlat;
+  const int hv = min(H, npair - p0);
   for (int idx = threadIdx.x; idx < H * S; idx += blockDim.x) {
     V z;
     z.x = 0; z.y = 0;
     Z[idx] = z;
   }
-  for (int h = threadIdx.x; h < H; h += blockDim.x)
-    gfac[h] = (p0 + h < npair) ? pair_factor<T>(P, p0 + h, gscale, use_w, spow) : (T)0;
+  for (int h = threadIdx.x; h < H; h += blockDim.x) gfac[h] = (h < hv) ? pair_factor<T>(P, p0 + h, gscale, use_w, spow) : (T)0;
   __syncthreads();
   const int nmu = mlim / P.mres + 1;
-  // batched loads (U items in flight per thread) for memory-level parallelism
+  // one (im, pair) item per thread; consecutive threads read consecutive pairs of one m
   constexpr int U = 4;
   for (int base0 = threadIdx.x; base0 < nmu * H; base0 += blockDim.x * U) {
     V Ev[U], Ov[U];
@@ -51,9 +89,9 @@ __global__ void __launch_bounds__(256) fft_syn_kernel(PlanDev P, FFTDesc fd, con
       const int idx = base0 + u * blockDim.x;
       Ev[u].x = Ev[u].y = Ov[u].x = Ov[u].y = 0;
       if (idx < nmu * H) {
-        const int im = idx / H, h = idx - im * H, pair = p0 + h;
-        if (pair < npair) {
-          const size_t base = ((size_t)k * P.nm + im) * 2 * npair + pair;
+        const int im = idx / H, h = idx - im * H;
+        if (h < hv) {
+          const size_t base = ((size_t)k * P.nm + im) * 2 * npair + p0 + h;
           Ev[u] = W[base];
           Ov[u] = W[base + npair];
         }
@@ -63,8 +101,7 @@ __global__ void __launch_bounds__(256) fft_syn_kernel(PlanDev P, FFTDesc fd, con
     for (int u = 0; u < U; ++u) {
       const int idx = base0 + u * blockDim.x;
       if (idx >= nmu * H) continue;
-      const int im = idx / H, h = idx - im * H, pair = p0 + h;
-      if (pair >= npair) continue;
+      const int im = idx / H, h = idx - im * H;
       const int m = im * P.mres;
       const V XN = cadd(Ev[u], Ov[u]), XS = csub(Ev[u], Ov[u]);
       if (m == 0) {
@@ -82,75 +119,103 @@ __global__ void __launch_bounds__(256) fft_syn_kernel(PlanDev P, FFTDesc fd, con
   }
   __syncthreads();
   fft_rows<T, V, GENERIC>(Z, scratch, H, S, fd, tw, +1);
-  GT* out = (ncomp == 2 && (k & 1)) ? out1 : out0;
+  T* out = (ncomp == 2 && (k & 1)) ? out1 : out0;
   const size_t kk = (ncomp == 2) ? (size_t)(k >> 1) : (size_t)k;
   const size_t fbase = kk * (size_t)nlat * N;
-  for (int idx = threadIdx.x; idx < N * H; idx += blockDim.x) {
-    const int j = idx / H, h = idx - j * H, pair = p0 + h;
-    if (pair >= npair) continue;
-    const V z = Z[h * S + fft_pad(rev[j])];
-    const T g = gfac[h];
-    out[fbase + (size_t)j * nlat + pair] = (GT)(z.x * g);
-    const int south = nlat - 1 - pair;
-    if (south != pair) out[fbase + (size_t)j * nlat + south] = (GT)(z.y * g);
+  constexpr int L = Vec16<T>::n;
+  const bool vec = (H % L == 0) && (hv == H) && (nlat % L == 0);
+  for (int q = threadIdx.x; q < N; q += blockDim.x) {
+    const int j = rinv[q];
+    T vn[H], vs[H];
+#pragma unroll
+    for (int h = 0; h < H; ++h) {
+      const V z = Z[h * S + fft_pad(q)];
+      vn[h] = z.x * gfac[h];
+      vs[h] = z.y * gfac[h];
+    }
+    T* row = out + fbase + (size_t)j * nlat;
+    if constexpr (H % L == 0) {
+      if (vec) {
+        T rs[H];
+#pragma unroll
+        for (int h = 0; h < H; ++h) rs[h] = vs[H - 1 - h];
+        store_seg<T, H>(row + p0, vn);
+        store_seg<T, H>(row + (nlat - p0 - H), rs);
+        continue;
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < H; ++h) {
+      if (h >= hv) continue;
+      const int pair = p0 + h;
+      row[pair] = vn[h];
+      const int south = nlat - 1 - pair;
+      if (south != pair) row[south] = vs[h];
+    }
   }
 }
 
-template <typename T, typename GT, bool GENERIC>
-__global__ void __launch_bounds__(256) fft_ana_kernel(PlanDev P, FFTDesc fd, const int* __restrict__ rev,
-                                                      const GT* __restrict__ in0,
-                                                       const GT* __restrict__ in1, int ncomp,
-                                                       typename V2<T>::type* __restrict__ W, int mlim, int H,
-                                                       double wscale, int use_w, int spow,
-                                                       const typename V2<T>::type* __restrict__ tw) {
+template <typename T, int H, bool GENERIC>
+__global__ void __launch_bounds__(512) fft_ana_kernel(PlanDev P, FFTDesc fd, const int* __restrict__ rev,
+                                                      const T* __restrict__ in0, const T* __restrict__ in1, int ncomp,
+                                                      typename V2<T>::type* __restrict__ W, int mlim, double wscale,
+                                                      int use_w, int spow, const typename V2<T>::type* __restrict__ tw) {
   using V = typename V2<T>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int N = fd.n, S = fft_row_stride(N);
   V* Z = reinterpret_cast<V*>(smem_raw);
   V* scratch = Z + H * S;
-  T* wfac = reinterpret_cast<T*>(Z + (fd.direct ? 2 : 1) * H * S);
+  T* wfac = reinterpret_cast<T*>(Z + ((GENERIC && fd.direct) ? 2 : 1) * H * S);
   const int p0 = blockIdx.x * H;
   const int k = blockIdx.y;
   const int npair = P.npair, nlat = P.nlat;
-  const GT* in = (ncomp == 2 && (k & 1)) ? in1 : in0;
+  const int hv = min(H, npair - p0);
+  const T* in = (ncomp == 2 && (k & 1)) ? in1 : in0;
   const size_t kk = (ncomp == 2) ? (size_t)(k >> 1) : (size_t)k;
   const size_t fbase = kk * (size_t)nlat * N;
-  for (int h = threadIdx.x; h < H; h += blockDim.x)
-    wfac[h] = (p0 + h < npair) ? pair_factor<T>(P, p0 + h, wscale, use_w, spow) : (T)0;
-  constexpr int U = 8;
-  for (int base0 = threadIdx.x; base0 < N * H; base0 += blockDim.x * U) {
-    T vn[U], vs[U];
+  for (int h = threadIdx.x; h < H; h += blockDim.x) wfac[h] = (h < hv) ? pair_factor<T>(P, p0 + h, wscale, use_w, spow) : (T)0;
+  constexpr int L = Vec16<T>::n;
+  const bool vec = (H % L == 0) && (hv == H) && (nlat % L == 0);
+  for (int j = threadIdx.x; j < N; j += blockDim.x) {
+    const T* row = in + fbase + (size_t)j * nlat;
+    T vn[H], vs[H];
+    bool done = false;
+    if constexpr (H % L == 0) {
+      if (vec) {
+        T rs[H];
+        load_seg<T, H>(row + p0, vn);
+        load_seg<T, H>(row + (nlat - p0 - H), rs);
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int idx = base0 + u * blockDim.x;
-      vn[u] = vs[u] = (T)0;
-      if (idx < N * H) {
-        const int j = idx / H, h = idx - j * H, pair = p0 + h;
-        if (pair < npair) {
-          vn[u] = (T)in[fbase + (size_t)j * nlat + pair];
+        for (int h = 0; h < H; ++h) vs[h] = rs[H - 1 - h];
+        done = true;
+      }
+    }
+    if (!done) {
+#pragma unroll
+      for (int h = 0; h < H; ++h) {
+        vn[h] = vs[h] = (T)0;
+        if (h < hv) {
+          const int pair = p0 + h;
+          vn[h] = row[pair];
           const int south = nlat - 1 - pair;
-          if (south != pair) vs[u] = (T)in[fbase + (size_t)j * nlat + south];
+          if (south != pair) vs[h] = row[south];
         }
       }
     }
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int idx = base0 + u * blockDim.x;
-      if (idx < N * H) {
-        const int j = idx / H, h = idx - j * H;
-        V z;
-        z.x = vn[u];
-        z.y = vs[u];
-        Z[h * S + fft_pad(j)] = z;
-      }
+    for (int h = 0; h < H; ++h) {
+      V z;
+      z.x = vn[h];
+      z.y = vs[h];
+      Z[h * S + fft_pad(j)] = z;
     }
   }
   __syncthreads();
   fft_rows<T, V, GENERIC>(Z, scratch, H, S, fd, tw, -1);
   const int nmu = mlim / P.mres + 1;
   for (int idx = threadIdx.x; idx < nmu * H; idx += blockDim.x) {
-    const int im = idx / H, h = idx - im * H, pair = p0 + h;
-    if (pair >= npair) continue;
+    const int im = idx / H, h = idx - im * H;
+    if (h >= hv) continue;
     const int m = im * P.mres;
     const V Zm = Z[h * S + fft_pad(rev[m])];
     V Zc = Z[h * S + fft_pad(rev[m == 0 ? 0 : N - m])];
@@ -160,71 +225,91 @@ __global__ void __launch_bounds__(256) fft_ana_kernel(PlanDev P, FFTDesc fd, con
     XN.x = sum.x * (T)0.5; XN.y = sum.y * (T)0.5;
     XS.x = d.y * (T)0.5;   XS.y = -d.x * (T)0.5;
     const T wt = wfac[h];
-    const size_t base = ((size_t)k * P.nm + im) * 2 * npair + pair;
+    const size_t base = ((size_t)k * P.nm + im) * 2 * npair + p0 + h;
     W[base] = cscale(cadd(XN, XS), wt);
     W[base + npair] = cscale(csub(XN, XS), wt);
   }
 }
 
-static int fft_config(const FFTDesc& fd, size_t celem, int npair, int* H, int* threads, size_t* smem) {
-  const int N = fd.n;
-  const int S = fft_row_stride(N);
-  // enough latitude pairs for 32-byte (FP64) / 32-byte (FP32) row segments, up to 16
-  int h = std::min(16, std::max(celem == 16 ? 2 : 4, 4096 / std::max(N, 1)));
-  h = std::max(1, std::min(h, npair));
-  auto need = [&](int hh) { return (size_t)hh * S * celem * (fd.direct ? 2 : 1) + (size_t)hh * 8 + 16; };
-  while (h > 1 && need(h) > 100 * 1024) --h;
-  if (need(h) > 220 * 1024) return set_error(SHTB_ERR_UNSUPPORTED, "nlon too large for the shared-memory FFT");
-  *H = h;
-  *threads = 256;
-  *smem = need(h);
+// H latitude pairs per CTA: the largest power of two <= 16 whose shared-memory
+// footprint stays within ~200 KB (one CTA of 512 threads per SM).
+static int fft_pick_h(const FFTDesc& fd, size_t celem, int npair) {
+  const size_t S = (size_t)fft_row_stride(fd.n);
+  int h = 16;
+  while (h > 1 && (size_t)h * S * celem * (fd.direct ? 2 : 1) + 16 * 8 > 200 * 1024) h >>= 1;
+  while (h > 1 && h / 2 >= npair) h >>= 1;
+  return h;
+}
+
+static size_t fft_smem(const FFTDesc& fd, size_t celem, int h) {
+  return (size_t)h * fft_row_stride(fd.n) * celem * (fd.direct ? 2 : 1) + (size_t)h * 8 + 16;
+}
+
+static bool fft_generic(const shtb_plan* p) {
+  bool g = p->fft.direct;
+  for (int i = 0; i < p->fft.nrad; ++i) {
+    const int r = p->fft.rad[i];
+    g = g || !(r == 2 || r == 3 || r == 4 || r == 5 || r == 8);
+  }
+  return g;
+}
+
+template <typename T, int H>
+static int launch_syn_h(const shtb_plan* p, const void* W, T* out0, T* out1, int ncomp, int nfw, int mlim,
+                        double gscale, int use_w, int spow, cudaStream_t st) {
+  using V = typename V2<T>::type;
+  const size_t smem = fft_smem(p->fft, sizeof(V), H);
+  if (smem > 227 * 1024) return set_error(SHTB_ERR_UNSUPPORTED, "nlon too large for the shared-memory FFT");
+  auto kern = fft_generic(p) ? fft_syn_kernel<T, H, true> : fft_syn_kernel<T, H, false>;
+  SHTB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "fft smem attr");
+  dim3 grid((p->npair + H - 1) / H, nfw);
+  const V* tw = std::is_same<T, double>::value ? (const V*)p->d_tw64 : (const V*)p->d_tw32;
+  prof_begin(st);
+  kern<<<grid, 512, smem, st>>>(p->dev, p->fft, p->d_rinv, (const V*)W, out0, out1, ncomp, mlim, gscale, use_w, spow, tw);
+  SHTB_LAUNCHED("fft synthesis kernel");
+  return SHTB_OK;
+}
+
+template <typename T, int H>
+static int launch_ana_h(const shtb_plan* p, const T* in0, const T* in1, int ncomp, void* W, int nfw, int mlim,
+                        double wscale, int use_w, int spow, cudaStream_t st) {
+  using V = typename V2<T>::type;
+  const size_t smem = fft_smem(p->fft, sizeof(V), H);
+  if (smem > 227 * 1024) return set_error(SHTB_ERR_UNSUPPORTED, "nlon too large for the shared-memory FFT");
+  auto kern = fft_generic(p) ? fft_ana_kernel<T, H, true> : fft_ana_kernel<T, H, false>;
+  SHTB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "fft smem attr");
+  dim3 grid((p->npair + H - 1) / H, nfw);
+  const V* tw = std::is_same<T, double>::value ? (const V*)p->d_tw64 : (const V*)p->d_tw32;
+  prof_begin(st);
+  kern<<<grid, 512, smem, st>>>(p->dev, p->fft, p->d_rev, in0, in1, ncomp, (V*)W, mlim, wscale, use_w, spow, tw);
+  SHTB_LAUNCHED("fft analysis kernel");
   return SHTB_OK;
 }
 
 template <typename T, typename GT>
 int launch_fft_syn(const shtb_plan* p, const void* W, GT* out0, GT* out1, int ncomp, int nfw, int mlim,
                    double gscale, int use_w, int spow, cudaStream_t st) {
-  using V = typename V2<T>::type;
-  int H, threads;
-  size_t smem;
-  int rc = fft_config(p->fft, sizeof(V), p->npair, &H, &threads, &smem);
-  if (rc) return rc;
-  bool generic = p->fft.direct;
-  for (int i = 0; i < p->fft.nrad; ++i) {
-    const int r = p->fft.rad[i];
-    generic = generic || !(r == 2 || r == 3 || r == 4 || r == 5 || r == 8);
+  static_assert(std::is_same<T, GT>::value, "grid and compute types match");
+  switch (fft_pick_h(p->fft, sizeof(typename V2<T>::type), p->npair)) {
+    case 16: return launch_syn_h<T, 16>(p, W, out0, out1, ncomp, nfw, mlim, gscale, use_w, spow, st);
+    case 8: return launch_syn_h<T, 8>(p, W, out0, out1, ncomp, nfw, mlim, gscale, use_w, spow, st);
+    case 4: return launch_syn_h<T, 4>(p, W, out0, out1, ncomp, nfw, mlim, gscale, use_w, spow, st);
+    case 2: return launch_syn_h<T, 2>(p, W, out0, out1, ncomp, nfw, mlim, gscale, use_w, spow, st);
+    default: return launch_syn_h<T, 1>(p, W, out0, out1, ncomp, nfw, mlim, gscale, use_w, spow, st);
   }
-  auto kern = generic ? fft_syn_kernel<T, GT, true> : fft_syn_kernel<T, GT, false>;
-  SHTB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "fft smem attr");
-  dim3 grid((p->npair + H - 1) / H, nfw);
-  const V* tw = std::is_same<T, double>::value ? (const V*)p->d_tw64 : (const V*)p->d_tw32;
-  prof_begin(st);
-  kern<<<grid, threads, smem, st>>>(p->dev, p->fft, p->d_rev, (const V*)W, out0, out1, ncomp, mlim, H, gscale, use_w, spow, tw);
-  SHTB_LAUNCHED("fft synthesis kernel");
-  return SHTB_OK;
 }
 
 template <typename T, typename GT>
 int launch_fft_ana(const shtb_plan* p, const GT* in0, const GT* in1, int ncomp, void* W, int nfw, int mlim,
                    double wscale, int use_w, int spow, cudaStream_t st) {
-  using V = typename V2<T>::type;
-  int H, threads;
-  size_t smem;
-  int rc = fft_config(p->fft, sizeof(V), p->npair, &H, &threads, &smem);
-  if (rc) return rc;
-  bool generic = p->fft.direct;
-  for (int i = 0; i < p->fft.nrad; ++i) {
-    const int r = p->fft.rad[i];
-    generic = generic || !(r == 2 || r == 3 || r == 4 || r == 5 || r == 8);
+  static_assert(std::is_same<T, GT>::value, "grid and compute types match");
+  switch (fft_pick_h(p->fft, sizeof(typename V2<T>::type), p->npair)) {
+    case 16: return launch_ana_h<T, 16>(p, in0, in1, ncomp, W, nfw, mlim, wscale, use_w, spow, st);
+    case 8: return launch_ana_h<T, 8>(p, in0, in1, ncomp, W, nfw, mlim, wscale, use_w, spow, st);
+    case 4: return launch_ana_h<T, 4>(p, in0, in1, ncomp, W, nfw, mlim, wscale, use_w, spow, st);
+    case 2: return launch_ana_h<T, 2>(p, in0, in1, ncomp, W, nfw, mlim, wscale, use_w, spow, st);
+    default: return launch_ana_h<T, 1>(p, in0, in1, ncomp, W, nfw, mlim, wscale, use_w, spow, st);
   }
-  auto kern = generic ? fft_ana_kernel<T, GT, true> : fft_ana_kernel<T, GT, false>;
-  SHTB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "fft smem attr");
-  dim3 grid((p->npair + H - 1) / H, nfw);
-  const V* tw = std::is_same<T, double>::value ? (const V*)p->d_tw64 : (const V*)p->d_tw32;
-  prof_begin(st);
-  kern<<<grid, threads, smem, st>>>(p->dev, p->fft, p->d_rev, in0, in1, ncomp, (V*)W, mlim, H, wscale, use_w, spow, tw);
-  SHTB_LAUNCHED("fft analysis kernel");
-  return SHTB_OK;
 }
 
 template int launch_fft_syn<double, double>(const shtb_plan*, const void*, double*, double*, int, int, int, double, int, int, cudaStream_t);

@@ -86,6 +86,7 @@ struct shtb_plan {
   const double2* d_tw64 = nullptr;        // exp(-2 pi i t / nlon)
   const float2* d_tw32 = nullptr;
   const int* d_rev = nullptr;             // FFT output position of bin k (digit reversal)
+  const int* d_rinv = nullptr;            // natural index stored at FFT position q (inverse of d_rev)
   const double* d_dcoef = nullptr;        // packed d(l,m) = sqrt((l^2-m^2)/(4l^2-1)), l in [m, lrec]
   std::vector<int2> htiles;
   int* d_err = nullptr;                   // device status word (bounded waits that gave up)

@@ -307,6 +307,8 @@ extern "C" int shtb_plan_create(shtb_plan** out, int lmax, int mmax, int mres, i
     }
     rev[k] = pos;
   }
+  std::vector<int> rinv(nlon);
+  for (int k = 0; k < nlon; ++k) rinv[rev[k]] = k;
   std::vector<float2> tw32(nlon);
   for (int t = 0; t < nlon; ++t) tw32[t] = make_float2((float)tw[t].x, (float)tw[t].y);
 
@@ -319,7 +321,7 @@ extern "C" int shtb_plan_create(shtb_plan** out, int lmax, int mmax, int mres, i
   const size_t o_ck = take((size_t)ntiles * npair * 16), o_tiles = take((size_t)ntiles * 8);
   const size_t o_scale = coeff_scale ? take((size_t)(lmax + 1) * (mmax + 1) * 8) : 0;
   const size_t o_tw = take((size_t)nlon * 16), o_tw32 = take((size_t)nlon * 8);
-  const size_t o_seed = take((mmax + 2) * 8), o_tb = take(nm * 4), o_rev = take((size_t)nlon * 4);
+  const size_t o_seed = take((mmax + 2) * 8), o_tb = take(nm * 4), o_rev = take((size_t)nlon * 4), o_rinv = take((size_t)nlon * 4);
   const size_t o_err = take(16);
   p->dbytes = o;
   cudaError_t ce = cudaMalloc(&p->dmem, o);
@@ -346,6 +348,7 @@ extern "C" int shtb_plan_create(shtb_plan** out, int lmax, int mmax, int mres, i
   if (ce == cudaSuccess) ce = up(o_seed, seedfac.data(), (mmax + 2) * 8);
   if (ce == cudaSuccess) ce = up(o_tb, tile_base.data(), nm * 4);
   if (ce == cudaSuccess) ce = up(o_rev, rev.data(), (size_t)nlon * 4);
+  if (ce == cudaSuccess) ce = up(o_rinv, rinv.data(), (size_t)nlon * 4);
   if (ce != cudaSuccess) {
     cudaFree(p->dmem);
     delete p;
@@ -370,6 +373,7 @@ extern "C" int shtb_plan_create(shtb_plan** out, int lmax, int mmax, int mres, i
   p->d_tw32 = (const float2*)(D + o_tw32);
   p->d_dcoef = (const double*)(D + o_d);
   p->d_rev = (const int*)(D + o_rev);
+  p->d_rinv = (const int*)(D + o_rinv);
   p->d_err = (int*)(D + o_err);
   if (ce == cudaSuccess) ce = cudaMemset(D + o_err, 0, 16);
 
