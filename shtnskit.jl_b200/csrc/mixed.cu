@@ -12,16 +12,17 @@
 // mixed_table_kernel from the FP64 recurrence (extended-range seeds and FP64
 // recurrence coefficients), so every P value is the FP64 result rounded once.
 //
-// CTA organisation (544 threads, one parity class per CTA): warps 0-7 are two
-// producer groups of 128 threads that load operands, split them into hi/lo and
-// store K-major tiles (no swizzle) into an 8-stage shared-memory ring,
-// alternating stages; warp 8 allocates TMEM and one of its threads issues the
-// MMAs (tcgen05.commit releases each stage). The tensor core accumulates only
-// kChunk K-steps into one of two TMEM buffers (hi*hi and the small cross terms
-// in separate accumulators); warps 9-16 drain each finished chunk with
-// tcgen05.ld into round-to-nearest FP32 register sums. Long accumulation chains
-// inside the tensor core round toward zero and would bias sums of many terms;
-// short chunks keep that bias below 1e-6 relative at any lmax.
+// CTA organisation (544 threads, one parity class per CTA): warps 0-3 copy
+// operands with cp.async straight into K-major tiles (no swizzle) of an 8-stage
+// shared-memory ring, up to 8 K-steps ahead; warps 4-7 round each landed stage in
+// place to TF32 hi and write the lo remainders; warp 8 allocates TMEM and one of its threads issues the
+// MMAs (tcgen05.commit releases each stage). The tensor core accumulates the
+// hi*hi products of only kChunk K-steps into one of two TMEM buffers; warps 9-16
+// drain each finished chunk with tcgen05.ld into round-to-nearest FP32 register
+// sums. Long accumulation chains inside the tensor core round toward zero and
+// would bias sums of many terms; short chunks keep that bias below 1e-6 relative
+// at any lmax. The cross terms hi*lo + lo*hi are ~2^-11 of the result, so they
+// accumulate over the whole tile in a third TMEM buffer and are drained once.
 // Every mbarrier wait is bounded (2 s of %globaltimer); a timeout sets the
 // plan's error word and the CTA drains and exits.
 #include <climits>
@@ -98,12 +99,6 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
   return true;
 }
 
-__device__ __forceinline__ float tf32_rn(float x) {
-  unsigned u;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(u) : "f"(x));
-  return __uint_as_float(u);
-}
-
 // K-major, no-swizzle tile: 8-row core matrices of 16-byte rows; the two 16-byte
 // K halves of a core-matrix pair are 128 bytes apart (LBO), 8-row groups 256 bytes (SBO).
 __device__ __forceinline__ int tile_off(int r, int khalf) { return (r >> 3) * 256 + khalf * 128 + (r & 7) * 16; }
@@ -135,29 +130,71 @@ __device__ __forceinline__ void mma_commit(unsigned long long* bar) {
                : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld16(unsigned taddr, float* v) {
+// NC consecutive TMEM columns of this thread's lane (32x32b shape), completed by the
+// wait::ld in the same asm statement so no use of the registers can precede it.
+template <int NC>
+__device__ __forceinline__ void tmem_ld(unsigned taddr, float* v);
+template <>
+__device__ __forceinline__ void tmem_ld<8>(unsigned taddr, float* v) {
+  unsigned r[8];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+      : "r"(taddr)
+      : "memory");
+#pragma unroll
+  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
+template <>
+__device__ __forceinline__ void tmem_ld<16>(unsigned taddr, float* v) {
   unsigned r[16];
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr)
+      : "memory");
 #pragma unroll
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
+template <>
+__device__ __forceinline__ void tmem_ld<32>(unsigned taddr, float* v) {
+  unsigned r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr)
+      : "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
 
-// Split 8 consecutive K values of one row into hi/lo tiles.
-__device__ __forceinline__ void store_split8(unsigned char* hi, unsigned char* lo, int row, const float* v) {
-  float4 h0, h1, l0, l1;
-  h0.x = tf32_rn(v[0]); h0.y = tf32_rn(v[1]); h0.z = tf32_rn(v[2]); h0.w = tf32_rn(v[3]);
-  h1.x = tf32_rn(v[4]); h1.y = tf32_rn(v[5]); h1.z = tf32_rn(v[6]); h1.w = tf32_rn(v[7]);
-  l0.x = tf32_rn(v[0] - h0.x); l0.y = tf32_rn(v[1] - h0.y); l0.z = tf32_rn(v[2] - h0.z); l0.w = tf32_rn(v[3] - h0.w);
-  l1.x = tf32_rn(v[4] - h1.x); l1.y = tf32_rn(v[5] - h1.y); l1.z = tf32_rn(v[6] - h1.z); l1.w = tf32_rn(v[7] - h1.w);
-  *reinterpret_cast<float4*>(hi + tile_off(row, 0)) = h0;
-  *reinterpret_cast<float4*>(hi + tile_off(row, 1)) = h1;
-  *reinterpret_cast<float4*>(lo + tile_off(row, 0)) = l0;
-  *reinterpret_cast<float4*>(lo + tile_off(row, 1)) = l1;
+__device__ __forceinline__ void cp_async4(void* dst, const void* src, bool ok) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(smem_u32(dst)), "l"(src), "r"(ok ? 4 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool ok) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src), "r"(ok ? 16 : 0)
+               : "memory");
+}
+// Arrive on bar once every cp.async this thread issued so far has landed (the barrier's
+// expected count includes this arrival).
+__device__ __forceinline__ void cp_async_arrive_noinc(unsigned long long* bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Round to the nearest TF32 value, ties away from zero: add half a TF32 ulp to the
+// magnitude bits and clear the 13 low mantissa bits (finite inputs).
+__device__ __forceinline__ float tf32_round(float x) {
+  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
+}
+// x = hi + lo with hi = tf32(x) and lo = tf32(x - hi) (x - hi is exact in FP32).
+__device__ __forceinline__ void split4(const float4& x, float4& h, float4& l) {
+  h.x = tf32_round(x.x); h.y = tf32_round(x.y); h.z = tf32_round(x.z); h.w = tf32_round(x.w);
+  l.x = tf32_round(x.x - h.x); l.y = tf32_round(x.y - h.y); l.z = tf32_round(x.z - h.z); l.w = tf32_round(x.w - h.w);
 }
 
 __device__ __forceinline__ float coef_factor(const Args& a, int l, int m) {
@@ -175,16 +212,8 @@ struct Smem {
   // per stage: A_hi, A_lo, B_hi, B_lo (one parity class per CTA)
   static constexpr int kStage = 2 * kTileBytesA + 2 * kTileB;
   static constexpr int kBar = kStages * kStage;
-  static constexpr int kBytes = kBar + (2 * kStages + 4) * 8 + 16;
+  static constexpr int kBytes = kBar + (3 * kStages + 4) * 8 + 16;
 };
-
-__device__ __forceinline__ void store_split4(unsigned char* hi, unsigned char* lo, int row, int khalf, const float* v) {
-  float4 h, l;
-  h.x = tf32_rn(v[0]); h.y = tf32_rn(v[1]); h.z = tf32_rn(v[2]); h.w = tf32_rn(v[3]);
-  l.x = tf32_rn(v[0] - h.x); l.y = tf32_rn(v[1] - h.y); l.z = tf32_rn(v[2] - h.z); l.w = tf32_rn(v[3] - h.w);
-  *reinterpret_cast<float4*>(hi + tile_off(row, khalf)) = h;
-  *reinterpret_cast<float4*>(lo + tile_off(row, khalf)) = l;
-}
 
 // MODE 0: synthesis, MODE 1: analysis. N = columns per CTA (2 x fields).
 // blockIdx.x = 2 * tile + parity; one CTA accumulates one parity class.
@@ -194,7 +223,8 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_gemm_kernel(const __grid_co
   extern __shared__ __align__(1024) unsigned char sm[];
   unsigned long long* full = reinterpret_cast<unsigned long long*>(sm + S::kBar);
   unsigned long long* empty = full + kStages;
-  unsigned long long* accf = empty + kStages;   // [2] chunk accumulated in TMEM buffer b
+  unsigned long long* ldfull = empty + kStages;  // [kStages] loader copies of the stage landed
+  unsigned long long* accf = ldfull + kStages;  // [2] chunk accumulated in TMEM buffer b
   unsigned long long* acce = accf + 2;          // [2] TMEM buffer b drained by the promotion warps
   unsigned* tmem_slot = reinterpret_cast<unsigned*>(acce + 2);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
@@ -225,6 +255,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_gemm_kernel(const __grid_co
     for (int s = 0; s < kStages; ++s) {
       mbar_init(&full[s], 128);
       mbar_init(&empty[s], 1);
+      mbar_init(&ldfull[s], 128);
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&accf[b], 1);
@@ -242,80 +273,120 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_gemm_kernel(const __grid_co
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const unsigned tmem = *tmem_slot;
-  // TMEM: buffer b holds the hi*hi chunk sum at column 2bN and the cross terms at 2bN + N
+  // TMEM: chunk buffer b (hi*hi) at column b*N; the cross terms of the whole tile at 2N
 
   if (warp < 8) {
     // ------------------------------------------------------------- producers
-    const int g = warp >> 2, t = tid & 127;
-    const int bf = t >> 1, bh = t & 1;           // B: field bf, K half bh (4 values)
-    const bool bact = bf < N / 2;
-    float va[kK], vb[2][4];
-    auto load = [&](int ks) {
+    // Warps 0-3 (loaders) copy the operands of every K-step with cp.async straight into
+    // their K-major slots of the hi tiles of stage ks % kStages and signal completion on
+    // ldfull with cp.async.mbarrier.arrive, running up to kStages K-steps ahead. Warps 4-7
+    // (splitters) round each landed stage in place to TF32, write the remainders into the
+    // lo tiles, and release the stage to the MMA issuer. Keeping the two roles in separate
+    // threads means a splitter's proxy fence never waits for copies still in flight.
+    const int t = tid & 127;
+    const int Jc = (MODE == 0) ? J : npair;   // valid K indices of this GEMM
+    if (warp < 4) {
+      // B copies: instruction r of warp w4 covers fields 2 (8 w4 + r) + (lane >> 4); within
+      // a field the 16 lanes take K slot bk = (lane >> 1) & 7, component bc = lane & 1, so
+      // each half-warp reads one field's contiguous span.
+      const int w4 = warp & 3, bk = (lane >> 1) & 7, bc = lane & 1, bfh = lane >> 4;
+      const int fl0 = 16 * w4 + bfh;                 // field of instruction 0
+      const int nfr = min(N / 2, a.nf - kb);         // fields of this CTA
+      const int nr = (nfr > fl0) ? min(8, (nfr - fl0 + 1) / 2) : 0;   // active instructions
+      const float* b0;
+      long long fstride, kstep;
       if (MODE == 0) {
-        const int pr = p0 + t;
-#pragma unroll
-        for (int k = 0; k < kK; ++k) {
-          const int j = ks * kK + k;
-          va[k] = (j < ln) ? a.tab[(sg + j) * a.npp + pr] : 0.f;
-        }
+        b0 = reinterpret_cast<const float*>(a.cin + (long long)(kb + fl0) * a.ld_k + (long long)m * (P.lmax + 1) + m + par +
+                                            2 * bk) + bc;
+        fstride = 4 * a.ld_k;                        // two fields, in floats
+        kstep = 32;                                  // 16 complex degrees per K-step
       } else {
-        const int j = j0 + t;
-        if (j < ln) {
-          const float4* q = reinterpret_cast<const float4*>(a.tab + (sg + j) * a.npp + ks * kK);
-          const float4 x0 = q[0], x1 = q[1];
-          va[0] = x0.x; va[1] = x0.y; va[2] = x0.z; va[3] = x0.w;
-          va[4] = x1.x; va[5] = x1.y; va[6] = x1.z; va[7] = x1.w;
-        } else {
-#pragma unroll
-          for (int k = 0; k < kK; ++k) va[k] = 0.f;
-        }
+        b0 = reinterpret_cast<const float*>(a.Win + (((long long)(kb + fl0) * P.nm + im) * 2 + par) * npair + bk) + bc;
+        fstride = 8ll * P.nm * npair;
+        kstep = 16;
       }
-      const int kf = kb + bf;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) vb[0][k] = vb[1][k] = 0.f;
-      if (bact && kf < a.nf) {
+      unsigned char* bdst0 = sm + 2 * kTileBytesA + tile_off(2 * fl0 + bc, bk >> 2) + (bk & 3) * 4;
+      // A copies
+      const float* a0 = (MODE == 0) ? a.tab + sg * a.npp + p0 + t : a.tab + (sg + j0 + t) * a.npp;
+      const bool arow_ok = (MODE == 0) || (j0 + t < ln);
+      for (int ks = 0; ks < nks; ++ks) {
+        const int b = ks % kStages;
+        if (ks >= kStages && !mbar_wait(&empty[b], ((ks / kStages) - 1) & 1, abort_flag, a.err)) break;
+        unsigned char* st = sm + (size_t)b * S::kStage;
         if (MODE == 0) {
-          const float2* c = a.cin + (long long)kf * a.ld_k + (long long)m * (P.lmax + 1);
 #pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            const int l = m + 2 * (ks * kK + 4 * bh + k) + par;
-            if (l <= a.lend) {
-              float2 v = c[l];
-              const float s = coef_factor(a, l, m);
-              vb[0][k] = v.x * s;
-              vb[1][k] = v.y * s;
-            }
+          for (int k = 0; k < kK; ++k) {
+            const int j = ks * kK + k;
+            const bool ok = j < ln;
+            cp_async4(st + tile_off(t, k >> 2) + (k & 3) * 4, ok ? a0 + (long long)j * a.npp : a.tab, ok);
           }
         } else {
-          const float2* w = a.Win + (((long long)kf * P.nm + im) * 2 + par) * npair;
+          const float* src = a0 + ks * kK;
+          cp_async16(st + tile_off(t, 0), arow_ok ? src : a.tab, arow_ok);
+          cp_async16(st + tile_off(t, 1), arow_ok ? src + 4 : a.tab, arow_ok);
+        }
+        const bool kok = ks * kK + bk < Jc;
+        const float* bs = b0 + ks * kstep;
+        unsigned char* bd = bdst0 + (size_t)b * S::kStage;
 #pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            const int pr = ks * kK + 4 * bh + k;
-            if (pr < npair) {
-              const float2 v = w[pr];
-              vb[0][k] = v.x;
-              vb[1][k] = v.y;
-            }
+        for (int r = 0; r < 8; ++r) {
+          if (r < nr) {
+            const bool ok = kok && (fl0 + 2 * r < nfr);
+            // field fl0 + 2r sits 4r rows below field fl0: (r >> 1) 8-row groups, (r & 1) * 4 rows
+            cp_async4(bd + (r >> 1) * 256 + (r & 1) * 64, ok ? bs + r * fstride : a.tab, ok);
           }
         }
+        cp_async_arrive_noinc(&ldfull[b]);
       }
-    };
-    if (g < nks) load(g);
-    for (int ks = g; ks < nks; ks += 2) {
-      const int b = ks % kStages;
-      if (ks >= kStages)
-        if (!mbar_wait(&empty[b], ((ks / kStages) - 1) & 1, abort_flag, a.err)) break;
-      unsigned char* st = sm + (size_t)b * S::kStage;
-      store_split8(st, st + kTileBytesA, t, va);
-      if (bact) {
-        unsigned char* bh_ = st + 2 * kTileBytesA;
-        unsigned char* bl_ = bh_ + S::kTileB;
-        store_split4(bh_, bl_, 2 * bf, bh, vb[0]);
-        store_split4(bh_, bl_, 2 * bf + 1, bh, vb[1]);
+      cp_async_wait_all();
+    } else {
+      // Splitter thread t rounds row t of the A tile and row t of the B tile.
+      const bool brow = t < N;
+      const bool scaled = (MODE == 0) && (a.sc_mode || a.mf0 != 1.f || a.mf1 != 1.f);
+      for (int ks = 0; ks < nks; ++ks) {
+        const int b = ks % kStages;
+        if (!mbar_wait(&ldfull[b], (ks / kStages) & 1, abort_flag, a.err)) break;
+        unsigned char* st = sm + (size_t)b * S::kStage;
+        unsigned char* Ah = st;
+        unsigned char* Al = st + kTileBytesA;
+        unsigned char* Bh = st + 2 * kTileBytesA;
+        unsigned char* Bl = Bh + S::kTileB;
+        const int o0 = tile_off(t, 0), o1 = tile_off(t, 1);
+        const float4 x0 = *reinterpret_cast<const float4*>(Ah + o0);
+        const float4 x1 = *reinterpret_cast<const float4*>(Ah + o1);
+        float4 y0 = make_float4(0.f, 0.f, 0.f, 0.f), y1 = y0;
+        if (brow) {
+          y0 = *reinterpret_cast<const float4*>(Bh + o0);
+          y1 = *reinterpret_cast<const float4*>(Bh + o1);
+          if (scaled) {
+            float sc[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+              const int l = m + par + 2 * (ks * kK + k);
+              sc[k] = (l <= a.lend) ? coef_factor(a, l, m) : 0.f;   // beyond lend the copies zero-filled
+            }
+            y0.x *= sc[0]; y0.y *= sc[1]; y0.z *= sc[2]; y0.w *= sc[3];
+            y1.x *= sc[4]; y1.y *= sc[5]; y1.z *= sc[6]; y1.w *= sc[7];
+          }
+        }
+        float4 h, l;
+        split4(x0, h, l);
+        *reinterpret_cast<float4*>(Ah + o0) = h;
+        *reinterpret_cast<float4*>(Al + o0) = l;
+        split4(x1, h, l);
+        *reinterpret_cast<float4*>(Ah + o1) = h;
+        *reinterpret_cast<float4*>(Al + o1) = l;
+        if (brow) {
+          split4(y0, h, l);
+          *reinterpret_cast<float4*>(Bh + o0) = h;
+          *reinterpret_cast<float4*>(Bl + o0) = l;
+          split4(y1, h, l);
+          *reinterpret_cast<float4*>(Bh + o1) = h;
+          *reinterpret_cast<float4*>(Bl + o1) = l;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_arrive(&full[b]);
       }
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      mbar_arrive(&full[b]);
-      if (ks + 2 < nks) load(ks + 2);
     }
   } else if (warp == 8) {
     // ------------------------------------------------------------- MMA issuer
@@ -326,7 +397,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_gemm_kernel(const __grid_co
         const int bb = c & 1;
         if (c >= 2 && !mbar_wait(&acce[bb], ((c >> 1) - 1) & 1, abort_flag, a.err)) break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const unsigned dH = tmem + 2 * bb * N, dX = dH + N;
+        const unsigned dH = tmem + bb * N, dX = tmem + 2 * N;
         const int k1 = min(nks, (c + 1) * kChunk);
         for (int ks = c * kChunk; ks < k1; ++ks) {
           const int b = ks % kStages;
@@ -340,7 +411,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_gemm_kernel(const __grid_co
           const unsigned long long bh_ = sdesc(st + 2 * kTileBytesA), bl_ = sdesc(st + 2 * kTileBytesA + S::kTileB);
           const unsigned acc = (ks == c * kChunk) ? 0u : 1u;
           mma_tf32(dH, ah, bh_, idesc, acc);
-          mma_tf32(dX, ah, bl_, idesc, acc);
+          mma_tf32(dX, ah, bl_, idesc, ks == 0 ? 0u : 1u);
           mma_tf32(dX, al, bh_, idesc, 1u);
           mma_commit(&empty[b]);
         }
@@ -353,6 +424,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_gemm_kernel(const __grid_co
     const int h = (warp - 9) >> 2;                 // column half
     const int row = 32 * q + lane;
     const unsigned lane_base = (unsigned)(32 * q) << 16;
+    constexpr int kLd = (N / 2 < 16) ? N / 2 : 16;   // columns per TMEM load
     float acc[N / 2];
 #pragma unroll
     for (int i = 0; i < N / 2; ++i) acc[i] = 0.f;
@@ -362,18 +434,28 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_gemm_kernel(const __grid_co
       if (ok) ok = mbar_wait(&accf[bb], (c >> 1) & 1, abort_flag, a.err);
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       __syncwarp();
-      const unsigned dH = tmem + lane_base + 2 * bb * N + h * (N / 2), dX = dH + N;
+      const unsigned dH = tmem + lane_base + bb * N + h * (N / 2);
 #pragma unroll
-      for (int i = 0; i < N / 2; i += 16) {
-        float vh[16], vx[16];
-        tmem_ld16(dH + i, vh);
-        tmem_ld16(dX + i, vx);
+      for (int i = 0; i < N / 2; i += kLd) {
+        float v[kLd];
+        tmem_ld<kLd>(dH + i, v);
 #pragma unroll
-        for (int u = 0; u < 16; ++u) acc[i + u] += vh[u] + vx[u];
+        for (int u = 0; u < kLd; ++u) acc[i + u] += v[u];
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       mbar_arrive(&acce[bb]);
       if (!ok) break;
+    }
+    if (ok && nch > 0) {
+      // cross terms, accumulated over the whole tile (the last chunk's commit covers them)
+      const unsigned dX = tmem + lane_base + 2 * N + h * (N / 2);
+#pragma unroll
+      for (int i = 0; i < N / 2; i += kLd) {
+        float v[kLd];
+        tmem_ld<kLd>(dX + i, v);
+#pragma unroll
+        for (int u = 0; u < kLd; ++u) acc[i + u] += v[u];
+      }
     }
     if (ok) {
 #pragma unroll
@@ -389,6 +471,18 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_gemm_kernel(const __grid_co
             const float s = coef_factor(a, l, m);
             a.cout[(long long)kf * a.ld_k + (long long)m * (P.lmax + 1) + l] = make_float2(acc[2 * qq] * s, acc[2 * qq + 1] * s);
           }
+        }
+      }
+      if (MODE == 1 && j0 == 0) {
+        // The first tile of each order also clears that order's degrees l < m and
+        // lcap < l <= lmax; the two parity CTAs take half of the fields each.
+        const int pt = tid - 9 * 32;
+        const int nfl = min(N / 2, a.nf - kb), hf = (nfl + 1) / 2;
+        const int f0 = par ? hf : 0, f1 = par ? nfl : hf;
+        const int ntail = P.lmax - a.lcap, per = m + ntail;
+        for (int fi = f0; fi < f1; ++fi) {
+          float2* col = a.cout + (long long)(kb + fi) * a.ld_k + (long long)m * (P.lmax + 1);
+          for (int r = pt; r < per; r += 256) col[r < m ? r : a.lcap + 1 + (r - m)] = make_float2(0.f, 0.f);
         }
       }
     }
@@ -495,12 +589,13 @@ static int dispatch_gemm(const shtb_plan* p, const Args& a, int nf, dim3 grid_xy
   return launch_gemm<MODE, 16>(p, a, g, st);
 }
 
-__global__ void zero_outside_kernel32(PlanDev P, float2* __restrict__ a, long long ld_k, int mlim, int lcap) {
-  const int l = blockIdx.x * blockDim.x + threadIdx.x;
-  const int m = blockIdx.y, k = blockIdx.z;
-  if (l > P.lmax) return;
-  if ((m % P.mres) != 0 || m > mlim || l < m || l > lcap)
-    a[(long long)k * ld_k + (long long)m * (P.lmax + 1) + l] = make_float2(0.f, 0.f);
+// Clears whole order columns the analysis GEMM does not visit (m not a multiple of
+// mres, or m > min(mmax, lcap)); one block per (m, field).
+__global__ void zero_columns_kernel32(PlanDev P, float2* __restrict__ a, long long ld_k, int mlim) {
+  const int m = blockIdx.x, k = blockIdx.y;
+  if ((m % P.mres) == 0 && m <= mlim) return;
+  float2* col = a + (long long)k * ld_k + (long long)m * (P.lmax + 1);
+  for (int l = threadIdx.x; l <= P.lmax; l += blockDim.x) col[l] = make_float2(0.f, 0.f);
 }
 
 static Args base_args(const shtb_plan* p) {
@@ -566,10 +661,12 @@ int mixed_analysis(const shtb_plan* p, const void* f, void* alm, int nf, int ltr
   a.tiles = p->d_mx_tiles;
   dim3 g(2 * (unsigned)tl.size(), 1);
   if ((rc = dispatch_gemm<1>(p, a, nf, g, st))) return rc;
-  dim3 zg((p->lmax + 1 + 127) / 128, p->mmax + 1, nf);
-  prof_begin(st);
-  zero_outside_kernel32<<<zg, 128, 0, st>>>(p->dev, (float2*)alm, a.ld_k, mlim, ltr);
-  SHTB_LAUNCHED("zero fill kernel");
+  if (p->mres > 1 || mlim < p->mmax) {
+    dim3 zg(p->mmax + 1, nf);
+    prof_begin(st);
+    zero_columns_kernel32<<<zg, 256, 0, st>>>(p->dev, (float2*)alm, a.ld_k, mlim);
+    SHTB_LAUNCHED("zero fill kernel");
+  }
   return SHTB_OK;
 }
 
