@@ -61,7 +61,8 @@ template <typename T, int H, bool GENERIC>
 __global__ void __launch_bounds__(512) fft_syn_kernel(PlanDev P, FFTDesc fd, const int* __restrict__ rinv,
                                                       const typename V2<T>::type* __restrict__ W, T* __restrict__ out0,
                                                       T* __restrict__ out1, int ncomp, int mlim, double gscale,
-                                                      int use_w, int spow, const typename V2<T>::type* __restrict__ tw) {
+                                                      int use_w, int spow, const typename V2<T>::type* __restrict__ tw,
+                                                      const typename V2<T>::type* __restrict__ twp) {
   using V = typename V2<T>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int N = fd.n, S = fft_row_stride(N);
@@ -72,10 +73,19 @@ __global__ void __launch_bounds__(512) fft_syn_kernel(PlanDev P, FFTDesc fd, con
   const int k = blockIdx.y;
   const int npair = P.npair, nlat = P.nlat;
   const int hv = min(H, npair - p0);
-  for (int idx = threadIdx.x; idx < H * S; idx += blockDim.x) {
-    V z;
-    z.x = 0; z.y = 0;
-    Z[idx] = z;
+  // Bins the order loop below does not write (|m| > mlim, or m off the mres lattice)
+  // must be zero; with mres == 1 those are the bins mlim < q < N - mlim.
+  {
+    const int zlo = (P.mres == 1) ? mlim + 1 : 0, zhi = (P.mres == 1) ? N - mlim : N;
+    const int zn = zhi - zlo;
+    if (zn > 0) {
+      V z;
+      z.x = 0; z.y = 0;
+      for (int idx = threadIdx.x; idx < H * zn; idx += blockDim.x) {
+        const int h = idx / zn, q = idx - h * zn;
+        Z[h * S + fft_pad(zlo + q)] = z;
+      }
+    }
   }
   for (int h = threadIdx.x; h < H; h += blockDim.x) gfac[h] = (h < hv) ? pair_factor<T>(P, p0 + h, gscale, use_w, spow) : (T)0;
   __syncthreads();
@@ -118,39 +128,50 @@ __global__ void __launch_bounds__(512) fft_syn_kernel(PlanDev P, FFTDesc fd, con
     }
   }
   __syncthreads();
-  fft_rows<T, V, GENERIC>(Z, scratch, H, S, fd, tw, +1);
+  fft_rows<T, V, GENERIC>(Z, scratch, H, S, fd, tw, twp, +1);
   T* out = (ncomp == 2 && (k & 1)) ? out1 : out0;
   const size_t kk = (ncomp == 2) ? (size_t)(k >> 1) : (size_t)k;
   const size_t fbase = kk * (size_t)nlat * N;
   constexpr int L = Vec16<T>::n;
   const bool vec = (H % L == 0) && (hv == H) && (nlat % L == 0);
-  for (int q = threadIdx.x; q < N; q += blockDim.x) {
-    const int j = rinv[q];
-    T vn[H], vs[H];
+  constexpr int QU = 4;   // longitudes per thread per round; their rinv entries load together
+  for (int q0 = threadIdx.x; q0 < N; q0 += QU * blockDim.x) {
+    int jq[QU];
 #pragma unroll
-    for (int h = 0; h < H; ++h) {
-      const V z = Z[h * S + fft_pad(q)];
-      vn[h] = z.x * gfac[h];
-      vs[h] = z.y * gfac[h];
+    for (int u = 0; u < QU; ++u) {
+      const int q = q0 + u * blockDim.x;
+      jq[u] = (q < N) ? rinv[q] : 0;
     }
-    T* row = out + fbase + (size_t)j * nlat;
-    if constexpr (H % L == 0) {
-      if (vec) {
-        T rs[H];
 #pragma unroll
-        for (int h = 0; h < H; ++h) rs[h] = vs[H - 1 - h];
-        store_seg<T, H>(row + p0, vn);
-        store_seg<T, H>(row + (nlat - p0 - H), rs);
-        continue;
+    for (int u = 0; u < QU; ++u) {
+      const int q = q0 + u * blockDim.x;
+      if (q >= N) break;
+      T vn[H], vs[H];
+#pragma unroll
+      for (int h = 0; h < H; ++h) {
+        const V z = Z[h * S + fft_pad(q)];
+        vn[h] = z.x * gfac[h];
+        vs[h] = z.y * gfac[h];
       }
-    }
+      T* row = out + fbase + (size_t)jq[u] * nlat;
+      if constexpr (H % L == 0) {
+        if (vec) {
+          T rs[H];
 #pragma unroll
-    for (int h = 0; h < H; ++h) {
-      if (h >= hv) continue;
-      const int pair = p0 + h;
-      row[pair] = vn[h];
-      const int south = nlat - 1 - pair;
-      if (south != pair) row[south] = vs[h];
+          for (int h = 0; h < H; ++h) rs[h] = vs[H - 1 - h];
+          store_seg<T, H>(row + p0, vn);
+          store_seg<T, H>(row + (nlat - p0 - H), rs);
+          continue;
+        }
+      }
+#pragma unroll
+      for (int h = 0; h < H; ++h) {
+        if (h >= hv) continue;
+        const int pair = p0 + h;
+        row[pair] = vn[h];
+        const int south = nlat - 1 - pair;
+        if (south != pair) row[south] = vs[h];
+      }
     }
   }
 }
@@ -159,7 +180,8 @@ template <typename T, int H, bool GENERIC>
 __global__ void __launch_bounds__(512) fft_ana_kernel(PlanDev P, FFTDesc fd, const int* __restrict__ rev,
                                                       const T* __restrict__ in0, const T* __restrict__ in1, int ncomp,
                                                       typename V2<T>::type* __restrict__ W, int mlim, double wscale,
-                                                      int use_w, int spow, const typename V2<T>::type* __restrict__ tw) {
+                                                      int use_w, int spow, const typename V2<T>::type* __restrict__ tw,
+                                                      const typename V2<T>::type* __restrict__ twp) {
   using V = typename V2<T>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int N = fd.n, S = fft_row_stride(N);
@@ -211,7 +233,7 @@ __global__ void __launch_bounds__(512) fft_ana_kernel(PlanDev P, FFTDesc fd, con
     }
   }
   __syncthreads();
-  fft_rows<T, V, GENERIC>(Z, scratch, H, S, fd, tw, -1);
+  fft_rows<T, V, GENERIC>(Z, scratch, H, S, fd, tw, twp, -1);
   const int nmu = mlim / P.mres + 1;
   for (int idx = threadIdx.x; idx < nmu * H; idx += blockDim.x) {
     const int im = idx / H, h = idx - im * H;
@@ -232,7 +254,9 @@ __global__ void __launch_bounds__(512) fft_ana_kernel(PlanDev P, FFTDesc fd, con
 }
 
 // H latitude pairs per CTA: the largest power of two <= 16 whose shared-memory
-// footprint stays within ~200 KB (one CTA of 512 threads per SM).
+// footprint stays within ~200 KB (one CTA of 512 threads per SM). Two CTAs of 256
+// threads with half the pairs measured slower on B200: their grid segments shrink to
+// 16 bytes and each FFT has half the threads.
 static int fft_pick_h(const FFTDesc& fd, size_t celem, int npair) {
   const size_t S = (size_t)fft_row_stride(fd.n);
   int h = 16;
@@ -264,8 +288,10 @@ static int launch_syn_h(const shtb_plan* p, const void* W, T* out0, T* out1, int
   SHTB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "fft smem attr");
   dim3 grid((p->npair + H - 1) / H, nfw);
   const V* tw = std::is_same<T, double>::value ? (const V*)p->d_tw64 : (const V*)p->d_tw32;
+  const V* twp = std::is_same<T, double>::value ? (const V*)p->d_twp64 : (const V*)p->d_twp32;
   prof_begin(st);
-  kern<<<grid, 512, smem, st>>>(p->dev, p->fft, p->d_rinv, (const V*)W, out0, out1, ncomp, mlim, gscale, use_w, spow, tw);
+  kern<<<grid, 512, smem, st>>>(p->dev, p->fft, p->d_rinv, (const V*)W, out0, out1, ncomp, mlim, gscale, use_w, spow, tw,
+                                twp);
   SHTB_LAUNCHED("fft synthesis kernel");
   return SHTB_OK;
 }
@@ -280,8 +306,9 @@ static int launch_ana_h(const shtb_plan* p, const T* in0, const T* in1, int ncom
   SHTB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "fft smem attr");
   dim3 grid((p->npair + H - 1) / H, nfw);
   const V* tw = std::is_same<T, double>::value ? (const V*)p->d_tw64 : (const V*)p->d_tw32;
+  const V* twp = std::is_same<T, double>::value ? (const V*)p->d_twp64 : (const V*)p->d_twp32;
   prof_begin(st);
-  kern<<<grid, 512, smem, st>>>(p->dev, p->fft, p->d_rev, in0, in1, ncomp, (V*)W, mlim, wscale, use_w, spow, tw);
+  kern<<<grid, 512, smem, st>>>(p->dev, p->fft, p->d_rev, in0, in1, ncomp, (V*)W, mlim, wscale, use_w, spow, tw, twp);
   SHTB_LAUNCHED("fft analysis kernel");
   return SHTB_OK;
 }

@@ -128,37 +128,65 @@ __device__ __forceinline__ void dft_small(V* u, int dir, const V* __restrict__ t
 
 // One DIF pass of radix r on sub-transforms of length Ns (all F rows, stride S):
 // for j < Ns/r, element group {base + j + q*Ns/r}: DFT_r, then twiddle
-// W_Ns^(j*q) on output q.
+// W_Ns^(j*q) on output q, read from this pass's table twp[(q-1)*span + j].
+// Group indices are split with multiply-high divisions (magic_div_mul), and each
+// thread loads two groups before computing either so their loads overlap.
+template <typename T, typename V, int RADIX>
+__device__ __forceinline__ void dif_group_load(const V* X, int S, int N, int span, unsigned mrow, unsigned mspan,
+                                               int per_row, int r, int b, V* u, int& rowoff, int& base, int& j) {
+  const int f = mrow ? (int)__umulhi((unsigned)b, mrow) : b;
+  const int t = b - f * per_row;
+  const int blk = mspan ? (int)__umulhi((unsigned)t, mspan) : t;
+  j = t - blk * span;
+  base = blk * span * r + j;
+  rowoff = f * S;
+#pragma unroll
+  for (int q = 0; q < RADIX; ++q)
+    if (q < r) u[q] = X[rowoff + fft_pad(base + q * span)];
+}
+
+template <typename T, typename V, int RADIX>
+__device__ __forceinline__ void dif_group_finish(V* X, int span, int r, const V* __restrict__ tw, int N,
+                                                 const V* __restrict__ twp, int dir, V* u, int rowoff, int base, int j) {
+  dft_small<T, V, RADIX>(u, dir, tw, N / r, r);
+  if (j != 0) {
+#pragma unroll
+    for (int q = 1; q < RADIX; ++q) {
+      if (q < r) {
+        V wv = twp[(q - 1) * span + j];
+        if (dir > 0) wv.y = -wv.y;
+        u[q] = cmul(u[q], wv);
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < RADIX; ++q)
+    if (q < r) X[rowoff + fft_pad(base + q * span)] = u[q];
+}
+
 template <typename T, typename V, int RADIX>
 __device__ __forceinline__ void dif_pass(V* X, int F, int N, int S, int Ns, int radix_rt, const V* __restrict__ tw,
-                                         int dir) {
+                                         const V* __restrict__ twp, unsigned mrow, unsigned mspan, int dir) {
   const int r = (RADIX >= 7) ? radix_rt : RADIX;
   const int span = Ns / r;            // distance between group members
   const int per_row = N / r;          // groups per row
-  const int twmul = N / Ns;           // table step for W_Ns
-  for (int b = threadIdx.x; b < F * per_row; b += blockDim.x) {
-    const int f = b / per_row, t = b - f * per_row;
-    const int blk = t / span, j = t - blk * span;
-    const int base = blk * Ns + j;
-    V* row = X + (size_t)f * S;
-    V u[RADIX];
-#pragma unroll
-    for (int q = 0; q < RADIX; ++q)
-      if (q < r) u[q] = row[fft_pad(base + q * span)];
-    dft_small<T, V, RADIX>(u, dir, tw, N / r, r);
-    if (j != 0) {
-#pragma unroll
-      for (int q = 1; q < RADIX; ++q) {
-        if (q < r) {
-          V wv = tw[j * q * twmul];
-          if (dir > 0) wv.y = -wv.y;
-          u[q] = cmul(u[q], wv);
-        }
-      }
+  const int total = F * per_row;
+  const int bd = blockDim.x;
+  // two groups in flight for FP32 radices <= 8; FP64 and the generic radix keep one (registers)
+  constexpr bool kTwo = (RADIX <= 8) && (sizeof(T) == 4);
+  const int step = kTwo ? 2 * bd : bd;
+  for (int b = threadIdx.x; b < total; b += step) {
+    V u0[RADIX], u1[kTwo ? RADIX : 1];
+    int ro0, ba0, j0, ro1 = 0, ba1 = 0, j1 = 0;
+    const bool two = kTwo && (b + bd < total);
+    dif_group_load<T, V, RADIX>(X, S, N, span, mrow, mspan, per_row, r, b, u0, ro0, ba0, j0);
+    if constexpr (kTwo) {
+      if (two) dif_group_load<T, V, RADIX>(X, S, N, span, mrow, mspan, per_row, r, b + bd, u1, ro1, ba1, j1);
     }
-#pragma unroll
-    for (int q = 0; q < RADIX; ++q)
-      if (q < r) row[fft_pad(base + q * span)] = u[q];
+    dif_group_finish<T, V, RADIX>(X, span, r, tw, N, twp, dir, u0, ro0, ba0, j0);
+    if constexpr (kTwo) {
+      if (two) dif_group_finish<T, V, RADIX>(X, span, r, tw, N, twp, dir, u1, ro1, ba1, j1);
+    }
   }
   __syncthreads();
 }
@@ -166,7 +194,8 @@ __device__ __forceinline__ void dif_pass(V* X, int F, int N, int S, int Ns, int 
 // Full in-place FFT of F rows (natural-order input; output bin k at rev[k]).
 // `scratch` (same size as X) is used only in direct mode (a prime factor above 13).
 template <typename T, typename V, bool GENERIC>
-__device__ void fft_rows(V* X, V* scratch, int F, int S, const FFTDesc& fd, const V* __restrict__ tw, int dir) {
+__device__ void fft_rows(V* X, V* scratch, int F, int S, const FFTDesc& fd, const V* __restrict__ tw,
+                         const V* __restrict__ twp, int dir) {
   const int N = fd.n;
   if (GENERIC && fd.direct) {
     // O(N^2) DFT into scratch, written at natural positions (rev = identity in direct mode)
@@ -195,14 +224,16 @@ __device__ void fft_rows(V* X, V* scratch, int F, int S, const FFTDesc& fd, cons
   int Ns = N;
   for (int s = 0; s < fd.nrad; ++s) {
     const int r = fd.rad[s];
+    const V* tp = twp + fd.twoff[s];
+    const unsigned mr = fd.mrow[s], ms = fd.mspan[s];
     switch (r) {
-      case 2: dif_pass<T, V, 2>(X, F, N, S, Ns, 2, tw, dir); break;
-      case 3: dif_pass<T, V, 3>(X, F, N, S, Ns, 3, tw, dir); break;
-      case 4: dif_pass<T, V, 4>(X, F, N, S, Ns, 4, tw, dir); break;
-      case 5: dif_pass<T, V, 5>(X, F, N, S, Ns, 5, tw, dir); break;
-      case 8: dif_pass<T, V, 8>(X, F, N, S, Ns, 8, tw, dir); break;
+      case 2: dif_pass<T, V, 2>(X, F, N, S, Ns, 2, tw, tp, mr, ms, dir); break;
+      case 3: dif_pass<T, V, 3>(X, F, N, S, Ns, 3, tw, tp, mr, ms, dir); break;
+      case 4: dif_pass<T, V, 4>(X, F, N, S, Ns, 4, tw, tp, mr, ms, dir); break;
+      case 5: dif_pass<T, V, 5>(X, F, N, S, Ns, 5, tw, tp, mr, ms, dir); break;
+      case 8: dif_pass<T, V, 8>(X, F, N, S, Ns, 8, tw, tp, mr, ms, dir); break;
       default:
-        if constexpr (GENERIC) dif_pass<T, V, 13>(X, F, N, S, Ns, r, tw, dir);
+        if constexpr (GENERIC) dif_pass<T, V, 13>(X, F, N, S, Ns, r, tw, tp, mr, ms, dir);
         break;
     }
     Ns /= r;

@@ -64,7 +64,15 @@ struct FFTDesc {
   int nrad;
   int rad[24];
   bool direct;             // a prime factor above the largest register radix: O(N^2) DFT
+  int twoff[24];           // pass s twiddles start at twoff[s] in the per-pass table
+  unsigned mrow[24];       // floor(2^32 / (n / rad[s])) + 1, or 0 when n / rad[s] == 1
+  unsigned mspan[24];      // the same for the group span Ns / rad[s]
 };
+
+// floor(v / d) for v * d < 2^32 with the multiplier m = floor(2^32 / d) + 1 (m = 0 means d = 1)
+__host__ __device__ inline unsigned magic_div_mul(unsigned d) {
+  return d <= 1 ? 0u : (unsigned)((1ull << 32) / d + 1);
+}
 
 }  // namespace shtb
 
@@ -87,6 +95,8 @@ struct shtb_plan {
   const float2* d_tw32 = nullptr;
   const int* d_rev = nullptr;             // FFT output position of bin k (digit reversal)
   const int* d_rinv = nullptr;            // natural index stored at FFT position q (inverse of d_rev)
+  const double2* d_twp64 = nullptr;       // per-pass twiddles: pass s, factor q (1..r-1), index j < span:
+  const float2* d_twp32 = nullptr;        //   entry twoff[s] + (q-1)*span + j = exp(-2 pi i j q / Ns)
   const double* d_dcoef = nullptr;        // packed d(l,m) = sqrt((l^2-m^2)/(4l^2-1)), l in [m, lrec]
   std::vector<int2> htiles;
   int* d_err = nullptr;                   // device status word (bounded waits that gave up)

@@ -141,7 +141,34 @@ static bool factor_fft(int n, FFTDesc& d) {
     d.direct = true;
     d.nrad = 0;
   }
+  int off = 0, Ns = n;
+  for (int s = 0; s < d.nrad; ++s) {
+    const int r = d.rad[s], span = Ns / r;
+    d.twoff[s] = off;
+    d.mrow[s] = magic_div_mul((unsigned)(n / r));
+    d.mspan[s] = magic_div_mul((unsigned)span);
+    off += (r - 1) * span;
+    Ns = span;
+  }
   return true;
+}
+
+// Per-pass twiddle table (layout of FFTDesc::twoff): entry twoff[s] + (q-1)*span + j.
+static int fft_pass_twiddles(const FFTDesc& d, std::vector<double2>& out) {
+  out.clear();
+  int Ns = d.n;
+  for (int s = 0; s < d.nrad; ++s) {
+    const int r = d.rad[s], span = Ns / r;
+    for (int q = 1; q < r; ++q)
+      for (int j = 0; j < span; ++j) {
+        const long long e = ((long long)j * q) % Ns;
+        const double ang = -2.0 * (double)e / (double)Ns;   // in units of pi
+        out.push_back(make_double2(std::cos(M_PI * ang), std::sin(M_PI * ang)));
+      }
+    Ns = span;
+  }
+  if (out.empty()) out.push_back(make_double2(1.0, 0.0));
+  return (int)out.size();
 }
 
 }  // namespace shtb
@@ -311,6 +338,10 @@ extern "C" int shtb_plan_create(shtb_plan** out, int lmax, int mmax, int mres, i
   for (int k = 0; k < nlon; ++k) rinv[rev[k]] = k;
   std::vector<float2> tw32(nlon);
   for (int t = 0; t < nlon; ++t) tw32[t] = make_float2((float)tw[t].x, (float)tw[t].y);
+  std::vector<double2> twp;
+  const int ntwp = fft_pass_twiddles(p->fft, twp);
+  std::vector<float2> twp32(ntwp);
+  for (int t = 0; t < ntwp; ++t) twp32[t] = make_float2((float)twp[t].x, (float)twp[t].y);
 
   // one device allocation for all tables
   size_t o = 0;
@@ -322,6 +353,7 @@ extern "C" int shtb_plan_create(shtb_plan** out, int lmax, int mmax, int mres, i
   const size_t o_scale = coeff_scale ? take((size_t)(lmax + 1) * (mmax + 1) * 8) : 0;
   const size_t o_tw = take((size_t)nlon * 16), o_tw32 = take((size_t)nlon * 8);
   const size_t o_seed = take((mmax + 2) * 8), o_tb = take(nm * 4), o_rev = take((size_t)nlon * 4), o_rinv = take((size_t)nlon * 4);
+  const size_t o_twp = take((size_t)ntwp * 16), o_twp32 = take((size_t)ntwp * 8);
   const size_t o_err = take(16);
   p->dbytes = o;
   cudaError_t ce = cudaMalloc(&p->dmem, o);
@@ -349,6 +381,8 @@ extern "C" int shtb_plan_create(shtb_plan** out, int lmax, int mmax, int mres, i
   if (ce == cudaSuccess) ce = up(o_tb, tile_base.data(), nm * 4);
   if (ce == cudaSuccess) ce = up(o_rev, rev.data(), (size_t)nlon * 4);
   if (ce == cudaSuccess) ce = up(o_rinv, rinv.data(), (size_t)nlon * 4);
+  if (ce == cudaSuccess) ce = up(o_twp, twp.data(), (size_t)ntwp * 16);
+  if (ce == cudaSuccess) ce = up(o_twp32, twp32.data(), (size_t)ntwp * 8);
   if (ce != cudaSuccess) {
     cudaFree(p->dmem);
     delete p;
@@ -374,6 +408,8 @@ extern "C" int shtb_plan_create(shtb_plan** out, int lmax, int mmax, int mres, i
   p->d_dcoef = (const double*)(D + o_d);
   p->d_rev = (const int*)(D + o_rev);
   p->d_rinv = (const int*)(D + o_rinv);
+  p->d_twp64 = (const double2*)(D + o_twp);
+  p->d_twp32 = (const float2*)(D + o_twp32);
   p->d_err = (int*)(D + o_err);
   if (ce == cudaSuccess) ce = cudaMemset(D + o_err, 0, 16);
 
