@@ -163,6 +163,35 @@ int shtb_analysis_sphtor_adjoint(const shtb_plan* plan, const void* Sbar, const 
 int shtb_synthesis_noalloc(const shtb_plan* plan, const void* alm, void* f, int nfields, int ltr,
                            void* stream);
 
+/*
+ * Uneven batches: n independent mixed-precision (FP32 buffers, 3xTF32 tensor-core
+ * Legendre stage) scalar transforms, each with its own plan (its own lmax, Gauss grid
+ * and nlon) and 1..8 fields. No single counterpart in the reference, whose transforms
+ * run one configuration per call (src/core_transforms.jl, src/batch_transforms.jl):
+ * a group runs every member's tiles in one persistent launch per stage (order-GEMM
+ * synthesis, FFT synthesis, FFT analysis, order-GEMM analysis), work items sorted by
+ * cost, the stage launches captured once in a CUDA graph and replayed.
+ * Members must use lcap = lmax and mres = 1. Buffers (device pointers, per member):
+ * alm_in and alm_out are (lmax+1, mmax+1, nfields) complex FP32 (Julia column-major),
+ * grid is (nlat, nlon, nfields) FP32. Results equal those of shtb_synthesis /
+ * shtb_analysis with SHTB_PREC_MIXED on the same member, bit for bit.
+ */
+typedef struct shtb_group shtb_group;
+int shtb_group_create(shtb_group** out, const shtb_plan* const* plans, int n, const int* nfields);
+int shtb_group_destroy(shtb_group* group);
+/* Bind per-member device buffers (arrays of n pointers); invalidates the captured graph. */
+int shtb_group_bind(shtb_group* group, void* const* alm_in, void* const* grid, void* const* alm_out);
+/* synthesis alm_in -> grid, then analysis grid -> alm_out, as one graph launch on stream. */
+int shtb_group_roundtrip(shtb_group* group, void* stream);
+/* The same stages launched directly (no graph); op = SHTB_OP_SYNTHESIS, SHTB_OP_ANALYSIS or -1 (both). */
+int shtb_group_launch(shtb_group* group, int op, void* stream);
+/* Time the candidate launch shapes on the bound buffers and keep the fastest (blocking). */
+int shtb_group_autotune(shtb_group* group, void* stream);
+/* Launch shape in use: FFT latitude pairs per CTA, FFT CTAs, GEMM CTAs. */
+int shtb_group_config(const shtb_group* group, int* fft_pairs, int* fft_ctas, int* gemm_ctas);
+/* After the last roundtrip completed: per-member completion time in ns after its start (n values). */
+int shtb_group_latency_ns(const shtb_group* group, uint64_t* ns);
+
 /* Number of kernels the library launched on this host thread since the last reset. */
 uint64_t shtb_launch_count(int reset);
 

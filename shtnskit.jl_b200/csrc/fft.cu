@@ -10,6 +10,8 @@
 // latitude count allows; W is read/written per order m as H contiguous complex values.
 // The FFT itself (fft.cuh) leaves bins in digit-reversed positions, so the synthesis
 // output loop walks shared memory in storage order q and writes longitude rinv[q].
+#include <cstring>
+
 #include "fft.cuh"
 #include "kernels.cuh"
 
@@ -57,20 +59,41 @@ __device__ __forceinline__ void store_seg(T* __restrict__ dst, const T* v) {
   }
 }
 
+// Everything one FFT launch needs about one transform; the grouped kernels stage it in
+// shared memory per work item.
+template <typename T>
+struct FFTJob {
+  PlanDev P;
+  FFTDesc fd;
+  const int* perm;                        // rinv (synthesis) or rev (analysis)
+  const typename V2<T>::type* Win;        // synthesis: Fourier buffer in
+  typename V2<T>::type* Wout;             // analysis: Fourier buffer out
+  T* g0;                                  // grid (synthesis out / analysis in), component 0
+  T* g1;                                  // component 1 when ncomp == 2
+  int ncomp, mlim, use_w, spow;
+  double scale;                           // synthesis: grid factor; analysis: weight factor
+  const typename V2<T>::type* tw;
+  const typename V2<T>::type* twp;
+};
+
+// Latitude pairs p0 .. p0+H-1 of field k.
 template <typename T, int H, bool GENERIC>
-__global__ void __launch_bounds__(512) fft_syn_kernel(PlanDev P, FFTDesc fd, const int* __restrict__ rinv,
-                                                      const typename V2<T>::type* __restrict__ W, T* __restrict__ out0,
-                                                      T* __restrict__ out1, int ncomp, int mlim, double gscale,
-                                                      int use_w, int spow, const typename V2<T>::type* __restrict__ tw,
-                                                      const typename V2<T>::type* __restrict__ twp) {
+__device__ __forceinline__ void fft_syn_body(const FFTJob<T>& J, int p0, int k, unsigned char* smem_raw) {
+  const PlanDev& P = J.P;
+  const FFTDesc& fd = J.fd;
+  const int* __restrict__ rinv = J.perm;
+  const typename V2<T>::type* __restrict__ W = J.Win;
+  T* __restrict__ out0 = J.g0;
+  T* __restrict__ out1 = J.g1;
+  const int ncomp = J.ncomp, mlim = J.mlim, use_w = J.use_w, spow = J.spow;
+  const double gscale = J.scale;
+  const typename V2<T>::type* __restrict__ tw = J.tw;
+  const typename V2<T>::type* __restrict__ twp = J.twp;
   using V = typename V2<T>::type;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   const int N = fd.n, S = fft_row_stride(N);
   V* Z = reinterpret_cast<V*>(smem_raw);
   V* scratch = Z + H * S;
   T* gfac = reinterpret_cast<T*>(Z + ((GENERIC && fd.direct) ? 2 : 1) * H * S);
-  const int p0 = blockIdx.x * H;
-  const int k = blockIdx.y;
   const int npair = P.npair, nlat = P.nlat;
   const int hv = min(H, npair - p0);
   // Bins the order loop below does not write (|m| > mlim, or m off the mres lattice)
@@ -176,20 +199,24 @@ __global__ void __launch_bounds__(512) fft_syn_kernel(PlanDev P, FFTDesc fd, con
   }
 }
 
+// Latitude pairs p0 .. p0+H-1 of field k.
 template <typename T, int H, bool GENERIC>
-__global__ void __launch_bounds__(512) fft_ana_kernel(PlanDev P, FFTDesc fd, const int* __restrict__ rev,
-                                                      const T* __restrict__ in0, const T* __restrict__ in1, int ncomp,
-                                                      typename V2<T>::type* __restrict__ W, int mlim, double wscale,
-                                                      int use_w, int spow, const typename V2<T>::type* __restrict__ tw,
-                                                      const typename V2<T>::type* __restrict__ twp) {
+__device__ __forceinline__ void fft_ana_body(const FFTJob<T>& J, int p0, int k, unsigned char* smem_raw) {
+  const PlanDev& P = J.P;
+  const FFTDesc& fd = J.fd;
+  const int* __restrict__ rev = J.perm;
+  const T* __restrict__ in0 = J.g0;
+  const T* __restrict__ in1 = J.g1;
+  typename V2<T>::type* __restrict__ W = J.Wout;
+  const int ncomp = J.ncomp, mlim = J.mlim, use_w = J.use_w, spow = J.spow;
+  const double wscale = J.scale;
+  const typename V2<T>::type* __restrict__ tw = J.tw;
+  const typename V2<T>::type* __restrict__ twp = J.twp;
   using V = typename V2<T>::type;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   const int N = fd.n, S = fft_row_stride(N);
   V* Z = reinterpret_cast<V*>(smem_raw);
   V* scratch = Z + H * S;
   T* wfac = reinterpret_cast<T*>(Z + ((GENERIC && fd.direct) ? 2 : 1) * H * S);
-  const int p0 = blockIdx.x * H;
-  const int k = blockIdx.y;
   const int npair = P.npair, nlat = P.nlat;
   const int hv = min(H, npair - p0);
   const T* in = (ncomp == 2 && (k & 1)) ? in1 : in0;
@@ -253,6 +280,61 @@ __global__ void __launch_bounds__(512) fft_ana_kernel(PlanDev P, FFTDesc fd, con
   }
 }
 
+template <typename T, int H, bool GENERIC>
+__global__ void __launch_bounds__(512) fft_syn_kernel(const __grid_constant__ FFTJob<T> J) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  fft_syn_body<T, H, GENERIC>(J, blockIdx.x * H, blockIdx.y, smem_raw);
+}
+
+template <typename T, int H, bool GENERIC>
+__global__ void __launch_bounds__(512) fft_ana_kernel(const __grid_constant__ FFTJob<T> J) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  fft_ana_body<T, H, GENERIC>(J, blockIdx.x * H, blockIdx.y, smem_raw);
+}
+
+// Persistent FFTs over many independent transforms: CTA i runs items i, i + gridDim.x,
+// ...; item = (transform, first latitude pair, field). Shared memory is sized for the
+// longest row of the group.
+template <typename T, int H, bool GENERIC, bool SYN>
+__global__ void __launch_bounds__(512) fft_group_kernel(const FFTJob<T>* __restrict__ jobs,
+                                                        const int4* __restrict__ items, int nitems) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ FFTJob<T> sj;
+  for (int i = blockIdx.x; i < nitems; i += gridDim.x) {
+    const int4 it = items[i];
+    if (threadIdx.x == 0) sj = jobs[it.x];
+    __syncthreads();
+    if (SYN)
+      fft_syn_body<T, H, GENERIC>(sj, it.y, it.z, smem_raw);
+    else
+      fft_ana_body<T, H, GENERIC>(sj, it.y, it.z, smem_raw);
+    __syncthreads();
+  }
+}
+
+template <typename T>
+static FFTJob<T> fft_job(const shtb_plan* p, const int* perm, const typename V2<T>::type* Win,
+                         typename V2<T>::type* Wout, T* g0, T* g1, int ncomp, int mlim, double scale, int use_w,
+                         int spow) {
+  using V = typename V2<T>::type;
+  FFTJob<T> J;
+  J.P = p->dev;
+  J.fd = p->fft;
+  J.perm = perm;
+  J.Win = Win;
+  J.Wout = Wout;
+  J.g0 = g0;
+  J.g1 = g1;
+  J.ncomp = ncomp;
+  J.mlim = mlim;
+  J.use_w = use_w;
+  J.spow = spow;
+  J.scale = scale;
+  J.tw = std::is_same<T, double>::value ? (const V*)p->d_tw64 : (const V*)p->d_tw32;
+  J.twp = std::is_same<T, double>::value ? (const V*)p->d_twp64 : (const V*)p->d_twp32;
+  return J;
+}
+
 // H latitude pairs per CTA: the largest power of two <= 16 whose shared-memory
 // footprint stays within ~200 KB (one CTA of 512 threads per SM). Two CTAs of 256
 // threads with half the pairs measured slower on B200: their grid segments shrink to
@@ -287,11 +369,9 @@ static int launch_syn_h(const shtb_plan* p, const void* W, T* out0, T* out1, int
   auto kern = fft_generic(p) ? fft_syn_kernel<T, H, true> : fft_syn_kernel<T, H, false>;
   SHTB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "fft smem attr");
   dim3 grid((p->npair + H - 1) / H, nfw);
-  const V* tw = std::is_same<T, double>::value ? (const V*)p->d_tw64 : (const V*)p->d_tw32;
-  const V* twp = std::is_same<T, double>::value ? (const V*)p->d_twp64 : (const V*)p->d_twp32;
+  const FFTJob<T> J = fft_job<T>(p, p->d_rinv, (const V*)W, nullptr, out0, out1, ncomp, mlim, gscale, use_w, spow);
   prof_begin(st);
-  kern<<<grid, 512, smem, st>>>(p->dev, p->fft, p->d_rinv, (const V*)W, out0, out1, ncomp, mlim, gscale, use_w, spow, tw,
-                                twp);
+  kern<<<grid, 512, smem, st>>>(J);
   SHTB_LAUNCHED("fft synthesis kernel");
   return SHTB_OK;
 }
@@ -305,10 +385,10 @@ static int launch_ana_h(const shtb_plan* p, const T* in0, const T* in1, int ncom
   auto kern = fft_generic(p) ? fft_ana_kernel<T, H, true> : fft_ana_kernel<T, H, false>;
   SHTB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "fft smem attr");
   dim3 grid((p->npair + H - 1) / H, nfw);
-  const V* tw = std::is_same<T, double>::value ? (const V*)p->d_tw64 : (const V*)p->d_tw32;
-  const V* twp = std::is_same<T, double>::value ? (const V*)p->d_twp64 : (const V*)p->d_twp32;
+  const FFTJob<T> J = fft_job<T>(p, p->d_rev, nullptr, (V*)W, const_cast<T*>(in0), const_cast<T*>(in1), ncomp, mlim,
+                                 wscale, use_w, spow);
   prof_begin(st);
-  kern<<<grid, 512, smem, st>>>(p->dev, p->fft, p->d_rev, in0, in1, ncomp, (V*)W, mlim, wscale, use_w, spow, tw, twp);
+  kern<<<grid, 512, smem, st>>>(J);
   SHTB_LAUNCHED("fft analysis kernel");
   return SHTB_OK;
 }
@@ -343,5 +423,47 @@ template int launch_fft_syn<double, double>(const shtb_plan*, const void*, doubl
 template int launch_fft_ana<double, double>(const shtb_plan*, const double*, const double*, int, void*, int, int, double, int, int, cudaStream_t);
 template int launch_fft_syn<float, float>(const shtb_plan*, const void*, float*, float*, int, int, int, double, int, int, cudaStream_t);
 template int launch_fft_ana<float, float>(const shtb_plan*, const float*, const float*, int, void*, int, int, double, int, int, cudaStream_t);
+
+// ---------------------------------------------------------------- grouped transforms
+// Host-side pieces of the persistent grouped FP32 FFTs.
+
+size_t fft_job_bytes_f32() { return sizeof(FFTJob<float>); }
+
+void fft_fill_job_f32(const shtb_plan* p, int syn, const void* W, void* grid, int nf, void* host_job) {
+  const int mlim = std::min(p->mmax, p->lmax);
+  FFTJob<float> J = syn ? fft_job<float>(p, p->d_rinv, (const float2*)W, nullptr, (float*)grid, nullptr, 1, mlim,
+                                         p->phi_inv_scale / p->nlon, 0, 0)
+                        : fft_job<float>(p, p->d_rev, nullptr, (float2*)const_cast<void*>(W), (float*)grid, nullptr, 1,
+                                         mlim, p->ana_scale, 1, 0);
+  (void)nf;
+  std::memcpy(host_job, &J, sizeof(J));
+}
+
+size_t fft_group_smem_f32(const shtb_plan* p, int h) { return fft_smem(p->fft, sizeof(float2), h); }
+
+bool fft_plan_generic(const shtb_plan* p) { return fft_generic(p); }
+
+template <int H, bool GENERIC>
+static int launch_fft_group_h(int syn, const void* jobs, const int4* items, int nitems, int grid, size_t smem,
+                              cudaStream_t st) {
+  auto kern = syn ? fft_group_kernel<float, H, GENERIC, true> : fft_group_kernel<float, H, GENERIC, false>;
+  SHTB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "group fft smem attr");
+  kern<<<grid, 512, smem, st>>>((const FFTJob<float>*)jobs, items, nitems);
+  count_launch();
+  SHTB_TRY_CUDA(cudaGetLastError(), "group fft launch");
+  return SHTB_OK;
+}
+
+int launch_fft_group_f32(int syn, int h, bool generic, const void* jobs, const int4* items, int nitems, int grid,
+                         size_t smem, cudaStream_t st) {
+  if (nitems <= 0) return SHTB_OK;
+  if (smem > 227 * 1024) return set_error(SHTB_ERR_UNSUPPORTED, "group FFT tile does not fit in shared memory");
+#define SHTB_GFFT(H_)                                                                   \
+  if (h == H_) return generic ? launch_fft_group_h<H_, true>(syn, jobs, items, nitems, grid, smem, st) \
+                              : launch_fft_group_h<H_, false>(syn, jobs, items, nitems, grid, smem, st);
+  SHTB_GFFT(16) SHTB_GFFT(8) SHTB_GFFT(4) SHTB_GFFT(2)
+#undef SHTB_GFFT
+  return set_error(SHTB_ERR_BAD_ARG, "group FFT: unsupported pairs per CTA");
+}
 
 }  // namespace shtb

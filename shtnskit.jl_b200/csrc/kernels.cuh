@@ -49,4 +49,19 @@ int launch_sphtor_post64(const shtb_plan* p, const double2* V, double2* S, doubl
                          const Factors& F, int div_ll, cudaStream_t st);
 int launch_zero_columns64(const shtb_plan* p, double2* a, int nf, int mlim, cudaStream_t st);
 
+// Grouped (uneven-batch) execution: persistent launches over the tiles of many plans.
+int mixed_prepare(const shtb_plan* p, cudaStream_t st);
+size_t mixed_args_bytes();
+void mixed_fill_args(const shtb_plan* p, int mode, const void* in, void* out, int nf, void* host_args);
+int mixed_group_ksteps(const shtb_plan* p, int mode, int im, int par);
+int mixed_group_tile_rows();
+int launch_gemm_group(int mode, const void* targs, const int4* items, int nitems, int grid, unsigned long long* done,
+                      cudaStream_t st);
+size_t fft_job_bytes_f32();
+void fft_fill_job_f32(const shtb_plan* p, int syn, const void* W, void* grid, int nf, void* host_job);
+size_t fft_group_smem_f32(const shtb_plan* p, int h);
+bool fft_plan_generic(const shtb_plan* p);
+int launch_fft_group_f32(int syn, int h, bool generic, const void* jobs, const int4* items, int nitems, int grid,
+                         size_t smem, cudaStream_t st);
+
 }  // namespace shtb

@@ -26,6 +26,7 @@
 // Every mbarrier wait is bounded (2 s of %globaltimer); a timeout sets the
 // plan's error word and the CTA drains and exits.
 #include <climits>
+#include <cstring>
 
 #include "kernels.cuh"
 
@@ -215,64 +216,105 @@ struct Smem {
   static constexpr int kBytes = kBar + (3 * kStages + 4) * 8 + 16;
 };
 
-// MODE 0: synthesis, MODE 1: analysis. N = columns per CTA (2 x fields).
-// blockIdx.x = 2 * tile + parity; one CTA accumulates one parity class.
-template <int MODE, int N>
-__global__ void __launch_bounds__(kThreads, 1) mixed_gemm_kernel(const __grid_constant__ Args a) {
+// Coordinates of one GEMM tile: order index im, first latitude pair p0 (synthesis) or
+// first degree index j0 (analysis), parity class par, first field kb.
+struct TileCoord {
+  int im, p0, j0, par, kb;
+};
+
+// Shared-memory barriers of a GEMM CTA (initialised once per CTA).
+struct Bars {
+  unsigned long long *full, *empty, *ldfull, *accf, *acce;
+  unsigned* tmem_slot;
+  volatile int* abort_flag;
+};
+
+template <int N>
+__device__ __forceinline__ Bars gemm_bars(unsigned char* sm) {
   using S = Smem<N>;
-  extern __shared__ __align__(1024) unsigned char sm[];
-  unsigned long long* full = reinterpret_cast<unsigned long long*>(sm + S::kBar);
-  unsigned long long* empty = full + kStages;
-  unsigned long long* ldfull = empty + kStages;  // [kStages] loader copies of the stage landed
-  unsigned long long* accf = ldfull + kStages;  // [2] chunk accumulated in TMEM buffer b
-  unsigned long long* acce = accf + 2;          // [2] TMEM buffer b drained by the promotion warps
-  unsigned* tmem_slot = reinterpret_cast<unsigned*>(acce + 2);
-  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  Bars B;
+  B.full = reinterpret_cast<unsigned long long*>(sm + S::kBar);
+  B.empty = B.full + kStages;
+  B.ldfull = B.empty + kStages;   // [kStages] loader copies of the stage landed
+  B.accf = B.ldfull + kStages;    // [2] chunk accumulated in TMEM buffer b
+  B.acce = B.accf + 2;            // [2] TMEM buffer b drained by the promotion warps
+  B.tmem_slot = reinterpret_cast<unsigned*>(B.acce + 2);
+  B.abort_flag = reinterpret_cast<volatile int*>(B.tmem_slot + 1);
+  return B;
+}
 
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const PlanDev& P = a.P;
-  const int npair = P.npair;
-  const int par = blockIdx.x & 1, tile = blockIdx.x >> 1;
-  int im, p0 = 0, j0 = 0;
-  if (MODE == 0) {
-    im = blockIdx.y;
-    p0 = tile * kM;
-  } else {
-    const int2 t = a.tiles[tile];
-    im = t.x;
-    j0 = t.y;
-  }
-  const int m = im * P.mres;
-  const int kb = blockIdx.z * (N / 2);
-  // degrees of this parity class in [m, lend]
-  const int J = (a.lend >= m + par) ? (a.lend - m - par) / 2 + 1 : 0;
-  const long long sg = a.seg[2 * im + par];
-  const long long ln = a.seg[2 * im + par + 1] - sg;
-  const int nks = (MODE == 0) ? (J + kK - 1) / kK : (npair + kK - 1) / kK;
-  const int nch = (nks + kChunk - 1) / kChunk;
+// K-steps of a tile (the same count in every role).
+template <int MODE>
+__device__ __forceinline__ int tile_ksteps(const Args& a, const TileCoord& tc) {
+  const int m = tc.im * a.P.mres;
+  const int J = (a.lend >= m + tc.par) ? (a.lend - m - tc.par) / 2 + 1 : 0;
+  return (MODE == 0) ? (J + kK - 1) / kK : (a.P.npair + kK - 1) / kK;
+}
 
+// Barrier setup and TMEM allocation, once per CTA.
+template <int N>
+__device__ __forceinline__ unsigned gemm_cta_setup(const Bars& B) {
+  const int tid = threadIdx.x, warp = tid >> 5;
   if (tid == 0) {
     for (int s = 0; s < kStages; ++s) {
-      mbar_init(&full[s], 128);
-      mbar_init(&empty[s], 1);
-      mbar_init(&ldfull[s], 128);
+      mbar_init(&B.full[s], 128);
+      mbar_init(&B.empty[s], 1);
+      mbar_init(&B.ldfull[s], 128);
     }
     for (int b = 0; b < 2; ++b) {
-      mbar_init(&accf[b], 1);
-      mbar_init(&acce[b], 256);
+      mbar_init(&B.accf[b], 1);
+      mbar_init(&B.acce[b], 256);
     }
-    *abort_flag = 0;
+    *B.abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 8) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(B.tmem_slot)),
                  "r"(4 * N));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  const unsigned tmem = *tmem_slot;
+  return *B.tmem_slot;
+}
+
+template <int N>
+__device__ __forceinline__ void gemm_cta_teardown(unsigned tmem) {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if ((threadIdx.x >> 5) == 8) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(4 * N));
+  }
+}
+
+// One GEMM tile. MODE 0: synthesis, MODE 1: analysis; N = columns per CTA (2 x fields).
+// A persistent CTA runs many tiles through the same barriers: ks0 and c0 count the
+// K-steps and chunks of the tiles before this one, which fixes every stage index and
+// barrier phase. Callers separate tiles with __syncthreads (the cross-term TMEM buffer
+// is reused).
+template <int MODE, int N>
+__device__ __forceinline__ void gemm_tile(const Args& a, const TileCoord& tc, unsigned char* sm, const Bars& B,
+                                          unsigned tmem, unsigned ks0, unsigned c0) {
+  using S = Smem<N>;
+  unsigned long long* full = B.full;
+  unsigned long long* empty = B.empty;
+  unsigned long long* ldfull = B.ldfull;
+  unsigned long long* accf = B.accf;
+  unsigned long long* acce = B.acce;
+  volatile int* abort_flag = B.abort_flag;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const PlanDev& P = a.P;
+  const int npair = P.npair;
+  const int par = tc.par, im = tc.im, p0 = tc.p0, j0 = tc.j0, kb = tc.kb;
+  const int m = im * P.mres;
+  // degrees of this parity class in [m, lend]
+  const int J = (a.lend >= m + par) ? (a.lend - m - par) / 2 + 1 : 0;
+  const long long sg = a.seg[2 * im + par];
+  const long long ln = a.seg[2 * im + par + 1] - sg;
+  const int nks = tile_ksteps<MODE>(a, tc);
+  const int nch = (nks + kChunk - 1) / kChunk;
   // TMEM: chunk buffer b (hi*hi) at column b*N; the cross terms of the whole tile at 2N
 
   if (warp < 8) {
@@ -310,8 +352,9 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_gemm_kernel(const __grid_co
       const float* a0 = (MODE == 0) ? a.tab + sg * a.npp + p0 + t : a.tab + (sg + j0 + t) * a.npp;
       const bool arow_ok = (MODE == 0) || (j0 + t < ln);
       for (int ks = 0; ks < nks; ++ks) {
-        const int b = ks % kStages;
-        if (ks >= kStages && !mbar_wait(&empty[b], ((ks / kStages) - 1) & 1, abort_flag, a.err)) break;
+        const unsigned g = ks0 + ks;
+        const int b = g % kStages;
+        if (g >= kStages && !mbar_wait(&empty[b], ((g / kStages) - 1) & 1, abort_flag, a.err)) break;
         unsigned char* st = sm + (size_t)b * S::kStage;
         if (MODE == 0) {
 #pragma unroll
@@ -344,8 +387,9 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_gemm_kernel(const __grid_co
       const bool brow = t < N;
       const bool scaled = (MODE == 0) && (a.sc_mode || a.mf0 != 1.f || a.mf1 != 1.f);
       for (int ks = 0; ks < nks; ++ks) {
-        const int b = ks % kStages;
-        if (!mbar_wait(&ldfull[b], (ks / kStages) & 1, abort_flag, a.err)) break;
+        const unsigned g = ks0 + ks;
+        const int b = g % kStages;
+        if (!mbar_wait(&ldfull[b], (g / kStages) & 1, abort_flag, a.err)) break;
         unsigned char* st = sm + (size_t)b * S::kStage;
         unsigned char* Ah = st;
         unsigned char* Al = st + kTileBytesA;
@@ -394,14 +438,16 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_gemm_kernel(const __grid_co
       const unsigned idesc = idesc_tf32<N>();
       bool ok = true;
       for (int c = 0; c < nch && ok; ++c) {
-        const int bb = c & 1;
-        if (c >= 2 && !mbar_wait(&acce[bb], ((c >> 1) - 1) & 1, abort_flag, a.err)) break;
+        const unsigned gc = c0 + c;
+        const int bb = gc & 1;
+        if (gc >= 2 && !mbar_wait(&acce[bb], ((gc >> 1) - 1) & 1, abort_flag, a.err)) break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const unsigned dH = tmem + bb * N, dX = tmem + 2 * N;
         const int k1 = min(nks, (c + 1) * kChunk);
         for (int ks = c * kChunk; ks < k1; ++ks) {
-          const int b = ks % kStages;
-          if (!mbar_wait(&full[b], (ks / kStages) & 1, abort_flag, a.err)) {
+          const unsigned g = ks0 + ks;
+          const int b = g % kStages;
+          if (!mbar_wait(&full[b], (g / kStages) & 1, abort_flag, a.err)) {
             ok = false;
             break;
           }
@@ -430,8 +476,9 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_gemm_kernel(const __grid_co
     for (int i = 0; i < N / 2; ++i) acc[i] = 0.f;
     bool ok = true;
     for (int c = 0; c < nch; ++c) {
-      const int bb = c & 1;
-      if (ok) ok = mbar_wait(&accf[bb], (c >> 1) & 1, abort_flag, a.err);
+      const unsigned gc = c0 + c;
+      const int bb = gc & 1;
+      if (ok) ok = mbar_wait(&accf[bb], (gc >> 1) & 1, abort_flag, a.err);
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       __syncwarp();
       const unsigned dH = tmem + lane_base + bb * N + h * (N / 2);
@@ -487,12 +534,68 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_gemm_kernel(const __grid_co
       }
     }
   }
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  __syncthreads();
-  if (warp == 8) {
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(4 * N));
+}
+
+// One tile per CTA: blockIdx.x = 2 * tile + parity, blockIdx.y = order (synthesis),
+// blockIdx.z = block of N/2 fields.
+template <int MODE, int N>
+__global__ void __launch_bounds__(kThreads, 1) mixed_gemm_kernel(const __grid_constant__ Args a) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  const Bars B = gemm_bars<N>(sm);
+  const unsigned tmem = gemm_cta_setup<N>(B);
+  TileCoord tc;
+  tc.par = blockIdx.x & 1;
+  const int tile = blockIdx.x >> 1;
+  if (MODE == 0) {
+    tc.im = blockIdx.y;
+    tc.p0 = tile * kM;
+    tc.j0 = 0;
+  } else {
+    const int2 t = a.tiles[tile];
+    tc.im = t.x;
+    tc.j0 = t.y;
+    tc.p0 = 0;
   }
+  tc.kb = blockIdx.z * (N / 2);
+  gemm_tile<MODE, N>(a, tc, sm, B, tmem, 0u, 0u);
+  gemm_cta_teardown<N>(tmem);
+}
+
+// Persistent GEMM over the tiles of many independent transforms: CTA i runs items
+// i, i + gridDim.x, ... of a list sorted by decreasing cost; item = (transform,
+// im, p0 or j0, parity). Each transform's Args is staged in shared memory per item.
+// done[t] receives the %globaltimer value at which a tile of transform t finished
+// (the maximum over its tiles).
+template <int MODE, int N>
+__global__ void __launch_bounds__(kThreads, 1) mixed_gemm_group_kernel(const Args* __restrict__ targs,
+                                                                        const int4* __restrict__ items, int nitems,
+                                                                        unsigned long long* __restrict__ done) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  __shared__ Args sa;
+  const Bars B = gemm_bars<N>(sm);
+  const unsigned tmem = gemm_cta_setup<N>(B);
+  unsigned ks0 = 0, c0 = 0;
+  for (int i = blockIdx.x; i < nitems; i += gridDim.x) {
+    const int4 it = items[i];
+    if (threadIdx.x == 0) sa = targs[it.x];
+    __syncthreads();
+    if (*B.abort_flag) break;
+    TileCoord tc;
+    tc.im = it.y;
+    tc.par = it.w;
+    tc.kb = 0;
+    tc.p0 = (MODE == 0) ? it.z : 0;
+    tc.j0 = (MODE == 0) ? 0 : it.z;
+    gemm_tile<MODE, N>(sa, tc, sm, B, tmem, ks0, c0);
+    const int nks = tile_ksteps<MODE>(sa, tc);
+    ks0 += nks;
+    c0 += (nks + kChunk - 1) / kChunk;
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (done && threadIdx.x == 0) atomicMax(done + it.x, gtimer());
+  }
+  gemm_cta_teardown<N>(tmem);
 }
 
 // Table: P_l^m(x_pair) as FP32 at row seg[2 im + (l-m)%2] + (l-m)/2, column pair.
@@ -667,6 +770,56 @@ int mixed_analysis(const shtb_plan* p, const void* f, void* alm, int nf, int ltr
     zero_columns_kernel32<<<zg, 256, 0, st>>>(p->dev, (float2*)alm, a.ld_k, mlim);
     SHTB_LAUNCHED("zero fill kernel");
   }
+  return SHTB_OK;
+}
+
+// ---------------------------------------------------------------- grouped transforms
+// Host-side pieces of the persistent grouped GEMMs (uneven batches of transforms with
+// up to 8 fields each, N = 16 columns).
+
+int mixed_prepare(const shtb_plan* p, cudaStream_t st) { return ensure_table(p, st); }
+
+size_t mixed_args_bytes() { return sizeof(Args); }
+
+void mixed_fill_args(const shtb_plan* p, int mode, const void* in, void* out, int nf, void* host_args) {
+  Args a = base_args(p);
+  if (mode == 0) {
+    a.cin = (const float2*)in;
+    a.Wout = (float2*)out;
+    a.sc_mode = p->d_scale ? 1 : 0;
+  } else {
+    a.Win = (const float2*)in;
+    a.cout = (float2*)out;
+    a.sc_mode = p->d_scale ? 2 : 0;
+  }
+  a.nf = nf;
+  a.lend = a.lcap = p->lmax;
+  std::memcpy(host_args, &a, sizeof(Args));
+}
+
+int mixed_group_ksteps(const shtb_plan* p, int mode, int im, int par) {
+  const int m = im * p->mres;
+  const int J = (p->lmax >= m + par) ? (p->lmax - m - par) / 2 + 1 : 0;
+  return mode == 0 ? (J + kK - 1) / kK : (p->npair + kK - 1) / kK;
+}
+
+int mixed_group_tile_rows() { return kM; }
+
+int launch_gemm_group(int mode, const void* targs, const int4* items, int nitems, int grid, unsigned long long* done,
+                      cudaStream_t st) {
+  if (nitems <= 0) return SHTB_OK;
+  const int smem = Smem<16>::kBytes;
+  if (mode == 0) {
+    auto kern = mixed_gemm_group_kernel<0, 16>;
+    SHTB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "group gemm smem attr");
+    kern<<<grid, kThreads, smem, st>>>((const Args*)targs, items, nitems, done);
+  } else {
+    auto kern = mixed_gemm_group_kernel<1, 16>;
+    SHTB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "group gemm smem attr");
+    kern<<<grid, kThreads, smem, st>>>((const Args*)targs, items, nitems, done);
+  }
+  count_launch();
+  SHTB_TRY_CUDA(cudaGetLastError(), "group gemm launch");
   return SHTB_OK;
 }
 

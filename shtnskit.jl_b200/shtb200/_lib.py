@@ -75,6 +75,14 @@ SIGNATURES = {
     "shtb_synthesis_sphtor_adjoint": (_I, [_P, _P, _P, _P, _P, _I, _P, _SZ, _P]),
     "shtb_analysis_sphtor_adjoint": (_I, [_P, _P, _P, _P, _P, _I, _P, _SZ, _P]),
     "shtb_synthesis_noalloc": (_I, [_P, _P, _P, _I, _I, _P]),
+    "shtb_group_create": (_I, [ctypes.POINTER(_P), _P, _I, _P]),
+    "shtb_group_destroy": (_I, [_P]),
+    "shtb_group_bind": (_I, [_P, _P, _P, _P]),
+    "shtb_group_roundtrip": (_I, [_P, _P]),
+    "shtb_group_launch": (_I, [_P, _I, _P]),
+    "shtb_group_autotune": (_I, [_P, _P]),
+    "shtb_group_config": (_I, [_P, _P, _P, _P]),
+    "shtb_group_latency_ns": (_I, [_P, _P]),
     "shtb_launch_count": (ctypes.c_uint64, [_I]),
     "shtb_profile_enable": (_I, [_I]),
     "shtb_profile_read": (_I, [_I, ctypes.c_char_p, _P, _P]),

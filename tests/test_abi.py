@@ -62,3 +62,21 @@ def test_null_plan_rejected():
     assert rc == _lib.SHTB_ERR_BAD_ARG
     assert lib.shtb_workspace_bytes(None, 0, 1, 0, 0) == 0
     assert lib.shtb_plan_status(None) == _lib.SHTB_ERR_BAD_ARG
+
+
+def test_group_arguments_rejected_before_gpu():
+    lib = _lib.load()
+    h = ctypes.c_void_p()
+    assert lib.shtb_group_create(ctypes.byref(h), None, 0, None) == _lib.SHTB_ERR_BAD_ARG
+    assert "n >= 1" in lib.shtb_last_error().decode()
+    assert lib.shtb_group_destroy(None) == _lib.SHTB_OK
+    assert lib.shtb_group_roundtrip(None, None) == _lib.SHTB_ERR_BAD_ARG
+    assert lib.shtb_group_bind(None, None, None, None) == _lib.SHTB_ERR_BAD_ARG
+    assert lib.shtb_group_latency_ns(None, None) == _lib.SHTB_ERR_BAD_ARG
+
+
+def test_group_smooth_nlon_matches_oracle():
+    from shtb200.group import smooth_nlon
+    for lmax in (31, 63, 100, 255, 300, 511):
+        n = smooth_nlon(lmax)
+        assert n >= 2 * (lmax + 1) and n == so.smooth_nlon(lmax)
