@@ -12,6 +12,7 @@ Paths: "mixed" (tensor-core Legendre GEMMs, FP32 I/O) and "fp64" (plain FP64).
 The headline value is the default path; the other path is measured too.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--path mixed|fp64]
+  python bench.py --workload uneven     # 256 mixed-size roundtrips as one grouped graph launch
 
 Multi-GPU (torchrun): every rank transforms its own 64 fields (weak scaling, no
 collective in the data path); timing is the max over ranks of the device time.
@@ -51,6 +52,9 @@ def parse():
     ap.add_argument("--nfields", type=int, default=NFIELDS)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", choices=["batched", "uneven"], default="batched",
+                    help="batched: the headline 64-field lmax=1023 roundtrip; uneven: 256 roundtrips of "
+                         "mixed sizes (lmax uniform in 31..511, seed 7) as one grouped graph launch")
     return ap.parse_args()
 
 
@@ -478,9 +482,203 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------
+# uneven batches: 256 independent roundtrips of mixed sizes
+# ---------------------------------------------------------------------------
+UNEVEN_METRIC = ("transforms/s, uneven batch: 256 scalar roundtrips, lmax uniform in 31..511 (seed 7), "
+                 "nlat=lmax+1, nlon=smallest 2^a3^b5^c>=2(lmax+1), mixed precision")
+UNEVEN_UNIT = "transforms/s"
+UNEVEN_N = 256
+
+
+def uneven_lmaxes(n=UNEVEN_N, seed=7):
+    import numpy as np
+
+    return [int(v) for v in np.random.default_rng(seed).integers(31, 512, size=n)]
+
+
+def pct(v, q):
+    import numpy as np
+
+    return float(np.percentile(np.asarray(v, dtype=float), q))
+
+
+def run_uneven_reference(args):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    from shtb200.group import smooth_nlon
+
+    lm = uneven_lmaxes()[:16]
+    cores = 1
+    t_all, per = 0.0, []
+    for l in lm:
+        times, cores = cpu_sample(l, l + 1, smooth_nlon(l), 1, steps=1)
+        per.append(times[0] * 1e3)
+        t_all += times[0]
+    value = len(lm) / t_all
+    sample = f"first {len(lm)} of {UNEVEN_N} members (1 field each), one roundtrip each, sequential"
+    line = {"impl": "reference", "metric": UNEVEN_METRIC, "value": value, "unit": UNEVEN_UNIT, "n_gpus": args.gpus,
+            "steps": 1, "warmup": 0, "ms_per_step": t_all * 1e3 * UNEVEN_N / len(lm), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "uneven batch (sample)", "engine": "oracle/sht_oracle.c, POSIX threads"},
+            "latency_ms": {"p50": pct(per, 50), "p99": pct(per, 99)},
+            "cpu_baseline": {"value": value, "unit": UNEVEN_UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNEVEN_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_uneven(args):
+    import torch
+    import torch.distributed as dist
+
+    import shtb200 as sht
+    from shtb200 import _lib
+    from shtb200 import transforms as T
+    from shtb200.group import UnevenBatch, smooth_nlon
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    def max_over_ranks(v: float) -> float:
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    lib = _lib.load()
+    lmaxes = uneven_lmaxes()
+    cfgs = [sht.create_gauss_config(l, l + 1, nlon=smooth_nlon(l)) for l in lmaxes]
+    batch = UnevenBatch(cfgs, 1, local)
+    for t, (c, a) in enumerate(zip(cfgs, batch.alm_in)):
+        a.copy_(make_inputs(torch, sht, c, 1, dev, 7000 + t + 100000 * rank, torch.complex64))
+    shape = batch.autotune()
+    for _ in range(max(args.warmup, 3)):
+        batch.roundtrip()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    sampler = ClockSampler(os.environ.get("SHTB_SMI_INDEX"))
+    sampler.start()
+    time.sleep(0.3)
+    lib.shtb_launch_count(1)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        batch.roundtrip()
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    launches = int(lib.shtb_launch_count(1))
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    batch.status()
+    lat = batch.latencies_ns() / 1e6
+    err = max(float(torch.linalg.vector_norm((o - i).flatten()) / torch.linalg.vector_norm(i.flatten()))
+              for i, o in zip(batch.alm_in, batch.alm_out))
+
+    # the same 256 roundtrips launched one transform at a time (4 kernels each), back to back
+    outs = [(sht.julia_empty((c.nlat, c.nlon, 1), torch.float32, dev),
+             sht.julia_empty((c.lmax + 1, c.mmax + 1, 1), torch.complex64, dev)) for c in cfgs]
+
+    def separate(record):
+        for t, c in enumerate(cfgs):
+            if record:
+                ev[t][0].record()
+            T.synthesis_device(c, batch.alm_in[t], outs[t][0], c.lmax, _lib.SHTB_PREC_MIXED)
+            T.analysis_device(c, outs[t][0], outs[t][1], c.lmax, _lib.SHTB_PREC_MIXED)
+            if record:
+                ev[t][1].record()
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in cfgs]
+    separate(False)
+    torch.cuda.synchronize()
+    separate(True)
+    torch.cuda.synchronize()
+    sep_lat = [a.elapsed_time(b) for a, b in ev]
+    sep_total = ev[0][0].elapsed_time(ev[-1][1])
+    same = all(torch.equal(outs[t][1], batch.alm_out[t]) for t in range(len(cfgs)))
+
+    # end to end: pinned host inputs in, recovered coefficients out, every step
+    e2e = None
+    if not args.no_e2e:
+        hin = [torch.empty(a.permute(2, 1, 0).shape, dtype=torch.complex64, pin_memory=True) for a in batch.alm_in]
+        hout = [torch.empty_like(h, pin_memory=True) for h in hin]
+        for h, a in zip(hin, batch.alm_in):
+            h.copy_(a.permute(2, 1, 0).cpu())
+
+        def e2e_step():
+            for h, a in zip(hin, batch.alm_in):
+                a.permute(2, 1, 0).copy_(h, non_blocking=True)
+            batch.roundtrip()
+            for h, a in zip(hout, batch.alm_out):
+                h.copy_(a.permute(2, 1, 0), non_blocking=True)
+
+        for _ in range(2):
+            e2e_step()
+        torch.cuda.synchronize()
+        k = max(3, min(args.steps, 10))
+        e0.record()
+        for _ in range(k):
+            e2e_step()
+        e1.record()
+        torch.cuda.synchronize()
+        ems = max_over_ranks(e0.elapsed_time(e1) / k)
+        nbytes = sum(h.numel() * h.element_size() for h in hin)
+        e2e = {"value": UNEVEN_N * world * 1000.0 / ems, "unit": UNEVEN_UNIT, "h2d_bytes_per_step": nbytes,
+               "d2h_bytes_per_step": nbytes, "ms_per_step": ems}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        lm = lmaxes[:8]
+        tot, cores = 0.0, 1
+        for l in lm:
+            times, cores = cpu_sample(l, l + 1, smooth_nlon(l), 1, steps=1)
+            tot += times[0]
+        cpu = {"value": len(lm) / tot, "unit": UNEVEN_UNIT, "cores": cores, "kind": "port",
+               "sample": f"first {len(lm)} of {UNEVEN_N} members, one roundtrip each (oracle/sht_oracle.c)"}
+
+    if rank == 0:
+        line = {
+            "metric": UNEVEN_METRIC, "value": UNEVEN_N * world * 1000.0 / ms, "unit": UNEVEN_UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32-io/3xtf32-tc", "data": "synthetic",
+            "config": {"workload": f"{UNEVEN_N} independent scalar roundtrips per GPU, one field each, lmax drawn "
+                                   "uniformly from 31..511 (seed 7), Gauss grid nlat=lmax+1, smooth nlon",
+                       "launch": "persistent grouped stages in one CUDA graph (shtb_group_roundtrip)",
+                       "autotuned_shape": {"fft_pairs_per_cta": shape[0], "fft_ctas": shape[1],
+                                           "gemm_ctas": shape[2]},
+                       "l2_flush": "none; the batch (~0.3 GB of buffers) is replayed as is",
+                       "parallelism": f"batches x{world}"},
+            "latency_ms": {"grouped": {"p50": pct(lat, 50), "p99": pct(lat, 99), "max": float(lat.max())},
+                           "separate": {"p50": pct(sep_lat, 50), "p99": pct(sep_lat, 99),
+                                        "total_ms": sep_total,
+                                        "transforms_per_s": UNEVEN_N * 1000.0 / sep_total}},
+            "speedup_vs_separate": sep_total / ms, "results_equal_separate": same,
+            "accuracy": {"roundtrip_rel_l2_max": err},
+            "cpu_baseline": cpu, "clocks": clocks, "e2e": e2e, "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    batch.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.workload == "uneven":
+        if args.impl == "reference":
+            run_uneven_reference(args)
+        else:
+            run_uneven(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -13,8 +13,9 @@
 // Per-member latency: the start marker records %globaltimer; the analysis GEMM stores,
 // per member, the time its last tile finished.
 //
-// Launch-shape autotuning times every FFT shape (latitude pairs per CTA, CTAs per SM)
-// on the bound buffers and keeps the fastest; the shape changes no result.
+// Launch-shape autotuning times every FFT shape (latitude pairs per CTA; 1, 2 or 4 CTAs
+// per SM, the extra CTAs queueing behind the resident ones) on the bound buffers and
+// keeps the fastest; the shape changes no result.
 #include <algorithm>
 #include <numeric>
 #include <vector>
@@ -212,8 +213,9 @@ extern "C" int shtb_group_create(shtb_group** out, const shtb_plan* const* plans
   sort_items(ana, cana);
   g->n_syn = (int)syn.size();
   g->n_ana = (int)ana.size();
-  g->gemm_ctas_syn = std::max(1, std::min(g->nsm, g->n_syn));
-  g->gemm_ctas_ana = std::max(1, std::min(g->nsm, g->n_ana));
+  // two GEMM CTAs of 16 columns fit on an SM
+  g->gemm_ctas_syn = std::max(1, std::min(2 * g->nsm, g->n_syn));
+  g->gemm_ctas_ana = std::max(1, std::min(2 * g->nsm, g->n_ana));
   // one device allocation
   g->argsz = mixed_args_bytes();
   g->jobsz = fft_job_bytes_f32();
@@ -346,8 +348,7 @@ extern "C" int shtb_group_autotune(shtb_group* g, void* stream) {
   int bh = g->fft_h, bc = g->fft_ctas;
   for (int h : {16, 8, 4}) {
     if (group_fft_smem(g, h) > 200 * 1024) continue;
-    const int per_sm = group_fft_smem(g, h) <= 100 * 1024 ? 2 : 1;
-    for (int mult = 1; mult <= per_sm; ++mult) {
+    for (int mult : {1, 2, 4}) {
       if ((rc = set_fft_shape(g, h, g->nsm * mult))) break;
       float ms_min = 1e30f;
       for (int rep = 0; rep < 3 && !rc; ++rep) {

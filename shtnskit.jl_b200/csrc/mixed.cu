@@ -216,6 +216,11 @@ struct Smem {
   static constexpr int kBytes = kBar + (3 * kStages + 4) * 8 + 16;
 };
 
+// Narrow tiles (N = 16: up to 8 fields) leave the tensor core mostly idle, so two CTAs
+// share an SM to overlap one tile's load latency with the other's work.
+template <int N>
+constexpr int kCtasPerSm = (N <= 16) ? 2 : 1;
+
 // Coordinates of one GEMM tile: order index im, first latitude pair p0 (synthesis) or
 // first degree index j0 (analysis), parity class par, first field kb.
 struct TileCoord {
@@ -539,7 +544,7 @@ __device__ __forceinline__ void gemm_tile(const Args& a, const TileCoord& tc, un
 // One tile per CTA: blockIdx.x = 2 * tile + parity, blockIdx.y = order (synthesis),
 // blockIdx.z = block of N/2 fields.
 template <int MODE, int N>
-__global__ void __launch_bounds__(kThreads, 1) mixed_gemm_kernel(const __grid_constant__ Args a) {
+__global__ void __launch_bounds__(kThreads, kCtasPerSm<N>) mixed_gemm_kernel(const __grid_constant__ Args a) {
   extern __shared__ __align__(1024) unsigned char sm[];
   const Bars B = gemm_bars<N>(sm);
   const unsigned tmem = gemm_cta_setup<N>(B);
@@ -567,7 +572,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_gemm_kernel(const __grid_co
 // done[t] receives the %globaltimer value at which a tile of transform t finished
 // (the maximum over its tiles).
 template <int MODE, int N>
-__global__ void __launch_bounds__(kThreads, 1) mixed_gemm_group_kernel(const Args* __restrict__ targs,
+__global__ void __launch_bounds__(kThreads, kCtasPerSm<N>) mixed_gemm_group_kernel(const Args* __restrict__ targs,
                                                                         const int4* __restrict__ items, int nitems,
                                                                         unsigned long long* __restrict__ done) {
   extern __shared__ __align__(1024) unsigned char sm[];
