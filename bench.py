@@ -398,7 +398,7 @@ def run_ours(args):
                     "unit": "TFLOP/s", "peak_source": "measured cuBLAS TF32 GEMM 8192^3 on this GPU",
                     "algorithmic_per_launch": f"{issued:.4g} issued tf32 flop = 3 x {nf} fields x 4*(nlat/2)*nlm"}
             # the same launch seen from HBM: P table + coefficients + Fourier buffer
-            tab = plan.table_bytes() - base_table_bytes
+            tab = (plan.table_bytes() - base_table_bytes) / 2   # one of the two tile images
             hbm_bytes = coef_bytes + fourier_bytes + tab
             roof["hbm_view"] = {"achieved": hbm_bytes / (dom_avg_ms * 1e-3) / 1e9,
                                 "peak": peaks.get("hbm_gbs") or 6650.0, "unit": "GB/s",

@@ -71,10 +71,25 @@ struct FFTJob {
   T* g0;                                  // grid (synthesis out / analysis in), component 0
   T* g1;                                  // component 1 when ncomp == 2
   int ncomp, mlim, use_w, spow;
+  int wtile;                              // analysis: 1 = write W as GEMM B tile images (below)
+  int nf;                                 // fields of the call (B tile images)
   double scale;                           // synthesis: grid factor; analysis: weight factor
   const typename V2<T>::type* tw;
   const typename V2<T>::type* twp;
 };
+
+// B tile images of the mixed analysis GEMM: for each (order im, parity, K-step of 8
+// latitude pairs) a region of nfp x 16 floats (nfp = nf rounded up to 4, so every tile
+// has whole 8-row core-matrix groups); fields come in blocks of 64, block b holding
+// rows 2f (real) and 2f+1 (imaginary) of its fields as a K-major no-swizzle tile
+// (8 K values = 8 pairs per row), so one bulk copy fills the GEMM's B tile.
+__device__ __forceinline__ size_t btile_base(int im, int par, int p, int k, int npair, int nf) {
+  const size_t nks8 = (size_t)(npair + 7) / 8, nfp = (size_t)(nf + 3) & ~(size_t)3;
+  return (((size_t)im * 2 + par) * nks8 + (p >> 3)) * nfp * 16 + (size_t)(k >> 6) * 1024;
+}
+__device__ __forceinline__ int btile_off(int row, int kk) {
+  return (row >> 3) * 64 + (kk >> 2) * 32 + (row & 7) * 4 + (kk & 3);
+}
 
 // Latitude pairs p0 .. p0+H-1 of field k.
 template <typename T, int H, bool GENERIC>
@@ -274,9 +289,35 @@ __device__ __forceinline__ void fft_ana_body(const FFTJob<T>& J, int p0, int k, 
     XN.x = sum.x * (T)0.5; XN.y = sum.y * (T)0.5;
     XS.x = d.y * (T)0.5;   XS.y = -d.x * (T)0.5;
     const T wt = wfac[h];
-    const size_t base = ((size_t)k * P.nm + im) * 2 * npair + p0 + h;
-    W[base] = cscale(cadd(XN, XS), wt);
-    W[base + npair] = cscale(csub(XN, XS), wt);
+    const V E = cscale(cadd(XN, XS), wt), O = cscale(csub(XN, XS), wt);
+    if (J.wtile) {
+      T* Wf = reinterpret_cast<T*>(W);
+      const int p = p0 + h;
+      const size_t b0 = btile_base(im, 0, p, k, npair, J.nf), b1 = btile_base(im, 1, p, k, npair, J.nf);
+      const int kk = p & 7, fl = k & 63;
+      Wf[b0 + btile_off(2 * fl, kk)] = E.x;
+      Wf[b0 + btile_off(2 * fl + 1, kk)] = E.y;
+      Wf[b1 + btile_off(2 * fl, kk)] = O.x;
+      Wf[b1 + btile_off(2 * fl + 1, kk)] = O.y;
+    } else {
+      const size_t base = ((size_t)k * P.nm + im) * 2 * npair + p0 + h;
+      W[base] = E;
+      W[base + npair] = O;
+    }
+  }
+  if (J.wtile && p0 <= npair - 1 && npair - 1 < p0 + H) {
+    // the block holding the last pair also zeroes the padding pairs npair .. npair8-1
+    T* Wf = reinterpret_cast<T*>(W);
+    const int pad = ((npair + 7) & ~7) - npair;
+    for (int idx = threadIdx.x; idx < nmu * pad; idx += blockDim.x) {
+      const int im = idx / pad, p = npair + idx - im * pad;
+      const int kk = p & 7, fl = k & 63;
+      for (int par = 0; par < 2; ++par) {
+        const size_t b = btile_base(im, par, p, k, npair, J.nf);
+        Wf[b + btile_off(2 * fl, kk)] = (T)0;
+        Wf[b + btile_off(2 * fl + 1, kk)] = (T)0;
+      }
+    }
   }
 }
 
@@ -315,7 +356,7 @@ __global__ void __launch_bounds__(512) fft_group_kernel(const FFTJob<T>* __restr
 template <typename T>
 static FFTJob<T> fft_job(const shtb_plan* p, const int* perm, const typename V2<T>::type* Win,
                          typename V2<T>::type* Wout, T* g0, T* g1, int ncomp, int mlim, double scale, int use_w,
-                         int spow) {
+                         int spow, int wtile = 0, int nf = 0) {
   using V = typename V2<T>::type;
   FFTJob<T> J;
   J.P = p->dev;
@@ -329,6 +370,8 @@ static FFTJob<T> fft_job(const shtb_plan* p, const int* perm, const typename V2<
   J.mlim = mlim;
   J.use_w = use_w;
   J.spow = spow;
+  J.wtile = wtile;
+  J.nf = nf;
   J.scale = scale;
   J.tw = std::is_same<T, double>::value ? (const V*)p->d_tw64 : (const V*)p->d_tw32;
   J.twp = std::is_same<T, double>::value ? (const V*)p->d_twp64 : (const V*)p->d_twp32;
@@ -378,7 +421,7 @@ static int launch_syn_h(const shtb_plan* p, const void* W, T* out0, T* out1, int
 
 template <typename T, int H>
 static int launch_ana_h(const shtb_plan* p, const T* in0, const T* in1, int ncomp, void* W, int nfw, int mlim,
-                        double wscale, int use_w, int spow, cudaStream_t st) {
+                        double wscale, int use_w, int spow, int wtile, cudaStream_t st) {
   using V = typename V2<T>::type;
   const size_t smem = fft_smem(p->fft, sizeof(V), H);
   if (smem > 227 * 1024) return set_error(SHTB_ERR_UNSUPPORTED, "nlon too large for the shared-memory FFT");
@@ -386,7 +429,7 @@ static int launch_ana_h(const shtb_plan* p, const T* in0, const T* in1, int ncom
   SHTB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "fft smem attr");
   dim3 grid((p->npair + H - 1) / H, nfw);
   const FFTJob<T> J = fft_job<T>(p, p->d_rev, nullptr, (V*)W, const_cast<T*>(in0), const_cast<T*>(in1), ncomp, mlim,
-                                 wscale, use_w, spow);
+                                 wscale, use_w, spow, wtile, nfw);
   prof_begin(st);
   kern<<<grid, 512, smem, st>>>(J);
   SHTB_LAUNCHED("fft analysis kernel");
@@ -408,21 +451,21 @@ int launch_fft_syn(const shtb_plan* p, const void* W, GT* out0, GT* out1, int nc
 
 template <typename T, typename GT>
 int launch_fft_ana(const shtb_plan* p, const GT* in0, const GT* in1, int ncomp, void* W, int nfw, int mlim,
-                   double wscale, int use_w, int spow, cudaStream_t st) {
+                   double wscale, int use_w, int spow, cudaStream_t st, int wtile) {
   static_assert(std::is_same<T, GT>::value, "grid and compute types match");
   switch (fft_pick_h(p->fft, sizeof(typename V2<T>::type), p->npair)) {
-    case 16: return launch_ana_h<T, 16>(p, in0, in1, ncomp, W, nfw, mlim, wscale, use_w, spow, st);
-    case 8: return launch_ana_h<T, 8>(p, in0, in1, ncomp, W, nfw, mlim, wscale, use_w, spow, st);
-    case 4: return launch_ana_h<T, 4>(p, in0, in1, ncomp, W, nfw, mlim, wscale, use_w, spow, st);
-    case 2: return launch_ana_h<T, 2>(p, in0, in1, ncomp, W, nfw, mlim, wscale, use_w, spow, st);
-    default: return launch_ana_h<T, 1>(p, in0, in1, ncomp, W, nfw, mlim, wscale, use_w, spow, st);
+    case 16: return launch_ana_h<T, 16>(p, in0, in1, ncomp, W, nfw, mlim, wscale, use_w, spow, wtile, st);
+    case 8: return launch_ana_h<T, 8>(p, in0, in1, ncomp, W, nfw, mlim, wscale, use_w, spow, wtile, st);
+    case 4: return launch_ana_h<T, 4>(p, in0, in1, ncomp, W, nfw, mlim, wscale, use_w, spow, wtile, st);
+    case 2: return launch_ana_h<T, 2>(p, in0, in1, ncomp, W, nfw, mlim, wscale, use_w, spow, wtile, st);
+    default: return launch_ana_h<T, 1>(p, in0, in1, ncomp, W, nfw, mlim, wscale, use_w, spow, wtile, st);
   }
 }
 
 template int launch_fft_syn<double, double>(const shtb_plan*, const void*, double*, double*, int, int, int, double, int, int, cudaStream_t);
-template int launch_fft_ana<double, double>(const shtb_plan*, const double*, const double*, int, void*, int, int, double, int, int, cudaStream_t);
+template int launch_fft_ana<double, double>(const shtb_plan*, const double*, const double*, int, void*, int, int, double, int, int, cudaStream_t, int);
 template int launch_fft_syn<float, float>(const shtb_plan*, const void*, float*, float*, int, int, int, double, int, int, cudaStream_t);
-template int launch_fft_ana<float, float>(const shtb_plan*, const float*, const float*, int, void*, int, int, double, int, int, cudaStream_t);
+template int launch_fft_ana<float, float>(const shtb_plan*, const float*, const float*, int, void*, int, int, double, int, int, cudaStream_t, int);
 
 // ---------------------------------------------------------------- grouped transforms
 // Host-side pieces of the persistent grouped FP32 FFTs.
@@ -434,8 +477,7 @@ void fft_fill_job_f32(const shtb_plan* p, int syn, const void* W, void* grid, in
   FFTJob<float> J = syn ? fft_job<float>(p, p->d_rinv, (const float2*)W, nullptr, (float*)grid, nullptr, 1, mlim,
                                          p->phi_inv_scale / p->nlon, 0, 0)
                         : fft_job<float>(p, p->d_rev, nullptr, (float2*)const_cast<void*>(W), (float*)grid, nullptr, 1,
-                                         mlim, p->ana_scale, 1, 0);
-  (void)nf;
+                                         mlim, p->ana_scale, 1, 0, 1, nf);
   std::memcpy(host_job, &J, sizeof(J));
 }
 

@@ -228,7 +228,9 @@ extern "C" int shtb_group_create(shtb_group** out, const shtb_plan* const* plans
   size_t wbytes = 0;
   for (int t = 0; t < n; ++t) {
     g->woff[t] = wbytes;
-    wbytes = align256(wbytes + (size_t)g->nf[t] * plans[t]->nm * 2 * plans[t]->npair * sizeof(float2));
+    // pairs padded to 8 and fields to 4: the analysis FFT writes the GEMM's B tile images
+    const size_t np8 = (size_t)(plans[t]->npair + 7) / 8 * 8, nfp = (size_t)(g->nf[t] + 3) / 4 * 4;
+    wbytes = align256(wbytes + nfp * plans[t]->nm * 2 * np8 * sizeof(float2));
   }
   const size_t o_w = take(wbytes);
   cudaError_t e = cudaMalloc(&g->dmem, o);

@@ -102,7 +102,8 @@ struct shtb_plan {
   int* d_err = nullptr;                   // device status word (bounded waits that gave up)
   // mixed-precision path: FP32 table of P_l^m grouped by (m, parity), built on first use
   std::mutex tab_mu;
-  float* d_tab = nullptr;
+  float* d_tab = nullptr;                 // synthesis tile images (start of the table allocation)
+  float* d_tab_ana = nullptr;             // analysis tile images
   const long long* d_tab_seg = nullptr;
   size_t tab_bytes = 0;
   int npp = 0;

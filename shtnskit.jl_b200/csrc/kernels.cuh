@@ -33,9 +33,10 @@ struct Factors {
 template <typename T, typename GT>
 int launch_fft_syn(const shtb_plan* p, const void* W, GT* out0, GT* out1, int ncomp, int nfw, int mlim,
                    double gscale, int use_w, int spow, cudaStream_t st);
+// wtile = 1 writes W as the mixed analysis GEMM's B tile images (FP32 only).
 template <typename T, typename GT>
 int launch_fft_ana(const shtb_plan* p, const GT* in0, const GT* in1, int ncomp, void* W, int nfw, int mlim,
-                   double wscale, int use_w, int spow, cudaStream_t st);
+                   double wscale, int use_w, int spow, cudaStream_t st, int wtile = 0);
 
 int launch_leg_syn64(const shtb_plan* p, const CoefSrc& src, const Factors& F, void* W, int nf, int row_end,
                      int mlim, cudaStream_t st);

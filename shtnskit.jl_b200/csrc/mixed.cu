@@ -8,15 +8,21 @@
 // nearest TF32): x*y ~ hi_x hi_y + hi_x lo_y + lo_x hi_y.
 //
 // P comes from a per-plan FP32 table of P_l^m(x_pair), l = m..lmax+1, grouped by
-// (m, parity) as rows of padded latitude pairs. The table is written once by
+// (m, parity) into segments of R rows (degrees, padded to a multiple of 8) by npp
+// latitude pairs (padded to a multiple of 128). The table is written once by
 // mixed_table_kernel from the FP64 recurrence (extended-range seeds and FP64
-// recurrence coefficients), so every P value is the FP64 result rounded once.
+// recurrence coefficients), so every P value is the FP64 result rounded once. It is
+// stored twice, as the byte images of the A tiles the two GEMMs load, so one bulk
+// copy (cp.async.bulk, completing on an mbarrier) fills a stage's A tile: synthesis
+// tiles are 128 pairs x 8 degrees, analysis tiles 128 degrees x 8 pairs, both in the
+// K-major no-swizzle core-matrix order of the MMA descriptors.
 //
-// CTA organisation (544 threads, one parity class per CTA): warps 0-3 copy
-// operands with cp.async straight into K-major tiles (no swizzle) of an 8-stage
-// shared-memory ring, up to 8 K-steps ahead; warps 4-7 round each landed stage in
-// place to TF32 hi and write the lo remainders; warp 8 allocates TMEM and one of its threads issues the
-// MMAs (tcgen05.commit releases each stage). The tensor core accumulates the
+// CTA organisation (544 threads, one parity class per CTA): warps 0-3 fill an 8- to
+// 16-stage shared-memory ring of K-major tiles (no swizzle), that many K-steps ahead:
+// bulk copies of the A tile images (and of the analysis B tile images) plus cp.async
+// gathers of the synthesis coefficients; warps 4-7 round each landed stage in place to
+// TF32 hi and write the lo remainders; warp 8 allocates TMEM and one of its threads
+// issues the MMAs (tcgen05.commit releases each stage). The tensor core accumulates the
 // hi*hi products of only kChunk K-steps into one of two TMEM buffers; warps 9-16
 // drain each finished chunk with tcgen05.ld into round-to-nearest FP32 register
 // sums. Long accumulation chains inside the tensor core round toward zero and
@@ -35,7 +41,6 @@ namespace mx {
 
 constexpr int kM = 128;          // UMMA M
 constexpr int kK = 8;            // TF32 K per instruction
-constexpr int kStages = 8;
 constexpr int kChunk = 4;          // K-steps accumulated in TMEM before promotion
 constexpr int kThreads = 544;       // 8 producer warps, 1 MMA warp, 8 promotion warps
 constexpr int kTileBytesA = kM * kK * 4;  // 4 KB
@@ -43,7 +48,7 @@ constexpr unsigned long long kWaitNs = 2000000000ull;
 
 struct Args {
   PlanDev P;
-  const float* tab;
+  const float* tab;          // tile images of this direction (synthesis or analysis)
   const long long* seg;      // [2*nm+1] first table row of segment (im, parity); rows hold npp pairs
   int npp;
   const float2* cin;         // synthesis: coefficients; analysis: unused
@@ -180,6 +185,17 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src, bool ok) 
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src), "r"(ok ? 16 : 0)
                : "memory");
 }
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// Bulk copy global -> this CTA's shared memory (no multicast), completing on bar.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
 // Arrive on bar once every cp.async this thread issued so far has landed (the barrier's
 // expected count includes this arrival).
 __device__ __forceinline__ void cp_async_arrive_noinc(unsigned long long* bar) {
@@ -212,8 +228,12 @@ struct Smem {
   static constexpr int kTileB = N * kK * 4;
   // per stage: A_hi, A_lo, B_hi, B_lo (one parity class per CTA)
   static constexpr int kStage = 2 * kTileBytesA + 2 * kTileB;
-  static constexpr int kBar = kStages * kStage;
-  static constexpr int kBytes = kBar + (3 * kStages + 4) * 8 + 16;
+  // Ring depth: enough stages in flight to cover the global-memory latency of the
+  // stage copies (12 x 16 KB for N = 128); the 16-column tiles keep 8 so that two CTAs
+  // share an SM.
+  static constexpr int kSt = (N == 128) ? 12 : (N == 16) ? 8 : 16;
+  static constexpr int kBar = kSt * kStage;
+  static constexpr int kBytes = kBar + (3 * kSt + 4) * 8 + 16;
 };
 
 // Narrow tiles (N = 16: up to 8 fields) leave the tensor core mostly idle, so two CTAs
@@ -236,12 +256,12 @@ struct Bars {
 
 template <int N>
 __device__ __forceinline__ Bars gemm_bars(unsigned char* sm) {
-  using S = Smem<N>;
+  using S = Smem<N>;  // barriers follow the stage ring
   Bars B;
   B.full = reinterpret_cast<unsigned long long*>(sm + S::kBar);
-  B.empty = B.full + kStages;
-  B.ldfull = B.empty + kStages;   // [kStages] loader copies of the stage landed
-  B.accf = B.ldfull + kStages;    // [2] chunk accumulated in TMEM buffer b
+  B.empty = B.full + S::kSt;
+  B.ldfull = B.empty + S::kSt;    // [kSt] loader copies of the stage landed
+  B.accf = B.ldfull + S::kSt;     // [2] chunk accumulated in TMEM buffer b
   B.acce = B.accf + 2;            // [2] TMEM buffer b drained by the promotion warps
   B.tmem_slot = reinterpret_cast<unsigned*>(B.acce + 2);
   B.abort_flag = reinterpret_cast<volatile int*>(B.tmem_slot + 1);
@@ -261,10 +281,10 @@ template <int N>
 __device__ __forceinline__ unsigned gemm_cta_setup(const Bars& B) {
   const int tid = threadIdx.x, warp = tid >> 5;
   if (tid == 0) {
-    for (int s = 0; s < kStages; ++s) {
+    for (int s = 0; s < Smem<N>::kSt; ++s) {
       mbar_init(&B.full[s], 128);
       mbar_init(&B.empty[s], 1);
-      mbar_init(&B.ldfull[s], 128);
+      mbar_init(&B.ldfull[s], 129);   // 128 loader cp.async arrivals + the A bulk copy's expect_tx
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&B.accf[b], 1);
@@ -325,8 +345,8 @@ __device__ __forceinline__ void gemm_tile(const Args& a, const TileCoord& tc, un
   if (warp < 8) {
     // ------------------------------------------------------------- producers
     // Warps 0-3 (loaders) copy the operands of every K-step with cp.async straight into
-    // their K-major slots of the hi tiles of stage ks % kStages and signal completion on
-    // ldfull with cp.async.mbarrier.arrive, running up to kStages K-steps ahead. Warps 4-7
+    // their K-major slots of the hi tiles of stage ks % kSt and signal completion on
+    // ldfull with cp.async.mbarrier.arrive, running up to kSt K-steps ahead. Warps 4-7
     // (splitters) round each landed stage in place to TF32, write the remainders into the
     // lo tiles, and release the stage to the MMA issuer. Keeping the two roles in separate
     // threads means a splitter's proxy fence never waits for copies still in flight.
@@ -353,25 +373,36 @@ __device__ __forceinline__ void gemm_tile(const Args& a, const TileCoord& tc, un
         kstep = 16;
       }
       unsigned char* bdst0 = sm + 2 * kTileBytesA + tile_off(2 * fl0 + bc, bk >> 2) + (bk & 3) * 4;
-      // A copies
-      const float* a0 = (MODE == 0) ? a.tab + sg * a.npp + p0 + t : a.tab + (sg + j0 + t) * a.npp;
-      const bool arow_ok = (MODE == 0) || (j0 + t < ln);
+      // A tile images: synthesis [ptile][ks] blocks of 4 KB after the segment start;
+      // analysis [jtile][ks] blocks of rows*32 bytes (rows = 128, fewer in the last jtile)
+      const float* aseg = a.tab + sg * a.npp;
+      const int arows = (MODE == 0) ? kM : min(kM, (int)ln - j0);
+      const float* a0 = (MODE == 0) ? aseg + (long long)(p0 / kM) * (ln / kK) * (kM * kK) : aseg + (long long)j0 * a.npp;
+      const unsigned abytes = (unsigned)arows * kK * 4;
+      // analysis B: tile images written by the FFT, region (im, par, ks) of nfp x 16 floats
+      // (nfp = nf rounded up to 4), this CTA's block of 64 fields at kb / 64 * 1024 floats
+      const int nks8 = (npair + kK - 1) / kK, nfp = (a.nf + 3) & ~3;
+      const float* bimg = reinterpret_cast<const float*>(a.Win) +
+                          ((long long)(im * 2 + par) * nks8) * nfp * 16 + (long long)(kb >> 6) * 1024;
+      const unsigned bbytes = (unsigned)min(64, nfp - kb) * 64;
       for (int ks = 0; ks < nks; ++ks) {
         const unsigned g = ks0 + ks;
-        const int b = g % kStages;
-        if (g >= kStages && !mbar_wait(&empty[b], ((g / kStages) - 1) & 1, abort_flag, a.err)) break;
+        const int b = g % S::kSt;
+        if (g >= S::kSt && !mbar_wait(&empty[b], ((g / S::kSt) - 1) & 1, abort_flag, a.err)) break;
         unsigned char* st = sm + (size_t)b * S::kStage;
-        if (MODE == 0) {
-#pragma unroll
-          for (int k = 0; k < kK; ++k) {
-            const int j = ks * kK + k;
-            const bool ok = j < ln;
-            cp_async4(st + tile_off(t, k >> 2) + (k & 3) * 4, ok ? a0 + (long long)j * a.npp : a.tab, ok);
+        if (MODE == 1) {
+          // A and B tile images, both by bulk copy
+          if (t == 0) {
+            mbar_expect_tx(&ldfull[b], abytes + bbytes);
+            bulk_g2s(st, a0 + (long long)ks * arows * kK, abytes, &ldfull[b]);
+            bulk_g2s(st + 2 * kTileBytesA, bimg + (long long)ks * nfp * 16, bbytes, &ldfull[b]);
           }
-        } else {
-          const float* src = a0 + ks * kK;
-          cp_async16(st + tile_off(t, 0), arow_ok ? src : a.tab, arow_ok);
-          cp_async16(st + tile_off(t, 1), arow_ok ? src + 4 : a.tab, arow_ok);
+          cp_async_arrive_noinc(&ldfull[b]);
+          continue;
+        }
+        if (t == 0) {
+          mbar_expect_tx(&ldfull[b], abytes);
+          bulk_g2s(st, a0 + (long long)ks * arows * kK, abytes, &ldfull[b]);
         }
         const bool kok = ks * kK + bk < Jc;
         const float* bs = b0 + ks * kstep;
@@ -393,8 +424,8 @@ __device__ __forceinline__ void gemm_tile(const Args& a, const TileCoord& tc, un
       const bool scaled = (MODE == 0) && (a.sc_mode || a.mf0 != 1.f || a.mf1 != 1.f);
       for (int ks = 0; ks < nks; ++ks) {
         const unsigned g = ks0 + ks;
-        const int b = g % kStages;
-        if (!mbar_wait(&ldfull[b], (g / kStages) & 1, abort_flag, a.err)) break;
+        const int b = g % S::kSt;
+        if (!mbar_wait(&ldfull[b], (g / S::kSt) & 1, abort_flag, a.err)) break;
         unsigned char* st = sm + (size_t)b * S::kStage;
         unsigned char* Ah = st;
         unsigned char* Al = st + kTileBytesA;
@@ -451,8 +482,8 @@ __device__ __forceinline__ void gemm_tile(const Args& a, const TileCoord& tc, un
         const int k1 = min(nks, (c + 1) * kChunk);
         for (int ks = c * kChunk; ks < k1; ++ks) {
           const unsigned g = ks0 + ks;
-          const int b = g % kStages;
-          if (!mbar_wait(&full[b], (g / kStages) & 1, abort_flag, a.err)) {
+          const int b = g % S::kSt;
+          if (!mbar_wait(&full[b], (g / S::kSt) & 1, abort_flag, a.err)) {
             ok = false;
             break;
           }
@@ -603,8 +634,10 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm<N>) mixed_gemm_group_kern
   gemm_cta_teardown<N>(tmem);
 }
 
-// Table: P_l^m(x_pair) as FP32 at row seg[2 im + (l-m)%2] + (l-m)/2, column pair.
-__global__ void mixed_table_kernel(PlanDev P, float* __restrict__ tab, const long long* __restrict__ seg, int npp) {
+// Table: P_l^m(x_pair) as FP32, degree row j = (l-m)/2 of segment (im, (l-m)%2), written
+// into both tile images (layout described at the top of this file).
+__global__ void mixed_table_kernel(PlanDev P, float* __restrict__ tabS, float* __restrict__ tabA,
+                                   const long long* __restrict__ seg, int npp) {
   const int pair = blockIdx.x * blockDim.x + threadIdx.x;
   const int im = blockIdx.y;
   if (pair >= P.npair) return;
@@ -613,6 +646,7 @@ __global__ void mixed_table_kernel(PlanDev P, float* __restrict__ tab, const lon
   const double x = P.x[pair];
   const int l0 = P.l0[(size_t)im * P.npair + pair];
   const double2 r01 = P.r01[(size_t)im * P.npair + pair];
+  const int pt = pair / kM, pr = pair % kM, pk = pair % kK, pks = pair / kK;
   double ra = 0.0, rb = 0.0;
   for (int l = m; l <= P.lrec; ++l) {
     double r;
@@ -625,7 +659,17 @@ __global__ void mixed_table_kernel(PlanDev P, float* __restrict__ tab, const lon
     rb = ra;
     ra = r;
     const int par = (l - m) & 1, j = (l - m) >> 1;
-    tab[(seg[2 * im + par] + j) * npp + pair] = (float)(P.cfac[poff + (l - m)] * r);
+    const long long sg = seg[2 * im + par];
+    const int R = (int)(seg[2 * im + par + 1] - sg);
+    const float v = (float)(P.cfac[poff + (l - m)] * r);
+    // synthesis: tile (pt, j/8), row pr, K slot j%8
+    const int k = j % kK;
+    tabS[sg * npp + ((long long)pt * (R / kK) + j / kK) * (kM * kK) + (pr >> 3) * 64 + (k >> 2) * 32 + (pr & 7) * 4 +
+         (k & 3)] = v;
+    // analysis: tile (j/128, pair/8) of rows = min(128, R - 128 (j/128)), row j%128, K slot pair%8
+    const int jt = j / kM, rr = j % kM, rows = min(kM, R - jt * kM);
+    tabA[sg * npp + (long long)jt * kM * npp + (long long)pks * rows * kK + (rr >> 3) * 64 + (pk >> 2) * 32 +
+         (rr & 7) * 4 + (pk & 3)] = v;
   }
 }
 
@@ -650,20 +694,21 @@ static int ensure_table(const shtb_plan* cp, cudaStream_t st) {
     }
   }
   p->htab_seg[2 * nm] = rows;
-  const size_t tb = (size_t)rows * p->npp * 4;
+  const size_t tb = (size_t)rows * p->npp * 4;   // one image
   void* mem = nullptr;
-  cudaError_t e = cudaMalloc(&mem, tb + (2 * nm + 1) * 8 + 256);
+  cudaError_t e = cudaMalloc(&mem, 2 * tb + (2 * nm + 1) * 8 + 256);
   if (e != cudaSuccess) return set_error(SHTB_ERR_OOM, std::string("mixed table: ") + cudaGetErrorString(e));
   float* tab = (float*)mem;
-  long long* dseg = (long long*)((char*)mem + (tb + 255) / 256 * 256);
+  float* taba = (float*)((char*)mem + tb);
+  long long* dseg = (long long*)((char*)mem + (2 * tb + 255) / 256 * 256);
   e = cudaMemcpyAsync(dseg, p->htab_seg.data(), (2 * nm + 1) * 8, cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(tab, 0, tb, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(tab, 0, 2 * tb, st);
   if (e != cudaSuccess) {
     cudaFree(mem);
     return set_error(SHTB_ERR_CUDA, std::string("mixed table init: ") + cudaGetErrorString(e));
   }
   dim3 grid((p->npair + 127) / 128, nm);
-  mixed_table_kernel<<<grid, 128, 0, st>>>(p->dev, tab, dseg, p->npp);
+  mixed_table_kernel<<<grid, 128, 0, st>>>(p->dev, tab, taba, dseg, p->npp);
   count_launch();
   e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -672,8 +717,9 @@ static int ensure_table(const shtb_plan* cp, cudaStream_t st) {
     return set_error(SHTB_ERR_CUDA, std::string("mixed table kernel: ") + cudaGetErrorString(e));
   }
   p->d_tab = tab;
+  p->d_tab_ana = taba;
   p->d_tab_seg = dseg;
-  p->tab_bytes = tb;
+  p->tab_bytes = 2 * tb;
   return SHTB_OK;
 }
 
@@ -739,7 +785,7 @@ int mixed_analysis(const shtb_plan* p, const void* f, void* alm, int nf, int ltr
   int rc = ensure_table(p, st);
   if (rc) return rc;
   const int mlim = std::min(p->mmax, ltr);
-  if ((rc = launch_fft_ana<float, float>(p, (const float*)f, nullptr, 1, work, nf, mlim, p->ana_scale, 1, 0, st)))
+  if ((rc = launch_fft_ana<float, float>(p, (const float*)f, nullptr, 1, work, nf, mlim, p->ana_scale, 1, 0, st, 1)))
     return rc;
   // analysis tiles: 128 degrees of each parity per tile
   std::vector<int2>& tl = const_cast<shtb_plan*>(p)->hmx_tiles;
@@ -760,6 +806,7 @@ int mixed_analysis(const shtb_plan* p, const void* f, void* alm, int nf, int ltr
     pm->mx_tiles_key = key;
   }
   Args a = base_args(p);
+  a.tab = p->d_tab_ana;
   a.Win = (const float2*)work;
   a.cout = (float2*)alm;
   a.sc_mode = p->d_scale ? 2 : 0;
@@ -793,6 +840,7 @@ void mixed_fill_args(const shtb_plan* p, int mode, const void* in, void* out, in
     a.Wout = (float2*)out;
     a.sc_mode = p->d_scale ? 1 : 0;
   } else {
+    a.tab = p->d_tab_ana;
     a.Win = (const float2*)in;
     a.cout = (float2*)out;
     a.sc_mode = p->d_scale ? 2 : 0;

@@ -145,6 +145,8 @@ using namespace shtb;
 // validation and workspace
 // ---------------------------------------------------------------------------
 static size_t wbytes_fourier(const shtb_plan* p, int nfw, size_t celem) {
+  // the mixed path's analysis writes B tile images: latitude pairs padded to 8, fields to 4
+  if (celem == 8) return (size_t)((nfw + 3) / 4 * 4) * p->nm * 2 * ((p->npair + 7) / 8 * 8) * celem;
   return (size_t)nfw * p->nm * 2 * p->npair * celem;
 }
 static size_t align256(size_t v) { return (v + 255) / 256 * 256; }
