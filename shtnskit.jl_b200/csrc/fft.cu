@@ -71,24 +71,19 @@ struct FFTJob {
   T* g0;                                  // grid (synthesis out / analysis in), component 0
   T* g1;                                  // component 1 when ncomp == 2
   int ncomp, mlim, use_w, spow;
-  int wtile;                              // analysis: 1 = write W as GEMM B tile images (below)
-  int nf;                                 // fields of the call (B tile images)
+  int wtile;                              // analysis: 1 = write W as the GEMM's B tile images,
+  int nf;                                 //   TF32 hi at W and lo at W + wlo (floats), nf fields
+  size_t wlo;
   double scale;                           // synthesis: grid factor; analysis: weight factor
   const typename V2<T>::type* tw;
   const typename V2<T>::type* twp;
 };
 
-// B tile images of the mixed analysis GEMM: for each (order im, parity, K-step of 8
-// latitude pairs) a region of nfp x 16 floats (nfp = nf rounded up to 4, so every tile
-// has whole 8-row core-matrix groups); fields come in blocks of 64, block b holding
-// rows 2f (real) and 2f+1 (imaginary) of its fields as a K-major no-swizzle tile
-// (8 K values = 8 pairs per row), so one bulk copy fills the GEMM's B tile.
+// Analysis B tile images: region (im, parity, K-step of 8 latitude pairs) =
+// ((im * 2 + par) * nks8 + p / 8); field k in block k / 64 (see btile_off).
 __device__ __forceinline__ size_t btile_base(int im, int par, int p, int k, int npair, int nf) {
-  const size_t nks8 = (size_t)(npair + 7) / 8, nfp = (size_t)(nf + 3) & ~(size_t)3;
-  return (((size_t)im * 2 + par) * nks8 + (p >> 3)) * nfp * 16 + (size_t)(k >> 6) * 1024;
-}
-__device__ __forceinline__ int btile_off(int row, int kk) {
-  return (row >> 3) * 64 + (kk >> 2) * 32 + (row & 7) * 4 + (kk & 3);
+  const size_t nks8 = (size_t)(npair + 7) / 8;
+  return (((size_t)im * 2 + par) * nks8 + (p >> 3)) * (size_t)btile_nfp(nf) * 16 + (size_t)(k >> 6) * 1024;
 }
 
 // Latitude pairs p0 .. p0+H-1 of field k.
@@ -291,14 +286,19 @@ __device__ __forceinline__ void fft_ana_body(const FFTJob<T>& J, int p0, int k, 
     const T wt = wfac[h];
     const V E = cscale(cadd(XN, XS), wt), O = cscale(csub(XN, XS), wt);
     if (J.wtile) {
-      T* Wf = reinterpret_cast<T*>(W);
+      float* Wf = reinterpret_cast<float*>(W);
       const int p = p0 + h;
       const size_t b0 = btile_base(im, 0, p, k, npair, J.nf), b1 = btile_base(im, 1, p, k, npair, J.nf);
       const int kk = p & 7, fl = k & 63;
-      Wf[b0 + btile_off(2 * fl, kk)] = E.x;
-      Wf[b0 + btile_off(2 * fl + 1, kk)] = E.y;
-      Wf[b1 + btile_off(2 * fl, kk)] = O.x;
-      Wf[b1 + btile_off(2 * fl + 1, kk)] = O.y;
+      const float v[4] = {(float)E.x, (float)E.y, (float)O.x, (float)O.y};
+      const size_t o[4] = {b0 + btile_off(2 * fl, kk), b0 + btile_off(2 * fl + 1, kk), b1 + btile_off(2 * fl, kk),
+                           b1 + btile_off(2 * fl + 1, kk)};
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const float hi = tf32_round(v[q]);
+        Wf[o[q]] = hi;
+        Wf[J.wlo + o[q]] = tf32_round(v[q] - hi);
+      }
     } else {
       const size_t base = ((size_t)k * P.nm + im) * 2 * npair + p0 + h;
       W[base] = E;
@@ -307,15 +307,17 @@ __device__ __forceinline__ void fft_ana_body(const FFTJob<T>& J, int p0, int k, 
   }
   if (J.wtile && p0 <= npair - 1 && npair - 1 < p0 + H) {
     // the block holding the last pair also zeroes the padding pairs npair .. npair8-1
-    T* Wf = reinterpret_cast<T*>(W);
+    float* Wf = reinterpret_cast<float*>(W);
     const int pad = ((npair + 7) & ~7) - npair;
     for (int idx = threadIdx.x; idx < nmu * pad; idx += blockDim.x) {
       const int im = idx / pad, p = npair + idx - im * pad;
       const int kk = p & 7, fl = k & 63;
       for (int par = 0; par < 2; ++par) {
         const size_t b = btile_base(im, par, p, k, npair, J.nf);
-        Wf[b + btile_off(2 * fl, kk)] = (T)0;
-        Wf[b + btile_off(2 * fl + 1, kk)] = (T)0;
+        for (int c = 0; c < 2; ++c) {
+          Wf[b + btile_off(2 * fl + c, kk)] = 0.f;
+          Wf[J.wlo + b + btile_off(2 * fl + c, kk)] = 0.f;
+        }
       }
     }
   }
@@ -353,6 +355,11 @@ __global__ void __launch_bounds__(512) fft_group_kernel(const FFTJob<T>* __restr
   }
 }
 
+// Floats of one analysis B tile image (the lo image follows the hi image).
+size_t fft_btile_floats(const shtb_plan* p, int nf) {
+  return (size_t)p->nm * 2 * ((p->npair + 7) / 8) * btile_nfp(nf) * 16;
+}
+
 template <typename T>
 static FFTJob<T> fft_job(const shtb_plan* p, const int* perm, const typename V2<T>::type* Win,
                          typename V2<T>::type* Wout, T* g0, T* g1, int ncomp, int mlim, double scale, int use_w,
@@ -372,6 +379,7 @@ static FFTJob<T> fft_job(const shtb_plan* p, const int* perm, const typename V2<
   J.spow = spow;
   J.wtile = wtile;
   J.nf = nf;
+  J.wlo = wtile ? fft_btile_floats(p, nf) : 0;
   J.scale = scale;
   J.tw = std::is_same<T, double>::value ? (const V*)p->d_tw64 : (const V*)p->d_tw32;
   J.twp = std::is_same<T, double>::value ? (const V*)p->d_twp64 : (const V*)p->d_twp32;

@@ -1,14 +1,15 @@
 // group.cu — uneven batches: many independent mixed-precision scalar transforms, each
 // with its own plan (lmax, Gauss grid, nlon) and 1..8 fields, run as four persistent
-// launches (order-GEMM synthesis, FFT synthesis, FFT analysis, order-GEMM analysis).
+// launches (B packing, order-GEMM synthesis, FFT synthesis, FFT analysis, order-GEMM
+// analysis).
 //
 // Every stage owns a list of work items over all members — GEMM tiles (member, order,
 // first latitude pair or degree, parity) and FFT tiles (member, first latitude pair,
 // field) — sorted by decreasing cost. A stage launches min(items, SMs x CTAs per SM)
 // CTAs and CTA i runs items i, i + gridDim.x, ...: the longest tiles start first and
 // the short ones fill in behind them, so a batch of mixed sizes keeps every SM busy
-// without one launch per member. The five launches of a roundtrip (a start marker plus
-// the four stages) are captured once into a CUDA graph and replayed.
+// without one launch per member. The six launches of a roundtrip (a start marker plus
+// the five stages) are captured once into a CUDA graph and replayed.
 //
 // Per-member latency: the start marker records %globaltimer; the analysis GEMM stores,
 // per member, the time its last tile finished.
@@ -50,7 +51,8 @@ struct shtb_group {
   unsigned char *d_args_syn = nullptr, *d_args_ana = nullptr, *d_jobs_syn = nullptr, *d_jobs_ana = nullptr;
   unsigned long long *d_done = nullptr, *d_t0 = nullptr;
   int4 *d_items_syn = nullptr, *d_items_ana = nullptr;
-  int n_syn = 0, n_ana = 0;
+  int2* d_items_pack = nullptr;
+  int n_syn = 0, n_ana = 0, n_pack = 0;
   unsigned char* d_w = nullptr;
   int4* d_items_fft = nullptr;          // rebuilt when the FFT shape changes
   int n_fft = 0;
@@ -129,6 +131,8 @@ static int group_launch_stages(shtb_group* g, int op, cudaStream_t st) {
     group_start_kernel<<<1, 256, 0, st>>>(g->d_done, g->n, g->d_t0);
     count_launch();
     SHTB_TRY_CUDA(cudaGetLastError(), "group start marker");
+    if ((rc = launch_pack_group(g->d_args_syn, g->d_items_pack, g->n_pack, std::min(g->n_pack, 8 * g->nsm), st)))
+      return rc;
     if ((rc = launch_gemm_group(0, g->d_args_syn, g->d_items_syn, g->n_syn, g->gemm_ctas_syn, nullptr, st))) return rc;
     if ((rc = launch_fft_group_f32(1, g->fft_h, g->generic, g->d_jobs_syn, g->d_items_fft, g->n_fft, g->fft_ctas,
                                    g->fft_smem, st)))
@@ -211,6 +215,19 @@ extern "C" int shtb_group_create(shtb_group** out, const shtb_plan* const* plans
   };
   sort_items(syn, csyn);
   sort_items(ana, cana);
+  std::vector<int2> pack;   // (member, order) for the synthesis B packing, most degrees first
+  {
+    std::vector<int4> tmp;
+    std::vector<int> cost;
+    for (int t = 0; t < n; ++t)
+      for (int im = 0; im <= std::min(plans[t]->mmax, plans[t]->lmax); ++im) {
+        tmp.push_back(make_int4(t, im, 0, 0));
+        cost.push_back(plans[t]->lmax - im);
+      }
+    sort_items(tmp, cost);
+    for (const int4& v : tmp) pack.push_back(make_int2(v.x, v.y));
+  }
+  g->n_pack = (int)pack.size();
   g->n_syn = (int)syn.size();
   g->n_ana = (int)ana.size();
   // two GEMM CTAs of 16 columns fit on an SM
@@ -223,14 +240,13 @@ extern "C" int shtb_group_create(shtb_group** out, const shtb_plan* const* plans
   auto take = [&](size_t b) { size_t r = o; o = align256(o + b); return r; };
   const size_t o_as = take(n * g->argsz), o_aa = take(n * g->argsz), o_js = take(n * g->jobsz), o_ja = take(n * g->jobsz);
   const size_t o_done = take(n * 8), o_t0 = take(8), o_is = take(syn.size() * sizeof(int4)),
-               o_ia = take(ana.size() * sizeof(int4));
+               o_ia = take(ana.size() * sizeof(int4)), o_ip = take(pack.size() * sizeof(int2));
   g->woff.resize(n);
   size_t wbytes = 0;
   for (int t = 0; t < n; ++t) {
     g->woff[t] = wbytes;
-    // pairs padded to 8 and fields to 4: the analysis FFT writes the GEMM's B tile images
-    const size_t np8 = (size_t)(plans[t]->npair + 7) / 8 * 8, nfp = (size_t)(g->nf[t] + 3) / 4 * 4;
-    wbytes = align256(wbytes + nfp * plans[t]->nm * 2 * np8 * sizeof(float2));
+    wbytes = align256(wbytes + std::max(mixed_workspace_bytes(plans[t], SHTB_OP_SYNTHESIS, g->nf[t]),
+                                        mixed_workspace_bytes(plans[t], SHTB_OP_ANALYSIS, g->nf[t])));
   }
   const size_t o_w = take(wbytes);
   cudaError_t e = cudaMalloc(&g->dmem, o);
@@ -243,9 +259,11 @@ extern "C" int shtb_group_create(shtb_group** out, const shtb_plan* const* plans
   g->d_t0 = (unsigned long long*)(g->dmem + o_t0);
   g->d_items_syn = (int4*)(g->dmem + o_is);
   g->d_items_ana = (int4*)(g->dmem + o_ia);
+  g->d_items_pack = (int2*)(g->dmem + o_ip);
   g->d_w = g->dmem + o_w;
   e = cudaMemcpy(g->d_items_syn, syn.data(), syn.size() * sizeof(int4), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(g->d_items_ana, ana.data(), ana.size() * sizeof(int4), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(g->d_items_pack, pack.data(), pack.size() * sizeof(int2), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemset(g->d_done, 0, n * 8);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&g->priv, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->ev_in, cudaEventDisableTiming);
@@ -330,7 +348,7 @@ extern "C" int shtb_group_roundtrip(shtb_group* g, void* stream) {
   SHTB_TRY_CUDA(cudaEventRecord(g->ev_in, st), "group event");
   SHTB_TRY_CUDA(cudaStreamWaitEvent(g->priv, g->ev_in, 0), "group wait");
   SHTB_TRY_CUDA(cudaGraphLaunch(g->exec, g->priv), "group graph launch");
-  for (int i = 0; i < 5; ++i) count_launch();   // start marker + four stage kernels
+  count_launch(6);   // start marker, B packing and four stage kernels
   SHTB_TRY_CUDA(cudaEventRecord(g->ev_out, g->priv), "group event");
   SHTB_TRY_CUDA(cudaStreamWaitEvent(st, g->ev_out, 0), "group wait");
   return SHTB_OK;

@@ -69,6 +69,22 @@ struct FFTDesc {
   unsigned mspan[24];      // the same for the group span Ns / rad[s]
 };
 
+// Round to the nearest TF32 value, ties away from zero: add half a TF32 ulp to the
+// magnitude bits and clear the 13 low mantissa bits (finite inputs).
+__device__ __forceinline__ float tf32_round(float x) {
+  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
+}
+
+// B operand tile images of the mixed-precision GEMMs: one region of nfp x 16 floats per
+// K-step (nfp = fields rounded up to 4, so tiles have whole 8-row core-matrix groups);
+// fields in blocks of 64 (1024 floats), block rows 2f (real) and 2f+1 (imaginary) in the
+// K-major no-swizzle core-matrix order, 8 K values per row. btile_off gives the float
+// offset of (row, K slot kk) inside a block.
+__host__ __device__ inline int btile_nfp(int nf) { return (nf + 3) & ~3; }
+__host__ __device__ inline int btile_off(int row, int kk) {
+  return (row >> 3) * 64 + (kk >> 2) * 32 + (row & 7) * 4 + (kk & 3);
+}
+
 // floor(v / d) for v * d < 2^32 with the multiplier m = floor(2^32 / d) + 1 (m = 0 means d = 1)
 __host__ __device__ inline unsigned magic_div_mul(unsigned d) {
   return d <= 1 ? 0u : (unsigned)((1ull << 32) / d + 1);

@@ -50,6 +50,11 @@ int launch_sphtor_post64(const shtb_plan* p, const double2* V, double2* S, doubl
                          const Factors& F, int div_ll, cudaStream_t st);
 int launch_zero_columns64(const shtb_plan* p, double2* a, int nf, int mlim, cudaStream_t st);
 
+// Floats of one analysis B tile image of the mixed path (hi and lo images back to back).
+size_t fft_btile_floats(const shtb_plan* p, int nf);
+// Bytes of the mixed path's workspace for op (SHTB_OP_SYNTHESIS or SHTB_OP_ANALYSIS).
+size_t mixed_workspace_bytes(const shtb_plan* p, int op, int nf);
+
 // Grouped (uneven-batch) execution: persistent launches over the tiles of many plans.
 int mixed_prepare(const shtb_plan* p, cudaStream_t st);
 size_t mixed_args_bytes();
@@ -58,6 +63,7 @@ int mixed_group_ksteps(const shtb_plan* p, int mode, int im, int par);
 int mixed_group_tile_rows();
 int launch_gemm_group(int mode, const void* targs, const int4* items, int nitems, int grid, unsigned long long* done,
                       cudaStream_t st);
+int launch_pack_group(const void* targs, const int2* items, int nitems, int grid, cudaStream_t st);
 size_t fft_job_bytes_f32();
 void fft_fill_job_f32(const shtb_plan* p, int syn, const void* W, void* grid, int nf, void* host_job);
 size_t fft_group_smem_f32(const shtb_plan* p, int h);

@@ -17,18 +17,17 @@
 // tiles are 128 pairs x 8 degrees, analysis tiles 128 degrees x 8 pairs, both in the
 // K-major no-swizzle core-matrix order of the MMA descriptors.
 //
-// CTA organisation (544 threads, one parity class per CTA): warps 0-3 fill an 8- to
-// 16-stage shared-memory ring of K-major tiles (no swizzle), that many K-steps ahead:
-// bulk copies of the A tile images (and of the analysis B tile images) plus cp.async
-// gathers of the synthesis coefficients; warps 4-7 round each landed stage in place to
-// TF32 hi and write the lo remainders; warp 8 allocates TMEM and one of its threads
-// issues the MMAs (tcgen05.commit releases each stage). The tensor core accumulates the
-// hi*hi products of only kChunk K-steps into one of two TMEM buffers; warps 9-16
-// drain each finished chunk with tcgen05.ld into round-to-nearest FP32 register
-// sums. Long accumulation chains inside the tensor core round toward zero and
-// would bias sums of many terms; short chunks keep that bias below 1e-6 relative
-// at any lmax. The cross terms hi*lo + lo*hi are ~2^-11 of the result, so they
-// accumulate over the whole tile in a third TMEM buffer and are drained once.
+// CTA organisation (576 threads, one parity class per CTA): one thread of warp 17 fills
+// a 16-stage shared-memory ring, 16 K-steps ahead, with bulk copies of the FP32 A tile
+// image and the pre-split (TF32 hi, lo) B tile images; warps 0-7, in two groups taking
+// alternate K-steps, split each A tile into TF32 hi/lo and store it into one of 16 TMEM
+// slots (8 for 16-column tiles); warp 8 allocates TMEM and one of its threads issues the
+// MMAs (A from TMEM, B from shared memory), one commit per chunk of kChunk K-steps
+// releasing that chunk's stages and slots. The tensor core accumulates the three
+// products of a chunk into one of two TMEM buffers; warps 9-16 drain each finished
+// chunk with tcgen05.ld into round-to-nearest FP32 register sums. Long accumulation
+// chains inside the tensor core round toward zero and would bias sums of many terms;
+// short chunks keep that bias below 1e-6 relative at any lmax.
 // Every mbarrier wait is bounded (2 s of %globaltimer); a timeout sets the
 // plan's error word and the CTA drains and exits.
 #include <climits>
@@ -42,7 +41,7 @@ namespace mx {
 constexpr int kM = 128;          // UMMA M
 constexpr int kK = 8;            // TF32 K per instruction
 constexpr int kChunk = 4;          // K-steps accumulated in TMEM before promotion
-constexpr int kThreads = 544;       // 8 producer warps, 1 MMA warp, 8 promotion warps
+constexpr int kThreads = 576;       // 8 splitter warps, 1 MMA warp, 8 promotion warps, 1 loader warp
 constexpr int kTileBytesA = kM * kK * 4;  // 4 KB
 constexpr unsigned long long kWaitNs = 2000000000ull;
 
@@ -51,8 +50,9 @@ struct Args {
   const float* tab;          // tile images of this direction (synthesis or analysis)
   const long long* seg;      // [2*nm+1] first table row of segment (im, parity); rows hold npp pairs
   int npp;
-  const float2* cin;         // synthesis: coefficients; analysis: unused
-  const float2* Win;         // analysis: Fourier buffer [f][nm][2][npair]
+  const float2* cin;         // synthesis: coefficients (input of the B packing)
+  float* bhi;                // B tile images, TF32 hi and lo (synthesis: packed coefficients,
+  float* blo;                //   analysis: written by the FFT)
   float2* Wout;              // synthesis: Fourier buffer
   float2* cout;              // analysis: coefficients
   long long ld_k;            // coefficient field stride (complex elements)
@@ -131,6 +131,34 @@ __device__ __forceinline__ void mma_tf32(unsigned tmem_d, unsigned long long a, 
       :
       : "r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(accum), "r"(z), "r"(z), "r"(z), "r"(z));
 }
+// A from TMEM (M = 128 lanes x 8 columns of TF32), B from shared memory.
+__device__ __forceinline__ void mma_tf32_ts(unsigned tmem_d, unsigned tmem_a, unsigned long long b, unsigned idesc,
+                                            unsigned accum) {
+  const unsigned z = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+      :
+      : "r"(tmem_d), "r"(tmem_a), "l"(b), "r"(idesc), "r"(accum), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+
+// Store this thread's 8 hi values at columns taddr.. and 8 lo values at taddr+8.. of
+// its TMEM lane, then wait for the stores.
+__device__ __forceinline__ void tmem_st8x2(unsigned taddr, const float4& h0, const float4& h1, const float4& l0,
+                                           const float4& l1) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%2, %3, %4, %5, %6, %7, %8, %9};\n\t"
+      "tcgen05.st.sync.aligned.32x32b.x8.b32 [%1], {%10, %11, %12, %13, %14, %15, %16, %17};\n\t"
+      "tcgen05.wait::st.sync.aligned;" ::"r"(taddr),
+      "r"(taddr + 8), "r"(__float_as_uint(h0.x)), "r"(__float_as_uint(h0.y)), "r"(__float_as_uint(h0.z)),
+      "r"(__float_as_uint(h0.w)), "r"(__float_as_uint(h1.x)), "r"(__float_as_uint(h1.y)), "r"(__float_as_uint(h1.z)),
+      "r"(__float_as_uint(h1.w)), "r"(__float_as_uint(l0.x)), "r"(__float_as_uint(l0.y)), "r"(__float_as_uint(l0.z)),
+      "r"(__float_as_uint(l0.w)), "r"(__float_as_uint(l1.x)), "r"(__float_as_uint(l1.y)), "r"(__float_as_uint(l1.z)),
+      "r"(__float_as_uint(l1.w))
+      : "memory");
+}
+
 __device__ __forceinline__ void mma_commit(unsigned long long* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                : "memory");
@@ -177,14 +205,6 @@ __device__ __forceinline__ void tmem_ld<32>(unsigned taddr, float* v) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ __forceinline__ void cp_async4(void* dst, const void* src, bool ok) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(smem_u32(dst)), "l"(src), "r"(ok ? 4 : 0)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool ok) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src), "r"(ok ? 16 : 0)
-               : "memory");
-}
 __device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
@@ -196,18 +216,6 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
                : "memory");
 }
 
-// Arrive on bar once every cp.async this thread issued so far has landed (the barrier's
-// expected count includes this arrival).
-__device__ __forceinline__ void cp_async_arrive_noinc(unsigned long long* bar) {
-  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-
-// Round to the nearest TF32 value, ties away from zero: add half a TF32 ulp to the
-// magnitude bits and clear the 13 low mantissa bits (finite inputs).
-__device__ __forceinline__ float tf32_round(float x) {
-  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
-}
 // x = hi + lo with hi = tf32(x) and lo = tf32(x - hi) (x - hi is exact in FP32).
 __device__ __forceinline__ void split4(const float4& x, float4& h, float4& l) {
   h.x = tf32_round(x.x); h.y = tf32_round(x.y); h.z = tf32_round(x.z); h.w = tf32_round(x.w);
@@ -226,14 +234,25 @@ __device__ __forceinline__ float coef_factor(const Args& a, int l, int m) {
 template <int N>
 struct Smem {
   static constexpr int kTileB = N * kK * 4;
-  // per stage: A_hi, A_lo, B_hi, B_lo (one parity class per CTA)
-  static constexpr int kStage = 2 * kTileBytesA + 2 * kTileB;
-  // Ring depth: enough stages in flight to cover the global-memory latency of the
-  // stage copies (12 x 16 KB for N = 128); the 16-column tiles keep 8 so that two CTAs
-  // share an SM.
-  static constexpr int kSt = (N == 128) ? 12 : (N == 16) ? 8 : 16;
+  // per stage: A as loaded (FP32), B_hi, B_lo (one parity class per CTA); the split A
+  // tiles live in TMEM
+  static constexpr int kStage = kTileBytesA + 2 * kTileB;
+  // Ring depth: 16 shared-memory stages (enough bulk copies in flight to cover the
+  // global-memory latency) and 16 TMEM slots for the split A tiles.
+  static constexpr int kSt = 16;
+  static constexpr int kStA = (N == 16) ? 8 : 16;   // two 16-column CTAs share an SM's TMEM
+  static constexpr int kRel = 16;   // chunk-release barriers (>= kSt, see gemm_tile)
   static constexpr int kBar = kSt * kStage;
-  static constexpr int kBytes = kBar + (3 * kSt + 4) * 8 + 16;
+  // barriers: full[kSt], ldfull[kSt], rel[kRel], acce[2]; then the loader's stage->chunk
+  // map (kSt ints), the splitters' slot->chunk maps (256 x kStA ints), TMEM slot, abort flag
+  static constexpr int kBytes = kBar + (2 * kSt + kRel + 2) * 8 + kSt * 4 + 256 * kStA * 4 + 16;
+  // TMEM: chunk accumulators H0 [0, N) and H1 [N, 2N); A slot s: hi at 2N + 16 s, lo at
+  // 2N + 16 s + 8
+  static constexpr int kTmemA = 2 * N;
+  static constexpr int kTmemNeed = 2 * N + 16 * kStA;
+  static constexpr int kTmemCols = kTmemNeed <= 32 ? 32 : kTmemNeed <= 64 ? 64 : kTmemNeed <= 128 ? 128
+                                   : kTmemNeed <= 256 ? 256 : 512;
+  static_assert(kTmemNeed <= 512, "TMEM columns");
 };
 
 // Narrow tiles (N = 16: up to 8 fields) leave the tensor core mostly idle, so two CTAs
@@ -249,7 +268,9 @@ struct TileCoord {
 
 // Shared-memory barriers of a GEMM CTA (initialised once per CTA).
 struct Bars {
-  unsigned long long *full, *empty, *ldfull, *accf, *acce;
+  unsigned long long *full, *ldfull, *rel, *acce;
+  unsigned* stage_chunk;   // [kSt] chunk of the K-step that last used each stage (loader)
+  unsigned* slot_chunk;    // [256][kStA] the same for TMEM A slots (one row per splitter thread)
   unsigned* tmem_slot;
   volatile int* abort_flag;
 };
@@ -258,12 +279,13 @@ template <int N>
 __device__ __forceinline__ Bars gemm_bars(unsigned char* sm) {
   using S = Smem<N>;  // barriers follow the stage ring
   Bars B;
-  B.full = reinterpret_cast<unsigned long long*>(sm + S::kBar);
-  B.empty = B.full + S::kSt;
-  B.ldfull = B.empty + S::kSt;    // [kSt] loader copies of the stage landed
-  B.accf = B.ldfull + S::kSt;     // [2] chunk accumulated in TMEM buffer b
-  B.acce = B.accf + 2;            // [2] TMEM buffer b drained by the promotion warps
-  B.tmem_slot = reinterpret_cast<unsigned*>(B.acce + 2);
+  B.full = reinterpret_cast<unsigned long long*>(sm + S::kBar);   // [kSt] stage split (A in TMEM)
+  B.ldfull = B.full + S::kSt;     // [kSt] bulk copies of the stage landed
+  B.rel = B.ldfull + S::kSt;      // [kRel] MMAs of chunk q done (q % kRel)
+  B.acce = B.rel + S::kRel;       // [2] TMEM chunk buffer b drained by the promotion warps
+  B.stage_chunk = reinterpret_cast<unsigned*>(B.acce + 2);
+  B.slot_chunk = B.stage_chunk + S::kSt;
+  B.tmem_slot = B.slot_chunk + 256 * S::kStA;
   B.abort_flag = reinterpret_cast<volatile int*>(B.tmem_slot + 1);
   return B;
 }
@@ -283,19 +305,16 @@ __device__ __forceinline__ unsigned gemm_cta_setup(const Bars& B) {
   if (tid == 0) {
     for (int s = 0; s < Smem<N>::kSt; ++s) {
       mbar_init(&B.full[s], 128);
-      mbar_init(&B.empty[s], 1);
-      mbar_init(&B.ldfull[s], 129);   // 128 loader cp.async arrivals + the A bulk copy's expect_tx
+      mbar_init(&B.ldfull[s], 1);
     }
-    for (int b = 0; b < 2; ++b) {
-      mbar_init(&B.accf[b], 1);
-      mbar_init(&B.acce[b], 256);
-    }
+    for (int s = 0; s < Smem<N>::kRel; ++s) mbar_init(&B.rel[s], 1);
+    for (int b = 0; b < 2; ++b) mbar_init(&B.acce[b], 256);
     *B.abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 8) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(B.tmem_slot)),
-                 "r"(4 * N));
+                 "r"(Smem<N>::kTmemCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -310,7 +329,7 @@ __device__ __forceinline__ void gemm_cta_teardown(unsigned tmem) {
   __syncthreads();
   if ((threadIdx.x >> 5) == 8) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(4 * N));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Smem<N>::kTmemCols));
   }
 }
 
@@ -319,14 +338,20 @@ __device__ __forceinline__ void gemm_cta_teardown(unsigned tmem) {
 // K-steps and chunks of the tiles before this one, which fixes every stage index and
 // barrier phase. Callers separate tiles with __syncthreads (the cross-term TMEM buffer
 // is reused).
+//
+// Synchronisation: the MMA issuer waits for all K-steps of a chunk (kChunk K-steps) to
+// be split, issues their 3 kChunk MMAs back to back and commits once, to rel[chunk %
+// kRel]. That one barrier releases the chunk's shared-memory stages (loader), its TMEM
+// A slots (splitters) and its accumulator (promotion warps); producers look up the
+// chunk of a stage's or slot's previous K-step in small per-role maps. kRel >= kSt
+// keeps a waiter from ever seeing a barrier two phases ahead.
 template <int MODE, int N>
 __device__ __forceinline__ void gemm_tile(const Args& a, const TileCoord& tc, unsigned char* sm, const Bars& B,
                                           unsigned tmem, unsigned ks0, unsigned c0) {
   using S = Smem<N>;
   unsigned long long* full = B.full;
-  unsigned long long* empty = B.empty;
   unsigned long long* ldfull = B.ldfull;
-  unsigned long long* accf = B.accf;
+  unsigned long long* rel = B.rel;
   unsigned long long* acce = B.acce;
   volatile int* abort_flag = B.abort_flag;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -334,137 +359,76 @@ __device__ __forceinline__ void gemm_tile(const Args& a, const TileCoord& tc, un
   const int npair = P.npair;
   const int par = tc.par, im = tc.im, p0 = tc.p0, j0 = tc.j0, kb = tc.kb;
   const int m = im * P.mres;
-  // degrees of this parity class in [m, lend]
-  const int J = (a.lend >= m + par) ? (a.lend - m - par) / 2 + 1 : 0;
   const long long sg = a.seg[2 * im + par];
   const long long ln = a.seg[2 * im + par + 1] - sg;
   const int nks = tile_ksteps<MODE>(a, tc);
   const int nch = (nks + kChunk - 1) / kChunk;
   // TMEM: chunk buffer b (hi*hi) at column b*N; the cross terms of the whole tile at 2N
 
-  if (warp < 8) {
+  if (warp < 8 || warp == 17) {
     // ------------------------------------------------------------- producers
-    // Warps 0-3 (loaders) copy the operands of every K-step with cp.async straight into
-    // their K-major slots of the hi tiles of stage ks % kSt and signal completion on
-    // ldfull with cp.async.mbarrier.arrive, running up to kSt K-steps ahead. Warps 4-7
-    // (splitters) round each landed stage in place to TF32, write the remainders into the
-    // lo tiles, and release the stage to the MMA issuer. Keeping the two roles in separate
-    // threads means a splitter's proxy fence never waits for copies still in flight.
+    // One thread (warp 17, lane 0) fills the shared-memory ring, kSt K-steps ahead, with
+    // three bulk copies per K-step: the FP32 A tile image and the pre-split B tile images
+    // (hi, lo). Two groups of splitter warps (0-3 and 4-7, even and odd K-steps) split each
+    // landed A tile into TF32 hi/lo and store it into a TMEM slot, which the MMAs read as
+    // their A operand.
     const int t = tid & 127;
-    const int Jc = (MODE == 0) ? J : npair;   // valid K indices of this GEMM
-    if (warp < 4) {
-      // B copies: instruction r of warp w4 covers fields 2 (8 w4 + r) + (lane >> 4); within
-      // a field the 16 lanes take K slot bk = (lane >> 1) & 7, component bc = lane & 1, so
-      // each half-warp reads one field's contiguous span.
-      const int w4 = warp & 3, bk = (lane >> 1) & 7, bc = lane & 1, bfh = lane >> 4;
-      const int fl0 = 16 * w4 + bfh;                 // field of instruction 0
-      const int nfr = min(N / 2, a.nf - kb);         // fields of this CTA
-      const int nr = (nfr > fl0) ? min(8, (nfr - fl0 + 1) / 2) : 0;   // active instructions
-      const float* b0;
-      long long fstride, kstep;
-      if (MODE == 0) {
-        b0 = reinterpret_cast<const float*>(a.cin + (long long)(kb + fl0) * a.ld_k + (long long)m * (P.lmax + 1) + m + par +
-                                            2 * bk) + bc;
-        fstride = 4 * a.ld_k;                        // two fields, in floats
-        kstep = 32;                                  // 16 complex degrees per K-step
-      } else {
-        b0 = reinterpret_cast<const float*>(a.Win + (((long long)(kb + fl0) * P.nm + im) * 2 + par) * npair + bk) + bc;
-        fstride = 8ll * P.nm * npair;
-        kstep = 16;
-      }
-      unsigned char* bdst0 = sm + 2 * kTileBytesA + tile_off(2 * fl0 + bc, bk >> 2) + (bk & 3) * 4;
-      // A tile images: synthesis [ptile][ks] blocks of 4 KB after the segment start;
-      // analysis [jtile][ks] blocks of rows*32 bytes (rows = 128, fewer in the last jtile)
-      const float* aseg = a.tab + sg * a.npp;
-      const int arows = (MODE == 0) ? kM : min(kM, (int)ln - j0);
-      const float* a0 = (MODE == 0) ? aseg + (long long)(p0 / kM) * (ln / kK) * (kM * kK) : aseg + (long long)j0 * a.npp;
-      const unsigned abytes = (unsigned)arows * kK * 4;
-      // analysis B: tile images written by the FFT, region (im, par, ks) of nfp x 16 floats
-      // (nfp = nf rounded up to 4), this CTA's block of 64 fields at kb / 64 * 1024 floats
-      const int nks8 = (npair + kK - 1) / kK, nfp = (a.nf + 3) & ~3;
-      const float* bimg = reinterpret_cast<const float*>(a.Win) +
-                          ((long long)(im * 2 + par) * nks8) * nfp * 16 + (long long)(kb >> 6) * 1024;
-      const unsigned bbytes = (unsigned)min(64, nfp - kb) * 64;
-      for (int ks = 0; ks < nks; ++ks) {
-        const unsigned g = ks0 + ks;
-        const int b = g % S::kSt;
-        if (g >= S::kSt && !mbar_wait(&empty[b], ((g / S::kSt) - 1) & 1, abort_flag, a.err)) break;
-        unsigned char* st = sm + (size_t)b * S::kStage;
-        if (MODE == 1) {
-          // A and B tile images, both by bulk copy
-          if (t == 0) {
-            mbar_expect_tx(&ldfull[b], abytes + bbytes);
-            bulk_g2s(st, a0 + (long long)ks * arows * kK, abytes, &ldfull[b]);
-            bulk_g2s(st + 2 * kTileBytesA, bimg + (long long)ks * nfp * 16, bbytes, &ldfull[b]);
+    if (warp == 17) {
+      if (lane == 0) {
+        // A tile images: synthesis [ptile][ks] blocks of 4 KB after the segment start;
+        // analysis [jtile][ks] blocks of rows*32 bytes (rows = 128, fewer in the last jtile)
+        const float* aseg = a.tab + sg * a.npp;
+        const int arows = (MODE == 0) ? kM : min(kM, (int)ln - j0);
+        const float* a0 =
+            (MODE == 0) ? aseg + (long long)(p0 / kM) * (ln / kK) * (kM * kK) : aseg + (long long)j0 * a.npp;
+        const unsigned abytes = (unsigned)arows * kK * 4;
+        // B tile images: region rb + ks of nfp x 16 floats, this CTA's block of 64 fields
+        const int nfp = btile_nfp(a.nf);
+        const long long rb = (MODE == 0) ? sg / kK : (long long)(im * 2 + par) * ((npair + kK - 1) / kK);
+        const long long boff = rb * nfp * 16 + (long long)(kb >> 6) * 1024;
+        const unsigned bbytes = (unsigned)min(64, nfp - kb) * 64;
+        for (int ks = 0; ks < nks; ++ks) {
+          const unsigned g = ks0 + ks;
+          const int b = g % S::kSt;
+          if (g >= S::kSt) {
+            const unsigned q = B.stage_chunk[b];
+            if (!mbar_wait(&rel[q % S::kRel], (q / S::kRel) & 1, abort_flag, a.err)) break;
           }
-          cp_async_arrive_noinc(&ldfull[b]);
-          continue;
-        }
-        if (t == 0) {
-          mbar_expect_tx(&ldfull[b], abytes);
+          B.stage_chunk[b] = c0 + ks / kChunk;
+          unsigned char* st = sm + (size_t)b * S::kStage;
+          const long long bo = boff + (long long)ks * nfp * 16;
+          mbar_expect_tx(&ldfull[b], abytes + 2 * bbytes);
           bulk_g2s(st, a0 + (long long)ks * arows * kK, abytes, &ldfull[b]);
+          bulk_g2s(st + kTileBytesA, a.bhi + bo, bbytes, &ldfull[b]);
+          bulk_g2s(st + kTileBytesA + S::kTileB, a.blo + bo, bbytes, &ldfull[b]);
         }
-        const bool kok = ks * kK + bk < Jc;
-        const float* bs = b0 + ks * kstep;
-        unsigned char* bd = bdst0 + (size_t)b * S::kStage;
-#pragma unroll
-        for (int r = 0; r < 8; ++r) {
-          if (r < nr) {
-            const bool ok = kok && (fl0 + 2 * r < nfr);
-            // field fl0 + 2r sits 4r rows below field fl0: (r >> 1) 8-row groups, (r & 1) * 4 rows
-            cp_async4(bd + (r >> 1) * 256 + (r & 1) * 64, ok ? bs + r * fstride : a.tab, ok);
-          }
-        }
-        cp_async_arrive_noinc(&ldfull[b]);
       }
-      cp_async_wait_all();
     } else {
-      // Splitter thread t rounds row t of the A tile and row t of the B tile.
-      const bool brow = t < N;
-      const bool scaled = (MODE == 0) && (a.sc_mode || a.mf0 != 1.f || a.mf1 != 1.f);
-      for (int ks = 0; ks < nks; ++ks) {
+      // Splitter thread t of group sg rounds row t of the A tile into TMEM lane t (its
+      // warp's quadrant) for the K-steps g with g % 2 == sg.
+      const int sgp = warp >> 2;
+      const unsigned ta_lane = tmem + ((unsigned)(32 * (warp & 3)) << 16);
+      const int o0 = tile_off(t, 0), o1 = tile_off(t, 1);
+      unsigned* my_slots = B.slot_chunk + (sgp * 128 + t) * S::kStA;
+      for (int ks = ((ks0 & 1) == (unsigned)sgp) ? 0 : 1; ks < nks; ks += 2) {
         const unsigned g = ks0 + ks;
-        const int b = g % S::kSt;
+        const int b = g % S::kSt, ba = g % S::kStA;
         if (!mbar_wait(&ldfull[b], (g / S::kSt) & 1, abort_flag, a.err)) break;
-        unsigned char* st = sm + (size_t)b * S::kStage;
-        unsigned char* Ah = st;
-        unsigned char* Al = st + kTileBytesA;
-        unsigned char* Bh = st + 2 * kTileBytesA;
-        unsigned char* Bl = Bh + S::kTileB;
-        const int o0 = tile_off(t, 0), o1 = tile_off(t, 1);
+        if (g >= S::kStA) {
+          const unsigned q = my_slots[ba];
+          if (!mbar_wait(&rel[q % S::kRel], (q / S::kRel) & 1, abort_flag, a.err)) break;
+        }
+        my_slots[ba] = c0 + ks / kChunk;
+        // the MMAs that last read TMEM slot ba have completed
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const unsigned char* Ah = sm + (size_t)b * S::kStage;
         const float4 x0 = *reinterpret_cast<const float4*>(Ah + o0);
         const float4 x1 = *reinterpret_cast<const float4*>(Ah + o1);
-        float4 y0 = make_float4(0.f, 0.f, 0.f, 0.f), y1 = y0;
-        if (brow) {
-          y0 = *reinterpret_cast<const float4*>(Bh + o0);
-          y1 = *reinterpret_cast<const float4*>(Bh + o1);
-          if (scaled) {
-            float sc[8];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-              const int l = m + par + 2 * (ks * kK + k);
-              sc[k] = (l <= a.lend) ? coef_factor(a, l, m) : 0.f;   // beyond lend the copies zero-filled
-            }
-            y0.x *= sc[0]; y0.y *= sc[1]; y0.z *= sc[2]; y0.w *= sc[3];
-            y1.x *= sc[4]; y1.y *= sc[5]; y1.z *= sc[6]; y1.w *= sc[7];
-          }
-        }
-        float4 h, l;
+        float4 h, l, h1, l1;
         split4(x0, h, l);
-        *reinterpret_cast<float4*>(Ah + o0) = h;
-        *reinterpret_cast<float4*>(Al + o0) = l;
-        split4(x1, h, l);
-        *reinterpret_cast<float4*>(Ah + o1) = h;
-        *reinterpret_cast<float4*>(Al + o1) = l;
-        if (brow) {
-          split4(y0, h, l);
-          *reinterpret_cast<float4*>(Bh + o0) = h;
-          *reinterpret_cast<float4*>(Bl + o0) = l;
-          split4(y1, h, l);
-          *reinterpret_cast<float4*>(Bh + o1) = h;
-          *reinterpret_cast<float4*>(Bl + o1) = l;
-        }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        split4(x1, h1, l1);
+        tmem_st8x2(ta_lane + (unsigned)(S::kTmemA + 16 * ba), h, h1, l, l1);
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         mbar_arrive(&full[b]);
       }
     }
@@ -472,32 +436,30 @@ __device__ __forceinline__ void gemm_tile(const Args& a, const TileCoord& tc, un
     // ------------------------------------------------------------- MMA issuer
     if (lane == 0) {
       const unsigned idesc = idesc_tf32<N>();
+      const unsigned long long bh0 = sdesc(sm + kTileBytesA), bl0 = sdesc(sm + kTileBytesA + S::kTileB);
+      constexpr unsigned long long kStageDesc = S::kStage >> 4;   // descriptor address step per stage
       bool ok = true;
       for (int c = 0; c < nch && ok; ++c) {
         const unsigned gc = c0 + c;
         const int bb = gc & 1;
         if (gc >= 2 && !mbar_wait(&acce[bb], ((gc >> 1) - 1) & 1, abort_flag, a.err)) break;
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const unsigned dH = tmem + bb * N, dX = tmem + 2 * N;
-        const int k1 = min(nks, (c + 1) * kChunk);
-        for (int ks = c * kChunk; ks < k1; ++ks) {
+        const int k0 = c * kChunk, k1 = min(nks, k0 + kChunk);
+        for (int ks = k0; ks < k1 && ok; ++ks) {
           const unsigned g = ks0 + ks;
-          const int b = g % S::kSt;
-          if (!mbar_wait(&full[b], (g / S::kSt) & 1, abort_flag, a.err)) {
-            ok = false;
-            break;
-          }
-          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-          unsigned char* st = sm + (size_t)b * S::kStage;
-          const unsigned long long ah = sdesc(st), al = sdesc(st + kTileBytesA);
-          const unsigned long long bh_ = sdesc(st + 2 * kTileBytesA), bl_ = sdesc(st + 2 * kTileBytesA + S::kTileB);
-          const unsigned acc = (ks == c * kChunk) ? 0u : 1u;
-          mma_tf32(dH, ah, bh_, idesc, acc);
-          mma_tf32(dX, ah, bl_, idesc, ks == 0 ? 0u : 1u);
-          mma_tf32(dX, al, bh_, idesc, 1u);
-          mma_commit(&empty[b]);
+          ok = mbar_wait(&full[g % S::kSt], (g / S::kSt) & 1, abort_flag, a.err);
         }
-        mma_commit(&accf[bb]);
+        if (!ok) break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const unsigned dH = tmem + bb * N;
+        for (int ks = k0; ks < k1; ++ks) {
+          const unsigned g = ks0 + ks;
+          const unsigned long long so = (unsigned long long)(g % S::kSt) * kStageDesc;
+          const unsigned ah = tmem + S::kTmemA + 16 * (g % S::kStA), al = ah + 8;
+          mma_tf32_ts(dH, ah, bh0 + so, idesc, ks == k0 ? 0u : 1u);
+          mma_tf32_ts(dH, ah, bl0 + so, idesc, 1u);
+          mma_tf32_ts(dH, al, bh0 + so, idesc, 1u);
+        }
+        mma_commit(&rel[gc % S::kRel]);
       }
     }
   } else {
@@ -514,7 +476,7 @@ __device__ __forceinline__ void gemm_tile(const Args& a, const TileCoord& tc, un
     for (int c = 0; c < nch; ++c) {
       const unsigned gc = c0 + c;
       const int bb = gc & 1;
-      if (ok) ok = mbar_wait(&accf[bb], (gc >> 1) & 1, abort_flag, a.err);
+      if (ok) ok = mbar_wait(&rel[gc % S::kRel], (gc / S::kRel) & 1, abort_flag, a.err);
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       __syncwarp();
       const unsigned dH = tmem + lane_base + bb * N + h * (N / 2);
@@ -528,17 +490,6 @@ __device__ __forceinline__ void gemm_tile(const Args& a, const TileCoord& tc, un
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       mbar_arrive(&acce[bb]);
       if (!ok) break;
-    }
-    if (ok && nch > 0) {
-      // cross terms, accumulated over the whole tile (the last chunk's commit covers them)
-      const unsigned dX = tmem + lane_base + 2 * N + h * (N / 2);
-#pragma unroll
-      for (int i = 0; i < N / 2; i += kLd) {
-        float v[kLd];
-        tmem_ld<kLd>(dX + i, v);
-#pragma unroll
-        for (int u = 0; u < kLd; ++u) acc[i + u] += v[u];
-      }
     }
     if (ok) {
 #pragma unroll
@@ -569,6 +520,59 @@ __device__ __forceinline__ void gemm_tile(const Args& a, const TileCoord& tc, un
         }
       }
     }
+  }
+}
+
+// Synthesis B tile images: the coefficients of order im, field k, times the per-(l, m)
+// factors, split into TF32 hi/lo. Rows are the degrees l = m + par + 2j of one parity
+// (region seg(im, par)/8 + j/8 of the images); every row of the segment is written,
+// zero beyond lend, so the GEMM's last K-step of each segment reads zeros there.
+__device__ __forceinline__ void pack_order(const Args& a, int im, int k) {
+  const PlanDev& P = a.P;
+  const int m = im * P.mres;
+  const int nfp = btile_nfp(a.nf), fl = k & 63;
+  const float2* c = a.cin + (long long)k * a.ld_k + (long long)m * (P.lmax + 1);
+  for (int par = 0; par < 2; ++par) {
+    const long long sg = a.seg[2 * im + par];
+    const int R = (int)(a.seg[2 * im + par + 1] - sg);
+    for (int j = threadIdx.x; j < R; j += blockDim.x) {
+      const int l = m + par + 2 * j;
+      float2 v = make_float2(0.f, 0.f);
+      if (l <= a.lend) {
+        v = c[l];
+        if (a.sc_mode || a.mf0 != 1.f || a.mf1 != 1.f) {
+          const float sc = coef_factor(a, l, m);
+          v.x *= sc;
+          v.y *= sc;
+        }
+      }
+      const long long base = (sg / kK + j / kK) * nfp * 16 + (long long)(k >> 6) * 1024;
+      const int kk = j & 7;
+      const long long o0 = base + btile_off(2 * fl, kk), o1 = base + btile_off(2 * fl + 1, kk);
+      const float hx = tf32_round(v.x), hy = tf32_round(v.y);
+      a.bhi[o0] = hx;
+      a.bhi[o1] = hy;
+      a.blo[o0] = tf32_round(v.x - hx);
+      a.blo[o1] = tf32_round(v.y - hy);
+    }
+  }
+}
+
+// blockIdx.x = order, blockIdx.y = field.
+__global__ void __launch_bounds__(256) mixed_pack_kernel(const __grid_constant__ Args a) {
+  pack_order(a, blockIdx.x, blockIdx.y);
+}
+
+// Persistent packing for grouped transforms: item = (transform, order), all its fields.
+__global__ void __launch_bounds__(256) mixed_pack_group_kernel(const Args* __restrict__ targs,
+                                                              const int2* __restrict__ items, int nitems) {
+  __shared__ Args sa;
+  for (int i = blockIdx.x; i < nitems; i += gridDim.x) {
+    const int2 it = items[i];
+    if (threadIdx.x == 0) sa = targs[it.x];
+    __syncthreads();
+    for (int k = 0; k < sa.nf; ++k) pack_order(sa, it.y, k);
+    __syncthreads();
   }
 }
 
@@ -677,23 +681,40 @@ __global__ void mixed_table_kernel(PlanDev P, float* __restrict__ tabS, float* _
 
 using namespace mx;
 
-static int ensure_table(const shtb_plan* cp, cudaStream_t st) {
-  shtb_plan* p = const_cast<shtb_plan*>(cp);
-  std::lock_guard<std::mutex> lk(p->tab_mu);
-  if (p->d_tab) return SHTB_OK;
+// Segment starts of the P table: rows (degrees m+par, m+par+2, .., lrec) of every
+// (order, parity), each segment padded to a multiple of 8 rows. Returns the row count.
+static long long table_segments(const shtb_plan* p, std::vector<long long>* seg) {
   const int nm = p->nm, LR = p->lrec;
-  p->npp = (p->npair + kM - 1) / kM * kM;
-  p->htab_seg.assign(2 * nm + 1, 0);
+  if (seg) seg->assign(2 * nm + 1, 0);
   long long rows = 0;
   for (int im = 0; im < nm; ++im) {
     const int m = im * p->mres;
     for (int par = 0; par < 2; ++par) {
-      p->htab_seg[2 * im + par] = rows;
+      if (seg) (*seg)[2 * im + par] = rows;
       const int cnt = (LR - m - par >= 0) ? (LR - m - par) / 2 + 1 : 0;
       rows += (cnt + kK - 1) / kK * kK;
     }
   }
-  p->htab_seg[2 * nm] = rows;
+  if (seg) (*seg)[2 * nm] = rows;
+  return rows;
+}
+
+static size_t align256(size_t v) { return (v + 255) / 256 * 256; }
+
+// Synthesis workspace: Fourier buffer [f][nm][2][npair] (float2), then the B tile
+// images hi and lo (table rows x nfp x 2 floats each).
+static size_t syn_w_bytes(const shtb_plan* p, int nf) { return align256((size_t)nf * p->nm * 2 * p->npair * 8); }
+static size_t syn_img_bytes(const shtb_plan* p, int nf) {
+  return align256((size_t)table_segments(p, nullptr) * btile_nfp(nf) * 2 * 4);
+}
+
+static int ensure_table(const shtb_plan* cp, cudaStream_t st) {
+  shtb_plan* p = const_cast<shtb_plan*>(cp);
+  std::lock_guard<std::mutex> lk(p->tab_mu);
+  if (p->d_tab) return SHTB_OK;
+  const int nm = p->nm;
+  p->npp = (p->npair + kM - 1) / kM * kM;
+  const long long rows = table_segments(p, &p->htab_seg);
   const size_t tb = (size_t)rows * p->npp * 4;   // one image
   void* mem = nullptr;
   cudaError_t e = cudaMalloc(&mem, 2 * tb + (2 * nm + 1) * 8 + 256);
@@ -772,13 +793,23 @@ int mixed_synthesis(const shtb_plan* p, const void* alm, void* f, int nf, int lt
   Args a = base_args(p);
   a.cin = (const float2*)alm;
   a.Wout = (float2*)work;
+  a.bhi = (float*)((char*)work + syn_w_bytes(p, nf));
+  a.blo = (float*)((char*)a.bhi + syn_img_bytes(p, nf));
   a.sc_mode = p->d_scale ? 1 : 0;
   a.nf = nf;
   a.lend = ltr;
   a.lcap = ltr;
+  prof_begin(st);
+  mixed_pack_kernel<<<dim3(mlim / p->mres + 1, nf), 256, 0, st>>>(a);
+  SHTB_LAUNCHED("tc gemm B packing kernel");
   dim3 g(2 * ((p->npair + kM - 1) / kM), mlim / p->mres + 1);
   if ((rc = dispatch_gemm<0>(p, a, nf, g, st))) return rc;
   return launch_fft_syn<float, float>(p, work, (float*)f, nullptr, 1, nf, mlim, p->phi_inv_scale / p->nlon, 0, 0, st);
+}
+
+size_t mixed_workspace_bytes(const shtb_plan* p, int op, int nf) {
+  if (op == SHTB_OP_SYNTHESIS) return syn_w_bytes(p, nf) + 2 * syn_img_bytes(p, nf);
+  return align256(2 * fft_btile_floats(p, nf) * 4);
 }
 
 int mixed_analysis(const shtb_plan* p, const void* f, void* alm, int nf, int ltr, void* work, cudaStream_t st) {
@@ -807,7 +838,8 @@ int mixed_analysis(const shtb_plan* p, const void* f, void* alm, int nf, int ltr
   }
   Args a = base_args(p);
   a.tab = p->d_tab_ana;
-  a.Win = (const float2*)work;
+  a.bhi = (float*)work;
+  a.blo = (float*)work + fft_btile_floats(p, nf);
   a.cout = (float2*)alm;
   a.sc_mode = p->d_scale ? 2 : 0;
   a.nf = nf;
@@ -838,10 +870,13 @@ void mixed_fill_args(const shtb_plan* p, int mode, const void* in, void* out, in
   if (mode == 0) {
     a.cin = (const float2*)in;
     a.Wout = (float2*)out;
+    a.bhi = (float*)((char*)out + syn_w_bytes(p, nf));
+    a.blo = (float*)((char*)a.bhi + syn_img_bytes(p, nf));
     a.sc_mode = p->d_scale ? 1 : 0;
   } else {
     a.tab = p->d_tab_ana;
-    a.Win = (const float2*)in;
+    a.bhi = (float*)const_cast<void*>(in);
+    a.blo = (float*)const_cast<void*>(in) + fft_btile_floats(p, nf);
     a.cout = (float2*)out;
     a.sc_mode = p->d_scale ? 2 : 0;
   }
@@ -857,6 +892,14 @@ int mixed_group_ksteps(const shtb_plan* p, int mode, int im, int par) {
 }
 
 int mixed_group_tile_rows() { return kM; }
+
+int launch_pack_group(const void* targs, const int2* items, int nitems, int grid, cudaStream_t st) {
+  if (nitems <= 0) return SHTB_OK;
+  mixed_pack_group_kernel<<<grid, 256, 0, st>>>((const Args*)targs, items, nitems);
+  count_launch();
+  SHTB_TRY_CUDA(cudaGetLastError(), "group pack launch");
+  return SHTB_OK;
+}
 
 int launch_gemm_group(int mode, const void* targs, const int4* items, int nitems, int grid, unsigned long long* done,
                       cudaStream_t st) {

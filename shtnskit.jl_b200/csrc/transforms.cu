@@ -145,8 +145,6 @@ using namespace shtb;
 // validation and workspace
 // ---------------------------------------------------------------------------
 static size_t wbytes_fourier(const shtb_plan* p, int nfw, size_t celem) {
-  // the mixed path's analysis writes B tile images: latitude pairs padded to 8, fields to 4
-  if (celem == 8) return (size_t)((nfw + 3) / 4 * 4) * p->nm * 2 * ((p->npair + 7) / 8 * 8) * celem;
   return (size_t)nfw * p->nm * 2 * p->npair * celem;
 }
 static size_t align256(size_t v) { return (v + 255) / 256 * 256; }
@@ -158,6 +156,7 @@ extern "C" size_t shtb_workspace_bytes(const shtb_plan* p, int op, int nfields, 
   switch (op) {
     case SHTB_OP_SYNTHESIS:
     case SHTB_OP_ANALYSIS:
+      if (precision == SHTB_PREC_MIXED) return mixed_workspace_bytes(p, op, nfields);
       return align256(wbytes_fourier(p, nfields, celem));
     case SHTB_OP_SYNTHESIS_SPHTOR:
     case SHTB_OP_ANALYSIS_SPHTOR:

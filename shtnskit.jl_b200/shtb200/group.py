@@ -1,8 +1,8 @@
 """Uneven batches: many independent mixed-precision scalar roundtrips of different sizes.
 
 Each member has its own configuration (lmax, Gauss grid, nlon) and 1..8 fields. The
-library runs all members' tiles in one persistent launch per stage (order-GEMM
-synthesis, FFT synthesis, FFT analysis, order-GEMM analysis), captured once into a
+library runs all members' tiles in one persistent launch per stage (B packing,
+order-GEMM synthesis, FFT synthesis, FFT analysis, order-GEMM analysis), captured once into a
 CUDA graph and replayed (``shtb_group_*`` in ``include/shtb200.h``). Results equal
 the per-member ``synthesis_batch`` / ``analysis_batch`` calls with
 ``precision="mixed"`` bit for bit.

@@ -56,7 +56,7 @@ def test_group_matches_per_member_bitwise():
     launches0 = _lib.load().shtb_launch_count(0)
     b.roundtrip()
     torch.cuda.synchronize()
-    assert _lib.load().shtb_launch_count(0) - launches0 == 5
+    assert _lib.load().shtb_launch_count(0) - launches0 == 6
     b.status()
     grids, alms = per_member(b)
     assert_same(b, grids, alms)
