@@ -450,14 +450,21 @@ __device__ __forceinline__ void gemm_tile(const Args& a, const TileCoord& tc, un
         }
         if (!ok) break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        // The accumulator rounds every addition toward zero at its current magnitude, so
+        // the small cross terms (hi*lo, lo*hi) of the whole chunk go in first, while the
+        // sum is still small, and the hi*hi products last.
         const unsigned dH = tmem + bb * N;
         for (int ks = k0; ks < k1; ++ks) {
           const unsigned g = ks0 + ks;
           const unsigned long long so = (unsigned long long)(g % S::kSt) * kStageDesc;
           const unsigned ah = tmem + S::kTmemA + 16 * (g % S::kStA), al = ah + 8;
-          mma_tf32_ts(dH, ah, bh0 + so, idesc, ks == k0 ? 0u : 1u);
-          mma_tf32_ts(dH, ah, bl0 + so, idesc, 1u);
+          mma_tf32_ts(dH, ah, bl0 + so, idesc, ks == k0 ? 0u : 1u);
           mma_tf32_ts(dH, al, bh0 + so, idesc, 1u);
+        }
+        for (int ks = k0; ks < k1; ++ks) {
+          const unsigned g = ks0 + ks;
+          const unsigned long long so = (unsigned long long)(g % S::kSt) * kStageDesc;
+          mma_tf32_ts(dH, tmem + S::kTmemA + 16 * (g % S::kStA), bh0 + so, idesc, 1u);
         }
         mma_commit(&rel[gc % S::kRel]);
       }
