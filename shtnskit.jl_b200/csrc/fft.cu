@@ -100,7 +100,7 @@ __device__ __forceinline__ void fft_syn_body(const FFTJob<T>& J, int p0, int k, 
   const typename V2<T>::type* __restrict__ tw = J.tw;
   const typename V2<T>::type* __restrict__ twp = J.twp;
   using V = typename V2<T>::type;
-  const int N = fd.n, S = fft_row_stride(N);
+  const int sh = fft_padsh(fd, sizeof(V)), N = fd.n, S = fft_row_stride(N, sh);
   V* Z = reinterpret_cast<V*>(smem_raw);
   V* scratch = Z + H * S;
   T* gfac = reinterpret_cast<T*>(Z + ((GENERIC && fd.direct) ? 2 : 1) * H * S);
@@ -116,7 +116,7 @@ __device__ __forceinline__ void fft_syn_body(const FFTJob<T>& J, int p0, int k, 
       z.x = 0; z.y = 0;
       for (int idx = threadIdx.x; idx < H * zn; idx += blockDim.x) {
         const int h = idx / zn, q = idx - h * zn;
-        Z[h * S + fft_pad(zlo + q)] = z;
+        Z[h * S + fft_pad(zlo + q, sh)] = z;
       }
     }
   }
@@ -155,8 +155,8 @@ __device__ __forceinline__ void fft_syn_body(const FFTJob<T>& J, int p0, int k, 
         V a, b;
         a.x = XN.x - XS.y; a.y = XN.y + XS.x;
         b.x = XN.x + XS.y; b.y = XS.x - XN.y;
-        Z[h * S + fft_pad(m)] = a;
-        Z[h * S + fft_pad(N - m)] = b;
+        Z[h * S + fft_pad(m, sh)] = a;
+        Z[h * S + fft_pad(N - m, sh)] = b;
       }
     }
   }
@@ -182,7 +182,7 @@ __device__ __forceinline__ void fft_syn_body(const FFTJob<T>& J, int p0, int k, 
       T vn[H], vs[H];
 #pragma unroll
       for (int h = 0; h < H; ++h) {
-        const V z = Z[h * S + fft_pad(q)];
+        const V z = Z[h * S + fft_pad(q, sh)];
         vn[h] = z.x * gfac[h];
         vs[h] = z.y * gfac[h];
       }
@@ -223,7 +223,7 @@ __device__ __forceinline__ void fft_ana_body(const FFTJob<T>& J, int p0, int k, 
   const typename V2<T>::type* __restrict__ tw = J.tw;
   const typename V2<T>::type* __restrict__ twp = J.twp;
   using V = typename V2<T>::type;
-  const int N = fd.n, S = fft_row_stride(N);
+  const int sh = fft_padsh(fd, sizeof(V)), N = fd.n, S = fft_row_stride(N, sh);
   V* Z = reinterpret_cast<V*>(smem_raw);
   V* scratch = Z + H * S;
   T* wfac = reinterpret_cast<T*>(Z + ((GENERIC && fd.direct) ? 2 : 1) * H * S);
@@ -266,7 +266,7 @@ __device__ __forceinline__ void fft_ana_body(const FFTJob<T>& J, int p0, int k, 
       V z;
       z.x = vn[h];
       z.y = vs[h];
-      Z[h * S + fft_pad(j)] = z;
+      Z[h * S + fft_pad(j, sh)] = z;
     }
   }
   __syncthreads();
@@ -276,8 +276,8 @@ __device__ __forceinline__ void fft_ana_body(const FFTJob<T>& J, int p0, int k, 
     const int im = idx / H, h = idx - im * H;
     if (h >= hv) continue;
     const int m = im * P.mres;
-    const V Zm = Z[h * S + fft_pad(rev[m])];
-    V Zc = Z[h * S + fft_pad(rev[m == 0 ? 0 : N - m])];
+    const V Zm = Z[h * S + fft_pad(rev[m], sh)];
+    V Zc = Z[h * S + fft_pad(rev[m == 0 ? 0 : N - m], sh)];
     Zc.y = -Zc.y;
     const V sum = cadd(Zm, Zc), d = csub(Zm, Zc);
     V XN, XS;
@@ -391,7 +391,7 @@ static FFTJob<T> fft_job(const shtb_plan* p, const int* perm, const typename V2<
 // threads with half the pairs measured slower on B200: their grid segments shrink to
 // 16 bytes and each FFT has half the threads.
 static int fft_pick_h(const FFTDesc& fd, size_t celem, int npair) {
-  const size_t S = (size_t)fft_row_stride(fd.n);
+  const size_t S = (size_t)fft_row_stride(fd.n, fft_padsh(fd, celem));
   int h = 16;
   while (h > 1 && (size_t)h * S * celem * (fd.direct ? 2 : 1) + 16 * 8 > 200 * 1024) h >>= 1;
   while (h > 1 && h / 2 >= npair) h >>= 1;
@@ -399,7 +399,7 @@ static int fft_pick_h(const FFTDesc& fd, size_t celem, int npair) {
 }
 
 static size_t fft_smem(const FFTDesc& fd, size_t celem, int h) {
-  return (size_t)h * fft_row_stride(fd.n) * celem * (fd.direct ? 2 : 1) + (size_t)h * 8 + 16;
+  return (size_t)h * fft_row_stride(fd.n, fft_padsh(fd, celem)) * celem * (fd.direct ? 2 : 1) + (size_t)h * 8 + 16;
 }
 
 static bool fft_generic(const shtb_plan* p) {

@@ -46,8 +46,11 @@ template <typename V> __device__ __forceinline__ V crot(V a, int dir) {
   return r;
 }
 
-__device__ __forceinline__ int fft_pad(int n) { return n + (n >> 3); }
-__host__ __device__ inline int fft_row_stride(int n) { return n + (n >> 3) + 1; }
+__device__ __forceinline__ int fft_pad(int n, int sh) { return n + (n >> sh); }
+__host__ __device__ inline int fft_row_stride(int n, int sh) { return n + (n >> sh) + 1; }
+// Skew of a row of complex elements of celem bytes: the plan's choice for FP32 (8-byte
+// elements); FP64 rows (16-byte elements) measured fastest with i + i/8 at every length.
+__host__ __device__ inline int fft_padsh(const FFTDesc& fd, size_t celem) { return celem == 8 ? fd.padsh : 3; }
 
 // In-register DFT of RADIX points in direction dir. Generic odd radices use the
 // twiddle table tw[t] = exp(-2 pi i t / N) with step twstep = N / radix.
@@ -133,7 +136,8 @@ __device__ __forceinline__ void dft_small(V* u, int dir, const V* __restrict__ t
 // thread loads two groups before computing either so their loads overlap.
 template <typename T, typename V, int RADIX>
 __device__ __forceinline__ void dif_group_load(const V* X, int S, int N, int span, unsigned mrow, unsigned mspan,
-                                               int per_row, int r, int b, V* u, int& rowoff, int& base, int& j) {
+                                               int per_row, int r, int b, V* u, int& rowoff, int& base, int& j,
+                                               int sh) {
   const int f = mrow ? (int)__umulhi((unsigned)b, mrow) : b;
   const int t = b - f * per_row;
   const int blk = mspan ? (int)__umulhi((unsigned)t, mspan) : t;
@@ -142,12 +146,13 @@ __device__ __forceinline__ void dif_group_load(const V* X, int S, int N, int spa
   rowoff = f * S;
 #pragma unroll
   for (int q = 0; q < RADIX; ++q)
-    if (q < r) u[q] = X[rowoff + fft_pad(base + q * span)];
+    if (q < r) u[q] = X[rowoff + fft_pad(base + q * span, sh)];
 }
 
 template <typename T, typename V, int RADIX>
 __device__ __forceinline__ void dif_group_finish(V* X, int span, int r, const V* __restrict__ tw, int N,
-                                                 const V* __restrict__ twp, int dir, V* u, int rowoff, int base, int j) {
+                                                 const V* __restrict__ twp, int dir, V* u, int rowoff, int base, int j,
+                                                 int sh) {
   dft_small<T, V, RADIX>(u, dir, tw, N / r, r);
   if (j != 0) {
 #pragma unroll
@@ -161,12 +166,12 @@ __device__ __forceinline__ void dif_group_finish(V* X, int span, int r, const V*
   }
 #pragma unroll
   for (int q = 0; q < RADIX; ++q)
-    if (q < r) X[rowoff + fft_pad(base + q * span)] = u[q];
+    if (q < r) X[rowoff + fft_pad(base + q * span, sh)] = u[q];
 }
 
 template <typename T, typename V, int RADIX>
 __device__ __forceinline__ void dif_pass(V* X, int F, int N, int S, int Ns, int radix_rt, const V* __restrict__ tw,
-                                         const V* __restrict__ twp, unsigned mrow, unsigned mspan, int dir) {
+                                         const V* __restrict__ twp, unsigned mrow, unsigned mspan, int dir, int sh) {
   const int r = (RADIX >= 7) ? radix_rt : RADIX;
   const int span = Ns / r;            // distance between group members
   const int per_row = N / r;          // groups per row
@@ -179,13 +184,13 @@ __device__ __forceinline__ void dif_pass(V* X, int F, int N, int S, int Ns, int 
     V u0[RADIX], u1[kTwo ? RADIX : 1];
     int ro0, ba0, j0, ro1 = 0, ba1 = 0, j1 = 0;
     const bool two = kTwo && (b + bd < total);
-    dif_group_load<T, V, RADIX>(X, S, N, span, mrow, mspan, per_row, r, b, u0, ro0, ba0, j0);
+    dif_group_load<T, V, RADIX>(X, S, N, span, mrow, mspan, per_row, r, b, u0, ro0, ba0, j0, sh);
     if constexpr (kTwo) {
-      if (two) dif_group_load<T, V, RADIX>(X, S, N, span, mrow, mspan, per_row, r, b + bd, u1, ro1, ba1, j1);
+      if (two) dif_group_load<T, V, RADIX>(X, S, N, span, mrow, mspan, per_row, r, b + bd, u1, ro1, ba1, j1, sh);
     }
-    dif_group_finish<T, V, RADIX>(X, span, r, tw, N, twp, dir, u0, ro0, ba0, j0);
+    dif_group_finish<T, V, RADIX>(X, span, r, tw, N, twp, dir, u0, ro0, ba0, j0, sh);
     if constexpr (kTwo) {
-      if (two) dif_group_finish<T, V, RADIX>(X, span, r, tw, N, twp, dir, u1, ro1, ba1, j1);
+      if (two) dif_group_finish<T, V, RADIX>(X, span, r, tw, N, twp, dir, u1, ro1, ba1, j1, sh);
     }
   }
   __syncthreads();
@@ -196,7 +201,7 @@ __device__ __forceinline__ void dif_pass(V* X, int F, int N, int S, int Ns, int 
 template <typename T, typename V, bool GENERIC>
 __device__ void fft_rows(V* X, V* scratch, int F, int S, const FFTDesc& fd, const V* __restrict__ tw,
                          const V* __restrict__ twp, int dir) {
-  const int N = fd.n;
+  const int N = fd.n, sh = fft_padsh(fd, sizeof(V));
   if (GENERIC && fd.direct) {
     // O(N^2) DFT into scratch, written at natural positions (rev = identity in direct mode)
     for (int idx = threadIdx.x; idx < F * N; idx += blockDim.x) {
@@ -207,16 +212,16 @@ __device__ void fft_rows(V* X, V* scratch, int F, int S, const FFTDesc& fd, cons
       for (int n = 0; n < N; ++n) {
         V wv = tw[t];
         if (dir > 0) wv.y = -wv.y;
-        acc = cadd(acc, cmul(X[(size_t)f * S + fft_pad(n)], wv));
+        acc = cadd(acc, cmul(X[(size_t)f * S + fft_pad(n, sh)], wv));
         t += k;
         if (t >= N) t -= N;
       }
-      scratch[(size_t)f * S + fft_pad(k)] = acc;
+      scratch[(size_t)f * S + fft_pad(k, sh)] = acc;
     }
     __syncthreads();
     for (int idx = threadIdx.x; idx < F * N; idx += blockDim.x) {
       const int f = idx / N, k = idx - f * N;
-      X[(size_t)f * S + fft_pad(k)] = scratch[(size_t)f * S + fft_pad(k)];
+      X[(size_t)f * S + fft_pad(k, sh)] = scratch[(size_t)f * S + fft_pad(k, sh)];
     }
     __syncthreads();
     return;
@@ -227,13 +232,13 @@ __device__ void fft_rows(V* X, V* scratch, int F, int S, const FFTDesc& fd, cons
     const V* tp = twp + fd.twoff[s];
     const unsigned mr = fd.mrow[s], ms = fd.mspan[s];
     switch (r) {
-      case 2: dif_pass<T, V, 2>(X, F, N, S, Ns, 2, tw, tp, mr, ms, dir); break;
-      case 3: dif_pass<T, V, 3>(X, F, N, S, Ns, 3, tw, tp, mr, ms, dir); break;
-      case 4: dif_pass<T, V, 4>(X, F, N, S, Ns, 4, tw, tp, mr, ms, dir); break;
-      case 5: dif_pass<T, V, 5>(X, F, N, S, Ns, 5, tw, tp, mr, ms, dir); break;
-      case 8: dif_pass<T, V, 8>(X, F, N, S, Ns, 8, tw, tp, mr, ms, dir); break;
+      case 2: dif_pass<T, V, 2>(X, F, N, S, Ns, 2, tw, tp, mr, ms, dir, sh); break;
+      case 3: dif_pass<T, V, 3>(X, F, N, S, Ns, 3, tw, tp, mr, ms, dir, sh); break;
+      case 4: dif_pass<T, V, 4>(X, F, N, S, Ns, 4, tw, tp, mr, ms, dir, sh); break;
+      case 5: dif_pass<T, V, 5>(X, F, N, S, Ns, 5, tw, tp, mr, ms, dir, sh); break;
+      case 8: dif_pass<T, V, 8>(X, F, N, S, Ns, 8, tw, tp, mr, ms, dir, sh); break;
       default:
-        if constexpr (GENERIC) dif_pass<T, V, 13>(X, F, N, S, Ns, r, tw, tp, mr, ms, dir);
+        if constexpr (GENERIC) dif_pass<T, V, 13>(X, F, N, S, Ns, r, tw, tp, mr, ms, dir, sh);
         break;
     }
     Ns /= r;

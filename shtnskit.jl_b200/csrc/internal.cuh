@@ -64,6 +64,7 @@ struct FFTDesc {
   int nrad;
   int rad[24];
   bool direct;             // a prime factor above the largest register radix: O(N^2) DFT
+  int padsh;               // shared-memory index skew: element i at i + (i >> padsh)
   int twoff[24];           // pass s twiddles start at twoff[s] in the per-pass table
   unsigned mrow[24];       // floor(2^32 / (n / rad[s])) + 1, or 0 when n / rad[s] == 1
   unsigned mspan[24];      // the same for the group span Ns / rad[s]

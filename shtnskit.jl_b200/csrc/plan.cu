@@ -141,6 +141,9 @@ static bool factor_fft(int n, FFTDesc& d) {
     d.direct = true;
     d.nrad = 0;
   }
+  // FP32 rows: skew i + i/16 leaves every pass of a power-of-two length free of bank
+  // conflicts; mixed radices (odd last passes) do better with i + i/8 (fft_padsh).
+  d.padsh = ((n & (n - 1)) == 0) ? 4 : 3;
   int off = 0, Ns = n;
   for (int s = 0; s < d.nrad; ++s) {
     const int r = d.rad[s], span = Ns / r;
