@@ -277,16 +277,11 @@ def run_ours(args):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
+    from shtb200.distributed import barrier
+    from shtb200.distributed import max_over_ranks as _max
 
     def max_over_ranks(v: float) -> float:
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return _max(v, dev)
 
     L, nf = args.lmax, args.nfields
     nlat, nlon = L + 1, 2 * (L + 1)
@@ -546,12 +541,10 @@ def run_uneven(args):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
 
+    from shtb200.distributed import max_over_ranks as _max
+
     def max_over_ranks(v: float) -> float:
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return _max(v, dev)
 
     lib = _lib.load()
     lmaxes = uneven_lmaxes()

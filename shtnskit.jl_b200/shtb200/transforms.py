@@ -514,6 +514,37 @@ def analysis_sphtor_batch(cfg: SHTConfig, Vt, Vp, *, use_rfft: bool = False, lca
     return _sphtor_anal(cfg, Vt, Vp, True, use_rfft, lcap)
 
 
+def synthesis_qst(cfg: SHTConfig, Qlm, Slm, Tlm, *, real_output: bool = True, use_rfft: bool = False,
+                  lcap: int | None = None):
+    """Radial/spheroidal/toroidal synthesis to ``(Vr, Vt, Vp)`` (src/qst_transforms.jl:112-135):
+    the scalar synthesis of Q and the spheroidal/toroidal synthesis of (S, T) on one grid."""
+    vr = synthesis(cfg, Qlm, real_output=real_output, use_rfft=use_rfft, lcap=lcap)
+    vt, vp = synthesis_sphtor(cfg, Slm, Tlm, real_output=real_output, use_rfft=use_rfft, lcap=lcap)
+    return vr, vt, vp
+
+
+def analysis_qst(cfg: SHTConfig, Vr, Vt, Vp, *, use_rfft: bool = False, lcap: int | None = None):
+    """``(Vr, Vt, Vp)`` to ``(Q, S, T)`` (src/qst_transforms.jl:138-160)."""
+    q = analysis(cfg, Vr, use_rfft=use_rfft, lcap=lcap)
+    s, t = analysis_sphtor(cfg, Vt, Vp, use_rfft=use_rfft, lcap=lcap)
+    return q, s, t
+
+
+def synthesis_qst_batch(cfg: SHTConfig, Qlm, Slm, Tlm, *, real_output: bool = True, use_rfft: bool = False,
+                        lcap: int | None = None):
+    """Batched QST synthesis (src/batch_transforms.jl:830-905)."""
+    vr = synthesis_batch(cfg, Qlm, real_output=real_output, use_rfft=use_rfft, lcap=lcap)
+    vt, vp = synthesis_sphtor_batch(cfg, Slm, Tlm, real_output=real_output, use_rfft=use_rfft, lcap=lcap)
+    return vr, vt, vp
+
+
+def analysis_qst_batch(cfg: SHTConfig, Vr, Vt, Vp, *, use_rfft: bool = False, lcap: int | None = None):
+    """Batched QST analysis (src/batch_transforms.jl:905-985)."""
+    q = analysis_batch(cfg, Vr, use_rfft=use_rfft, lcap=lcap)
+    s, t = analysis_sphtor_batch(cfg, Vt, Vp, use_rfft=use_rfft, lcap=lcap)
+    return q, s, t
+
+
 def gpu_clear_cache(cfg: SHTConfig | None = None) -> None:
     """Release device plans (``gpu_clear_cache!``, src/device_utils.jl:296-301)."""
     if cfg is not None:

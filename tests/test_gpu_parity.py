@@ -67,11 +67,10 @@ def test_shtns37_fixture(fid):
         Q, S, T, Vr, Vt, Vp = (g(n) for n in "Q S T Vr Vt Vp".split())
         b = Q.ndim == 3
         if not analysis_only:
-            assert isapprox(host(sht.synthesis(cfg, Q)), Vr, atol, rtol)
-            vt, vp = sht.synthesis_sphtor(cfg, S, T)
+            vr, vt, vp = (sht.synthesis_qst_batch if b else sht.synthesis_qst)(cfg, Q, S, T)
+            assert isapprox(host(vr), Vr, atol, rtol)
             assert isapprox(host(vt), Vt, atol, rtol) and isapprox(host(vp), Vp, atol, rtol)
-        q = (sht.analysis_batch if b else sht.analysis)(cfg, Vr)
-        s, t = (sht.analysis_sphtor_batch if b else sht.analysis_sphtor)(cfg, Vt, Vp)
+        q, s, t = (sht.analysis_qst_batch if b else sht.analysis_qst)(cfg, Vr, Vt, Vp)
         assert isapprox(host(q), Q, atol, rtol)
         assert isapprox(host(s), S, atol, rtol) and isapprox(host(t), T, atol, rtol)
     else:
