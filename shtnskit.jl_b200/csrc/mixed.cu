@@ -304,11 +304,11 @@ __device__ __forceinline__ unsigned gemm_cta_setup(const Bars& B) {
   const int tid = threadIdx.x, warp = tid >> 5;
   if (tid == 0) {
     for (int s = 0; s < Smem<N>::kSt; ++s) {
-      mbar_init(&B.full[s], 128);
+      mbar_init(&B.full[s], 4);    // one arrival per splitter warp of the K-step's group
       mbar_init(&B.ldfull[s], 1);
     }
     for (int s = 0; s < Smem<N>::kRel; ++s) mbar_init(&B.rel[s], 1);
-    for (int b = 0; b < 2; ++b) mbar_init(&B.acce[b], 256);
+    for (int b = 0; b < 2; ++b) mbar_init(&B.acce[b], 8);   // one arrival per promotion warp
     *B.abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -413,11 +413,13 @@ __device__ __forceinline__ void gemm_tile(const Args& a, const TileCoord& tc, un
       for (int ks = ((ks0 & 1) == (unsigned)sgp) ? 0 : 1; ks < nks; ks += 2) {
         const unsigned g = ks0 + ks;
         const int b = g % S::kSt, ba = g % S::kStA;
-        if (!mbar_wait(&ldfull[b], (g / S::kSt) & 1, abort_flag, a.err)) break;
-        if (g >= S::kStA) {
+        bool ok = mbar_wait(&ldfull[b], (g / S::kSt) & 1, abort_flag, a.err);
+        if (ok && g >= S::kStA) {
           const unsigned q = my_slots[ba];
-          if (!mbar_wait(&rel[q % S::kRel], (q / S::kRel) & 1, abort_flag, a.err)) break;
+          ok = mbar_wait(&rel[q % S::kRel], (q / S::kRel) & 1, abort_flag, a.err);
         }
+        // the warp leaves together (the TMEM stores below are warp-collective)
+        if (!__all_sync(0xffffffffu, ok)) break;
         my_slots[ba] = c0 + ks / kChunk;
         // the MMAs that last read TMEM slot ba have completed
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -429,7 +431,8 @@ __device__ __forceinline__ void gemm_tile(const Args& a, const TileCoord& tc, un
         split4(x1, h1, l1);
         tmem_st8x2(ta_lane + (unsigned)(S::kTmemA + 16 * ba), h, h1, l, l1);
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        mbar_arrive(&full[b]);
+        __syncwarp();   // one arrival per warp: 128 arrivals on one word serialize
+        if (lane == 0) mbar_arrive(&full[b]);
       }
     }
   } else if (warp == 8) {
@@ -484,8 +487,8 @@ __device__ __forceinline__ void gemm_tile(const Args& a, const TileCoord& tc, un
       const unsigned gc = c0 + c;
       const int bb = gc & 1;
       if (ok) ok = mbar_wait(&rel[gc % S::kRel], (gc / S::kRel) & 1, abort_flag, a.err);
+      ok = __all_sync(0xffffffffu, ok);   // warp-uniform: the TMEM loads are warp-collective
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      __syncwarp();
       const unsigned dH = tmem + lane_base + bb * N + h * (N / 2);
 #pragma unroll
       for (int i = 0; i < N / 2; i += kLd) {
@@ -495,7 +498,8 @@ __device__ __forceinline__ void gemm_tile(const Args& a, const TileCoord& tc, un
         for (int u = 0; u < kLd; ++u) acc[i + u] += v[u];
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      mbar_arrive(&acce[bb]);
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acce[bb]);
       if (!ok) break;
     }
     if (ok) {
