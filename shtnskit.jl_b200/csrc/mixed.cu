@@ -78,6 +78,9 @@ __device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned coun
 __device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
+__device__ __forceinline__ void mbar_arrive_cnt(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
 __device__ __forceinline__ bool mbar_test(unsigned long long* bar, unsigned parity) {
   unsigned ok;
   asm volatile(
@@ -234,18 +237,21 @@ __device__ __forceinline__ float coef_factor(const Args& a, int l, int m) {
 template <int N>
 struct Smem {
   static constexpr int kTileB = N * kK * 4;
-  // per stage: A as loaded (FP32), B_hi, B_lo (one parity class per CTA); the split A
-  // tiles live in TMEM
-  static constexpr int kStage = kTileBytesA + 2 * kTileB;
-  // Ring depth: 16 shared-memory stages (enough bulk copies in flight to cover the
-  // global-memory latency) and 16 TMEM slots for the split A tiles.
-  static constexpr int kSt = 16;
+  // One stage holds a chunk: kChunk K-steps of A as loaded (FP32), then of B_hi and B_lo
+  // (one parity class per CTA), each operand filled by one bulk copy; the split A tiles
+  // live in TMEM.
+  static constexpr int kStageA = kChunk * kTileBytesA;
+  static constexpr int kStage = kChunk * (kTileBytesA + 2 * kTileB);
+  // Ring depth: 192 KB of stages per CTA (80 KB for the two 16-column CTAs of an SM),
+  // 16 per-chunk split barriers and 16 TMEM slots for the split A tiles.
+  static constexpr int kSt = (N == 128) ? 4 : (N == 64) ? 6 : (N == 32) ? 8 : 4;
+  static constexpr int kFull = 16;   // per-chunk split barriers
   static constexpr int kStA = (N == 16) ? 8 : 16;   // two 16-column CTAs share an SM's TMEM
-  static constexpr int kRel = 16;   // chunk-release barriers (>= kSt, see gemm_tile)
+  static constexpr int kRel = 16;   // chunk-release barriers (>= kSt and kStA, see the tile roles below)
   static constexpr int kBar = kSt * kStage;
-  // barriers: full[kSt], ldfull[kSt], rel[kRel], acce[2]; then the loader's stage->chunk
-  // map (kSt ints), the splitters' slot->chunk maps (256 x kStA ints), TMEM slot, abort flag
-  static constexpr int kBytes = kBar + (2 * kSt + kRel + 2) * 8 + kSt * 4 + 256 * kStA * 4 + 16;
+  // barriers: full[kFull], ldfull[kSt], rel[kRel], acce[2]; then the splitters' slot->chunk
+  // maps (256 x kStA ints), TMEM slot, abort flag
+  static constexpr int kBytes = kBar + (kFull + kSt + kRel + 2) * 8 + 256 * kStA * 4 + 16;
   // TMEM: chunk accumulators H0 [0, N) and H1 [N, 2N); A slot s: hi at 2N + 16 s, lo at
   // 2N + 16 s + 8
   static constexpr int kTmemA = 2 * N;
@@ -253,6 +259,7 @@ struct Smem {
   static constexpr int kTmemCols = kTmemNeed <= 32 ? 32 : kTmemNeed <= 64 ? 64 : kTmemNeed <= 128 ? 128
                                    : kTmemNeed <= 256 ? 256 : 512;
   static_assert(kTmemNeed <= 512, "TMEM columns");
+  static_assert(kSt <= kRel && kStA <= kRel, "release barriers");
 };
 
 // Narrow tiles (N = 16: up to 8 fields) leave the tensor core mostly idle, so two CTAs
@@ -269,7 +276,6 @@ struct TileCoord {
 // Shared-memory barriers of a GEMM CTA (initialised once per CTA).
 struct Bars {
   unsigned long long *full, *ldfull, *rel, *acce;
-  unsigned* stage_chunk;   // [kSt] chunk of the K-step that last used each stage (loader)
   unsigned* slot_chunk;    // [256][kStA] the same for TMEM A slots (one row per splitter thread)
   unsigned* tmem_slot;
   volatile int* abort_flag;
@@ -279,12 +285,11 @@ template <int N>
 __device__ __forceinline__ Bars gemm_bars(unsigned char* sm) {
   using S = Smem<N>;  // barriers follow the stage ring
   Bars B;
-  B.full = reinterpret_cast<unsigned long long*>(sm + S::kBar);   // [kSt] stage split (A in TMEM)
-  B.ldfull = B.full + S::kSt;     // [kSt] bulk copies of the stage landed
+  B.full = reinterpret_cast<unsigned long long*>(sm + S::kBar);   // [kFull] chunk gc split (A in TMEM)
+  B.ldfull = B.full + S::kFull;   // [kSt] bulk copies of the stage landed
   B.rel = B.ldfull + S::kSt;      // [kRel] MMAs of chunk q done (q % kRel)
   B.acce = B.rel + S::kRel;       // [2] TMEM chunk buffer b drained by the promotion warps
-  B.stage_chunk = reinterpret_cast<unsigned*>(B.acce + 2);
-  B.slot_chunk = B.stage_chunk + S::kSt;
+  B.slot_chunk = reinterpret_cast<unsigned*>(B.acce + 2);
   B.tmem_slot = B.slot_chunk + 256 * S::kStA;
   B.abort_flag = reinterpret_cast<volatile int*>(B.tmem_slot + 1);
   return B;
@@ -303,10 +308,9 @@ template <int N>
 __device__ __forceinline__ unsigned gemm_cta_setup(const Bars& B) {
   const int tid = threadIdx.x, warp = tid >> 5;
   if (tid == 0) {
-    for (int s = 0; s < Smem<N>::kSt; ++s) {
-      mbar_init(&B.full[s], 4);    // one arrival per splitter warp of the K-step's group
-      mbar_init(&B.ldfull[s], 1);
-    }
+    // one arrival per splitter warp and K-step of a full chunk (4 warps x kChunk)
+    for (int s = 0; s < Smem<N>::kFull; ++s) mbar_init(&B.full[s], 4 * kChunk);
+    for (int s = 0; s < Smem<N>::kSt; ++s) mbar_init(&B.ldfull[s], 1);
     for (int s = 0; s < Smem<N>::kRel; ++s) mbar_init(&B.rel[s], 1);
     for (int b = 0; b < 2; ++b) mbar_init(&B.acce[b], 8);   // one arrival per promotion warp
     *B.abort_flag = 0;
@@ -333,204 +337,276 @@ __device__ __forceinline__ void gemm_cta_teardown(unsigned tmem) {
   }
 }
 
-// One GEMM tile. MODE 0: synthesis, MODE 1: analysis; N = columns per CTA (2 x fields).
-// A persistent CTA runs many tiles through the same barriers: ks0 and c0 count the
-// K-steps and chunks of the tiles before this one, which fixes every stage index and
-// barrier phase. Callers separate tiles with __syncthreads (the cross-term TMEM buffer
-// is reused).
+// GEMM tiles. MODE 0: synthesis, MODE 1: analysis; N = columns per CTA (2 x fields).
 //
-// Synchronisation: the MMA issuer waits for all K-steps of a chunk (kChunk K-steps) to
-// be split, issues their 3 kChunk MMAs back to back and commits once, to rel[chunk %
-// kRel]. That one barrier releases the chunk's shared-memory stages (loader), its TMEM
-// A slots (splitters) and its accumulator (promotion warps); producers look up the
-// chunk of a stage's or slot's previous K-step in small per-role maps. kRel >= kSt
-// keeps a waiter from ever seeing a barrier two phases ahead.
-template <int MODE, int N>
-__device__ __forceinline__ void gemm_tile(const Args& a, const TileCoord& tc, unsigned char* sm, const Bars& B,
-                                          unsigned tmem, unsigned ks0, unsigned c0) {
-  using S = Smem<N>;
-  unsigned long long* full = B.full;
-  unsigned long long* ldfull = B.ldfull;
-  unsigned long long* rel = B.rel;
-  unsigned long long* acce = B.acce;
-  volatile int* abort_flag = B.abort_flag;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const PlanDev& P = a.P;
-  const int npair = P.npair;
-  const int par = tc.par, im = tc.im, p0 = tc.p0, j0 = tc.j0, kb = tc.kb;
-  const int m = im * P.mres;
-  const long long sg = a.seg[2 * im + par];
-  const long long ln = a.seg[2 * im + par + 1] - sg;
-  const int nks = tile_ksteps<MODE>(a, tc);
-  const int nch = (nks + kChunk - 1) / kChunk;
-  // TMEM: chunk buffer b (hi*hi) at column b*N; the cross terms of the whole tile at 2N
+// A CTA runs a sequence of tiles (tile i = blockIdx.x, blockIdx.x + gridDim.x, ...), and
+// each role walks that sequence on its own: the loader and splitters run ahead into the
+// next tile while the promotion warps still drain and store the previous one. ks0 and
+// c0, counted identically by every role, number the K-steps and chunks of the tiles
+// before the current one and fix every stage index, TMEM slot and barrier phase.
+//
+// Synchronisation: chunk gc (kChunk K-steps, fewer at the end of a tile) occupies
+// shared-memory stage gc % kSt. The MMA issuer waits for all K-steps of a chunk to be
+// split (one barrier per chunk, full[gc % kFull], which every splitter warp arrives on
+// once per K-step), issues their 3 kChunk MMAs back to back and commits once, to
+// rel[gc % kRel]. Each mbarrier wait costs a few hundred cycles even when the phase has
+// completed, so the MMA issuer waits on two barriers per chunk only.
+// That one barrier releases the chunk's stage (loader), its TMEM A slots (splitters)
+// and its accumulator (promotion warps); the splitters look up the chunk of a slot's
+// previous K-step in a small per-thread map. kRel >= kSt, kStA keeps a waiter from ever
+// seeing a barrier two phases ahead.
+struct TileInfo {
+  int m, nks, nch;
+  long long sg, ln;   // table segment start and rows of (im, par)
+  int arows;          // rows of the A tile image (128, fewer in the last analysis tile)
+  unsigned bstr;      // bytes from one K-step's B tile to the next in a stage
+};
 
-  if (warp < 8 || warp == 17) {
-    // ------------------------------------------------------------- producers
-    // One thread (warp 17, lane 0) fills the shared-memory ring, kSt K-steps ahead, with
-    // three bulk copies per K-step: the FP32 A tile image and the pre-split B tile images
-    // (hi, lo). Two groups of splitter warps (0-3 and 4-7, even and odd K-steps) split each
-    // landed A tile into TF32 hi/lo and store it into a TMEM slot, which the MMAs read as
-    // their A operand.
-    const int t = tid & 127;
-    if (warp == 17) {
-      if (lane == 0) {
-        // A tile images: synthesis [ptile][ks] blocks of 4 KB after the segment start;
-        // analysis [jtile][ks] blocks of rows*32 bytes (rows = 128, fewer in the last jtile)
-        const float* aseg = a.tab + sg * a.npp;
-        const int arows = (MODE == 0) ? kM : min(kM, (int)ln - j0);
-        const float* a0 =
-            (MODE == 0) ? aseg + (long long)(p0 / kM) * (ln / kK) * (kM * kK) : aseg + (long long)j0 * a.npp;
-        const unsigned abytes = (unsigned)arows * kK * 4;
-        // B tile images: region rb + ks of nfp x 16 floats, this CTA's block of 64 fields
-        const int nfp = btile_nfp(a.nf);
-        const long long rb = (MODE == 0) ? sg / kK : (long long)(im * 2 + par) * ((npair + kK - 1) / kK);
-        const long long boff = rb * nfp * 16 + (long long)(kb >> 6) * 1024;
-        const unsigned bbytes = (unsigned)min(64, nfp - kb) * 64;
-        for (int ks = 0; ks < nks; ++ks) {
-          const unsigned g = ks0 + ks;
-          const int b = g % S::kSt;
-          if (g >= S::kSt) {
-            const unsigned q = B.stage_chunk[b];
-            if (!mbar_wait(&rel[q % S::kRel], (q / S::kRel) & 1, abort_flag, a.err)) break;
-          }
-          B.stage_chunk[b] = c0 + ks / kChunk;
-          unsigned char* st = sm + (size_t)b * S::kStage;
-          const long long bo = boff + (long long)ks * nfp * 16;
-          mbar_expect_tx(&ldfull[b], abytes + 2 * bbytes);
-          bulk_g2s(st, a0 + (long long)ks * arows * kK, abytes, &ldfull[b]);
-          bulk_g2s(st + kTileBytesA, a.bhi + bo, bbytes, &ldfull[b]);
-          bulk_g2s(st + kTileBytesA + S::kTileB, a.blo + bo, bbytes, &ldfull[b]);
-        }
-      }
+template <int MODE>
+__device__ __forceinline__ TileInfo tile_info(const Args& a, const TileCoord& tc) {
+  TileInfo T;
+  T.m = tc.im * a.P.mres;
+  T.sg = a.seg[2 * tc.im + tc.par];
+  T.ln = a.seg[2 * tc.im + tc.par + 1] - T.sg;
+  T.nks = tile_ksteps<MODE>(a, tc);
+  T.nch = (T.nks + kChunk - 1) / kChunk;
+  T.arows = (MODE == 0) ? kM : min(kM, (int)T.ln - tc.j0);
+  // B images of consecutive K-steps are contiguous when all fields fit one 64-field block
+  const int nfp = btile_nfp(a.nf);
+  T.bstr = (nfp <= 64) ? (unsigned)nfp * 64 : (unsigned)(kM / 2) * 64;
+  return T;
+}
+
+// One thread fills the shared-memory ring, kSt chunks ahead, with one bulk copy per
+// operand and chunk (the FP32 A tile images and the pre-split B tile images, hi and lo)
+// when the B images of the chunk are contiguous, one per K-step for B otherwise.
+template <int MODE, int N>
+__device__ __forceinline__ bool loader_tile(const Args& a, const TileCoord& tc, const TileInfo& T, unsigned char* sm,
+                                            const Bars& B, unsigned c0) {
+  using S = Smem<N>;
+  const int npair = a.P.npair;
+  // A tile images: synthesis [ptile][ks] blocks of 4 KB after the segment start;
+  // analysis [jtile][ks] blocks of rows*32 bytes (rows = 128, fewer in the last jtile)
+  const float* aseg = a.tab + T.sg * a.npp;
+  const float* a0 = (MODE == 0) ? aseg + (long long)(tc.p0 / kM) * (T.ln / kK) * (kM * kK) : aseg + (long long)tc.j0 * a.npp;
+  const unsigned abytes = (unsigned)T.arows * kK * 4;
+  // B tile images: region rb + ks of nfp x 16 floats, this CTA's block of 64 fields
+  const int nfp = btile_nfp(a.nf);
+  const long long rb = (MODE == 0) ? T.sg / kK : (long long)(tc.im * 2 + tc.par) * ((npair + kK - 1) / kK);
+  const long long boff = rb * nfp * 16 + (long long)(tc.kb >> 6) * 1024;
+  const unsigned bbytes = (unsigned)min(64, nfp - tc.kb) * 64;
+  const bool bcontig = nfp <= 64;
+  const float* bh = a.bhi + boff;
+  const float* bl = a.blo + boff;
+  int* err = a.err;
+  for (int c = 0; c < T.nch; ++c) {
+    const unsigned gc = c0 + c;
+    const int st = gc % S::kSt;
+    if (gc >= S::kSt) {
+      const unsigned q = gc - S::kSt;   // the chunk that last used this stage
+      if (!mbar_wait(&B.rel[q % S::kRel], (q / S::kRel) & 1, B.abort_flag, err)) return false;
+    }
+    const int k0 = c * kChunk, nk = min(kChunk, T.nks - k0);
+    unsigned char* sa = sm + (size_t)st * S::kStage;
+    unsigned char* sbh = sa + S::kStageA;
+    unsigned char* sbl = sbh + kChunk * S::kTileB;
+    unsigned long long* bar = &B.ldfull[st];
+    mbar_expect_tx(bar, (unsigned)nk * (abytes + 2 * bbytes));
+    bulk_g2s(sa, a0 + (long long)k0 * T.arows * kK, nk * abytes, bar);
+    if (bcontig) {
+      bulk_g2s(sbh, bh + (long long)k0 * nfp * 16, nk * bbytes, bar);
+      bulk_g2s(sbl, bl + (long long)k0 * nfp * 16, nk * bbytes, bar);
     } else {
-      // Splitter thread t of group sg rounds row t of the A tile into TMEM lane t (its
-      // warp's quadrant) for the K-steps g with g % 2 == sg.
-      const int sgp = warp >> 2;
-      const unsigned ta_lane = tmem + ((unsigned)(32 * (warp & 3)) << 16);
-      const int o0 = tile_off(t, 0), o1 = tile_off(t, 1);
-      unsigned* my_slots = B.slot_chunk + (sgp * 128 + t) * S::kStA;
-      for (int ks = ((ks0 & 1) == (unsigned)sgp) ? 0 : 1; ks < nks; ks += 2) {
-        const unsigned g = ks0 + ks;
-        const int b = g % S::kSt, ba = g % S::kStA;
-        bool ok = mbar_wait(&ldfull[b], (g / S::kSt) & 1, abort_flag, a.err);
-        if (ok && g >= S::kStA) {
-          const unsigned q = my_slots[ba];
-          ok = mbar_wait(&rel[q % S::kRel], (q / S::kRel) & 1, abort_flag, a.err);
-        }
-        // the warp leaves together (the TMEM stores below are warp-collective)
-        if (!__all_sync(0xffffffffu, ok)) break;
-        my_slots[ba] = c0 + ks / kChunk;
-        // the MMAs that last read TMEM slot ba have completed
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const unsigned char* Ah = sm + (size_t)b * S::kStage;
-        const float4 x0 = *reinterpret_cast<const float4*>(Ah + o0);
-        const float4 x1 = *reinterpret_cast<const float4*>(Ah + o1);
-        float4 h, l, h1, l1;
-        split4(x0, h, l);
-        split4(x1, h1, l1);
-        tmem_st8x2(ta_lane + (unsigned)(S::kTmemA + 16 * ba), h, h1, l, l1);
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncwarp();   // one arrival per warp: 128 arrivals on one word serialize
-        if (lane == 0) mbar_arrive(&full[b]);
+      for (int s = 0; s < nk; ++s) {
+        bulk_g2s(sbh + s * S::kTileB, bh + (long long)(k0 + s) * nfp * 16, bbytes, bar);
+        bulk_g2s(sbl + s * S::kTileB, bl + (long long)(k0 + s) * nfp * 16, bbytes, bar);
       }
     }
-  } else if (warp == 8) {
-    // ------------------------------------------------------------- MMA issuer
-    if (lane == 0) {
-      const unsigned idesc = idesc_tf32<N>();
-      const unsigned long long bh0 = sdesc(sm + kTileBytesA), bl0 = sdesc(sm + kTileBytesA + S::kTileB);
-      constexpr unsigned long long kStageDesc = S::kStage >> 4;   // descriptor address step per stage
-      bool ok = true;
-      for (int c = 0; c < nch && ok; ++c) {
-        const unsigned gc = c0 + c;
-        const int bb = gc & 1;
-        if (gc >= 2 && !mbar_wait(&acce[bb], ((gc >> 1) - 1) & 1, abort_flag, a.err)) break;
-        const int k0 = c * kChunk, k1 = min(nks, k0 + kChunk);
-        for (int ks = k0; ks < k1 && ok; ++ks) {
-          const unsigned g = ks0 + ks;
-          ok = mbar_wait(&full[g % S::kSt], (g / S::kSt) & 1, abort_flag, a.err);
-        }
-        if (!ok) break;
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        // The accumulator rounds every addition toward zero at its current magnitude, so
-        // the small cross terms (hi*lo, lo*hi) of the whole chunk go in first, while the
-        // sum is still small, and the hi*hi products last.
-        const unsigned dH = tmem + bb * N;
-        for (int ks = k0; ks < k1; ++ks) {
-          const unsigned g = ks0 + ks;
-          const unsigned long long so = (unsigned long long)(g % S::kSt) * kStageDesc;
-          const unsigned ah = tmem + S::kTmemA + 16 * (g % S::kStA), al = ah + 8;
-          mma_tf32_ts(dH, ah, bl0 + so, idesc, ks == k0 ? 0u : 1u);
-          mma_tf32_ts(dH, al, bh0 + so, idesc, 1u);
-        }
-        for (int ks = k0; ks < k1; ++ks) {
-          const unsigned g = ks0 + ks;
-          const unsigned long long so = (unsigned long long)(g % S::kSt) * kStageDesc;
-          mma_tf32_ts(dH, tmem + S::kTmemA + 16 * (g % S::kStA), bh0 + so, idesc, 1u);
-        }
-        mma_commit(&rel[gc % S::kRel]);
-      }
+  }
+  return true;
+}
+
+// Splitter thread t of group sgp rounds row t of the A tile into TMEM lane t (its warp's
+// quadrant) for the K-steps g with g % 2 == sgp.
+template <int MODE, int N>
+__device__ __forceinline__ bool splitter_tile(const Args& a, const TileInfo& T, unsigned char* sm, const Bars& B,
+                                              unsigned tmem, unsigned ks0, unsigned c0) {
+  const unsigned astr = (unsigned)T.arows * kK * 4;   // A tile image bytes per K-step
+  using S = Smem<N>;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, t = tid & 127, sgp = warp >> 2;
+  const unsigned ta_lane = tmem + ((unsigned)(32 * (warp & 3)) << 16);
+  const int o0 = tile_off(t, 0), o1 = tile_off(t, 1);
+  unsigned* my_slots = B.slot_chunk + (sgp * 128 + t) * S::kStA;
+  for (int ks = ((ks0 & 1) == (unsigned)sgp) ? 0 : 1; ks < T.nks; ks += 2) {
+    const unsigned g = ks0 + ks, gc = c0 + ks / kChunk;
+    const int ba = g % S::kStA;
+    bool ok = mbar_wait(&B.ldfull[gc % S::kSt], (gc / S::kSt) & 1, B.abort_flag, a.err);
+    if (ok && g >= S::kStA) {
+      const unsigned q = my_slots[ba];
+      ok = mbar_wait(&B.rel[q % S::kRel], (q / S::kRel) & 1, B.abort_flag, a.err);
+    }
+    // the warp leaves together (the TMEM stores below are warp-collective)
+    if (!__all_sync(0xffffffffu, ok)) return false;
+    my_slots[ba] = c0 + ks / kChunk;
+    // the MMAs that last read TMEM slot ba have completed
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const unsigned char* Ah = sm + (size_t)(gc % S::kSt) * S::kStage + (ks % kChunk) * astr;
+    const float4 x0 = *reinterpret_cast<const float4*>(Ah + o0);
+    const float4 x1 = *reinterpret_cast<const float4*>(Ah + o1);
+    float4 h, l, h1, l1;
+    split4(x0, h, l);
+    split4(x1, h1, l1);
+    tmem_st8x2(ta_lane + (unsigned)(S::kTmemA + 16 * ba), h, h1, l, l1);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncwarp();   // one arrival per warp: 128 arrivals on one word serialize
+    // the last K-step of a short chunk also arrives for the missing ones
+    const int nk = min(kChunk, T.nks - (ks / kChunk) * kChunk);
+    if (lane == 0) mbar_arrive_cnt(&B.full[gc % S::kFull], (ks % kChunk == nk - 1) ? 1 + kChunk - nk : 1);
+  }
+  return true;
+}
+
+// One thread issues the MMAs, a chunk at a time, and commits once per chunk.
+template <int MODE, int N>
+__device__ __forceinline__ bool mma_tile(const Args& a, const TileInfo& T, unsigned char* sm, const Bars& B,
+                                         unsigned tmem, unsigned ks0, unsigned c0) {
+  using S = Smem<N>;
+  const unsigned idesc = idesc_tf32<N>();
+  const unsigned long long bh0 = sdesc(sm + S::kStageA), bl0 = sdesc(sm + S::kStageA + kChunk * S::kTileB);
+  constexpr unsigned long long kStageDesc = S::kStage >> 4;   // descriptor address step per stage
+  const unsigned long long kstepDesc = T.bstr >> 4;          // and per K-step within a stage
+  for (int c = 0; c < T.nch; ++c) {
+    const unsigned gc = c0 + c;
+    const int bb = gc & 1;
+    if (gc >= 2 && !mbar_wait(&B.acce[bb], ((gc >> 1) - 1) & 1, B.abort_flag, a.err)) return false;
+    const int k0 = c * kChunk, k1 = min(T.nks, k0 + kChunk);
+    if (!mbar_wait(&B.full[gc % S::kFull], (gc / S::kFull) & 1, B.abort_flag, a.err)) return false;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // The accumulator rounds every addition toward zero at its current magnitude, so
+    // the small cross terms (hi*lo, lo*hi) of the whole chunk go in first, while the
+    // sum is still small, and the hi*hi products last.
+    const unsigned dH = tmem + bb * N;
+    const unsigned long long sc = (unsigned long long)(gc % S::kSt) * kStageDesc;
+    for (int ks = k0; ks < k1; ++ks) {
+      const unsigned g = ks0 + ks;
+      const unsigned long long so = sc + (ks - k0) * kstepDesc;
+      const unsigned ah = tmem + S::kTmemA + 16 * (g % S::kStA), al = ah + 8;
+      mma_tf32_ts(dH, ah, bl0 + so, idesc, ks == k0 ? 0u : 1u);
+      mma_tf32_ts(dH, al, bh0 + so, idesc, 1u);
+    }
+    for (int ks = k0; ks < k1; ++ks) {
+      const unsigned g = ks0 + ks;
+      const unsigned long long so = sc + (ks - k0) * kstepDesc;
+      mma_tf32_ts(dH, tmem + S::kTmemA + 16 * (g % S::kStA), bh0 + so, idesc, 1u);
+    }
+    mma_commit(&B.rel[gc % S::kRel]);
+  }
+  return true;
+}
+
+// Promotion warps (9..16): drain each chunk into round-to-nearest FP32 sums, then store
+// the tile (the analysis also clears l < m and l > lcap in the first tile of an order).
+template <int MODE, int N>
+__device__ __forceinline__ bool promo_tile(const Args& a, const TileCoord& tc, const TileInfo& T, const Bars& B,
+                                           unsigned tmem, unsigned c0) {
+  using S = Smem<N>;
+  const PlanDev& P = a.P;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int q = warp & 3;                        // TMEM lane quadrant this warp may access
+  const int h = (warp - 9) >> 2;                 // column half
+  const int row = 32 * q + lane;
+  const unsigned lane_base = (unsigned)(32 * q) << 16;
+  constexpr int kLd = (N / 2 < 16) ? N / 2 : 16;   // columns per TMEM load
+  float acc[N / 2];
+#pragma unroll
+  for (int i = 0; i < N / 2; ++i) acc[i] = 0.f;
+  bool ok = true;
+  for (int c = 0; c < T.nch; ++c) {
+    const unsigned gc = c0 + c;
+    const int bb = gc & 1;
+    if (ok) ok = mbar_wait(&B.rel[gc % S::kRel], (gc / S::kRel) & 1, B.abort_flag, a.err);
+    ok = __all_sync(0xffffffffu, ok);   // warp-uniform: the TMEM loads are warp-collective
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const unsigned dH = tmem + lane_base + bb * N + h * (N / 2);
+#pragma unroll
+    for (int i = 0; i < N / 2; i += kLd) {
+      float v[kLd];
+      tmem_ld<kLd>(dH + i, v);
+#pragma unroll
+      for (int u = 0; u < kLd; ++u) acc[i + u] += v[u];
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&B.acce[bb]);
+    if (!ok) return false;
+  }
+  // Every Args field and the scale factor are read before the first store: the stores
+  // go through generic pointers, after which the compiler would reload them.
+  const int npair = P.npair, im = tc.im, par = tc.par, m = T.m, kb = tc.kb;
+  const int nf = a.nf, kf0 = kb + h * (N / 4);
+  const int nq = min(N / 4, nf - kf0);
+  if (MODE == 0) {
+    const int pr = tc.p0 + row;
+    if (pr < npair) {
+      const size_t fstride = (size_t)P.nm * 2 * npair;
+      float2* w = a.Wout + (((size_t)kf0 * P.nm + im) * 2 + par) * npair + pr;
+#pragma unroll
+      for (int qq = 0; qq < N / 4; ++qq)
+        if (qq < nq) w[qq * fstride] = make_float2(acc[2 * qq], acc[2 * qq + 1]);
     }
   } else {
-    // ------------------------------------------------------------- promotion warps (9..16)
-    const int q = warp & 3;                        // TMEM lane quadrant this warp may access
-    const int h = (warp - 9) >> 2;                 // column half
-    const int row = 32 * q + lane;
-    const unsigned lane_base = (unsigned)(32 * q) << 16;
-    constexpr int kLd = (N / 2 < 16) ? N / 2 : 16;   // columns per TMEM load
-    float acc[N / 2];
+    const int l = m + 2 * (tc.j0 + row) + par;
+    if (l <= a.lcap) {
+      const float s = coef_factor(a, l, m);
+      const long long ld = a.ld_k;
+      float2* c = a.cout + (long long)kf0 * ld + (long long)m * (P.lmax + 1) + l;
 #pragma unroll
-    for (int i = 0; i < N / 2; ++i) acc[i] = 0.f;
-    bool ok = true;
-    for (int c = 0; c < nch; ++c) {
-      const unsigned gc = c0 + c;
-      const int bb = gc & 1;
-      if (ok) ok = mbar_wait(&rel[gc % S::kRel], (gc / S::kRel) & 1, abort_flag, a.err);
-      ok = __all_sync(0xffffffffu, ok);   // warp-uniform: the TMEM loads are warp-collective
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const unsigned dH = tmem + lane_base + bb * N + h * (N / 2);
-#pragma unroll
-      for (int i = 0; i < N / 2; i += kLd) {
-        float v[kLd];
-        tmem_ld<kLd>(dH + i, v);
-#pragma unroll
-        for (int u = 0; u < kLd; ++u) acc[i + u] += v[u];
-      }
-      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&acce[bb]);
-      if (!ok) break;
+      for (int qq = 0; qq < N / 4; ++qq)
+        if (qq < nq) c[qq * ld] = make_float2(acc[2 * qq] * s, acc[2 * qq + 1] * s);
     }
-    if (ok) {
-#pragma unroll
-      for (int qq = 0; qq < N / 4; ++qq) {
-        const int kf = kb + h * (N / 4) + qq;
-        if (kf >= a.nf) continue;
-        if (MODE == 0) {
-          const int pr = p0 + row;
-          if (pr < npair) a.Wout[(((size_t)kf * P.nm + im) * 2 + par) * npair + pr] = make_float2(acc[2 * qq], acc[2 * qq + 1]);
-        } else {
-          const int l = m + 2 * (j0 + row) + par;
-          if (l <= a.lcap) {
-            const float s = coef_factor(a, l, m);
-            a.cout[(long long)kf * a.ld_k + (long long)m * (P.lmax + 1) + l] = make_float2(acc[2 * qq] * s, acc[2 * qq + 1] * s);
-          }
-        }
-      }
-      if (MODE == 1 && j0 == 0) {
-        // The first tile of each order also clears that order's degrees l < m and
-        // lcap < l <= lmax; the two parity CTAs take half of the fields each.
-        const int pt = tid - 9 * 32;
-        const int nfl = min(N / 2, a.nf - kb), hf = (nfl + 1) / 2;
-        const int f0 = par ? hf : 0, f1 = par ? nfl : hf;
-        const int ntail = P.lmax - a.lcap, per = m + ntail;
-        for (int fi = f0; fi < f1; ++fi) {
-          float2* col = a.cout + (long long)(kb + fi) * a.ld_k + (long long)m * (P.lmax + 1);
-          for (int r = pt; r < per; r += 256) col[r < m ? r : a.lcap + 1 + (r - m)] = make_float2(0.f, 0.f);
-        }
-      }
+  }
+  if (MODE == 1 && tc.j0 == 0) {
+    // The first tile of each order also clears that order's degrees l < m and
+    // lcap < l <= lmax; the two parity tiles take half of the fields each.
+    const int pt = tid - 9 * 32;
+    const int nfl = min(N / 2, nf - kb), hf = (nfl + 1) / 2;
+    const int f0 = par ? hf : 0, f1 = par ? nfl : hf;
+    const int lcap = a.lcap, ntail = P.lmax - lcap, per = m + ntail;
+    const long long ld = a.ld_k;
+    float2* col0 = a.cout + (long long)m * (P.lmax + 1);
+    for (int fi = f0; fi < f1; ++fi) {
+      float2* col = col0 + (long long)(kb + fi) * ld;
+      for (int r = pt; r < per; r += 256) col[r < m ? r : lcap + 1 + (r - m)] = make_float2(0.f, 0.f);
     }
+  }
+  return true;
+}
+
+// Runs the tiles blockIdx.x, blockIdx.x + gridDim.x, ... of src (args(i), coord(i), n).
+template <int MODE, int N, class Src>
+__device__ __forceinline__ void gemm_tiles(const Src& src, unsigned char* sm, const Bars& B, unsigned tmem) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const bool loader = (warp == 17 && lane == 0), splitter = warp < 8, mma = (warp == 8 && lane == 0),
+             promo = (warp >= 9 && warp <= 16);
+  if (!(loader || splitter || mma || promo)) return;
+  unsigned ks0 = 0, c0 = 0;
+  for (int i = blockIdx.x; i < src.n; i += gridDim.x) {
+    const Args& a = src.args(i);
+    const TileCoord tc = src.coord(i);
+    const TileInfo T = tile_info<MODE>(a, tc);
+    bool ok;
+    if (loader)
+      ok = loader_tile<MODE, N>(a, tc, T, sm, B, c0);
+    else if (splitter)
+      ok = splitter_tile<MODE, N>(a, T, sm, B, tmem, ks0, c0);
+    else if (mma)
+      ok = mma_tile<MODE, N>(a, T, sm, B, tmem, ks0, c0);
+    else
+      ok = promo_tile<MODE, N>(a, tc, T, B, tmem, c0);
+    if (!ok) break;
+    if (promo) src.tile_done(i);
+    ks0 += T.nks;
+    c0 += T.nch;
   }
 }
 
@@ -587,65 +663,88 @@ __global__ void __launch_bounds__(256) mixed_pack_group_kernel(const Args* __res
   }
 }
 
-// One tile per CTA: blockIdx.x = 2 * tile + parity, blockIdx.y = order (synthesis),
-// blockIdx.z = block of N/2 fields.
+// Tiles of one transform, in order of decreasing work: synthesis tile i = ((im * nz + z)
+// * ntp + ptile) * 2 + par (lower orders have more degrees); analysis tile i = (list
+// index * nz + z) * 2 + par over the (im, j0) list. z = block of N/2 fields.
 template <int MODE, int N>
-__global__ void __launch_bounds__(kThreads, kCtasPerSm<N>) mixed_gemm_kernel(const __grid_constant__ Args a) {
+struct SingleSrc {
+  const Args& a;
+  int n, nz, ntp;
+  __device__ const Args& args(int) const { return a; }
+  __device__ void tile_done(int) const {}
+  __device__ TileCoord coord(int i) const {
+    TileCoord tc;
+    tc.par = i & 1;
+    int r = i >> 1;
+    if (MODE == 0) {
+      const int pt = r % ntp;
+      r /= ntp;
+      tc.kb = (r % nz) * (N / 2);
+      tc.im = r / nz;
+      tc.p0 = pt * kM;
+      tc.j0 = 0;
+    } else {
+      tc.kb = (r % nz) * (N / 2);
+      const int2 t = a.tiles[r / nz];
+      tc.im = t.x;
+      tc.j0 = t.y;
+      tc.p0 = 0;
+    }
+    return tc;
+  }
+};
+
+// ntiles: synthesis nmu * nz * ntp * 2, analysis ntiles_list * nz * 2.
+template <int MODE, int N>
+__global__ void __launch_bounds__(kThreads, kCtasPerSm<N>) mixed_gemm_kernel(const __grid_constant__ Args a, int ntiles,
+                                                                             int nz, int ntp) {
   extern __shared__ __align__(1024) unsigned char sm[];
   const Bars B = gemm_bars<N>(sm);
   const unsigned tmem = gemm_cta_setup<N>(B);
-  TileCoord tc;
-  tc.par = blockIdx.x & 1;
-  const int tile = blockIdx.x >> 1;
-  if (MODE == 0) {
-    tc.im = blockIdx.y;
-    tc.p0 = tile * kM;
-    tc.j0 = 0;
-  } else {
-    const int2 t = a.tiles[tile];
-    tc.im = t.x;
-    tc.j0 = t.y;
-    tc.p0 = 0;
-  }
-  tc.kb = blockIdx.z * (N / 2);
-  gemm_tile<MODE, N>(a, tc, sm, B, tmem, 0u, 0u);
+  const SingleSrc<MODE, N> src{a, ntiles, nz, ntp};
+  gemm_tiles<MODE, N>(src, sm, B, tmem);
   gemm_cta_teardown<N>(tmem);
 }
 
-// Persistent GEMM over the tiles of many independent transforms: CTA i runs items
-// i, i + gridDim.x, ... of a list sorted by decreasing cost; item = (transform,
-// im, p0 or j0, parity). Each transform's Args is staged in shared memory per item.
-// done[t] receives the %globaltimer value at which a tile of transform t finished
-// (the maximum over its tiles).
-template <int MODE, int N>
-__global__ void __launch_bounds__(kThreads, kCtasPerSm<N>) mixed_gemm_group_kernel(const Args* __restrict__ targs,
-                                                                        const int4* __restrict__ items, int nitems,
-                                                                        unsigned long long* __restrict__ done) {
-  extern __shared__ __align__(1024) unsigned char sm[];
-  __shared__ Args sa;
-  const Bars B = gemm_bars<N>(sm);
-  const unsigned tmem = gemm_cta_setup<N>(B);
-  unsigned ks0 = 0, c0 = 0;
-  for (int i = blockIdx.x; i < nitems; i += gridDim.x) {
+// Tiles of many independent transforms: item = (transform, im, p0 or j0, parity), list
+// sorted by decreasing cost. done[t] receives the %globaltimer value at which the last
+// tile of transform t was stored (the maximum over its tiles).
+template <int MODE>
+struct GroupSrc {
+  const Args* targs;
+  const int4* items;
+  int n;
+  unsigned long long* done;
+  __device__ const Args& args(int i) const { return targs[items[i].x]; }
+  __device__ TileCoord coord(int i) const {
     const int4 it = items[i];
-    if (threadIdx.x == 0) sa = targs[it.x];
-    __syncthreads();
-    if (*B.abort_flag) break;
     TileCoord tc;
     tc.im = it.y;
     tc.par = it.w;
     tc.kb = 0;
     tc.p0 = (MODE == 0) ? it.z : 0;
     tc.j0 = (MODE == 0) ? 0 : it.z;
-    gemm_tile<MODE, N>(sa, tc, sm, B, tmem, ks0, c0);
-    const int nks = tile_ksteps<MODE>(sa, tc);
-    ks0 += nks;
-    c0 += (nks + kChunk - 1) / kChunk;
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (done && threadIdx.x == 0) atomicMax(done + it.x, gtimer());
+    return tc;
   }
+  // called by each promotion warp after its stores of tile i
+  __device__ void tile_done(int i) const {
+    if (!done) return;
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) atomicMax(done + items[i].x, gtimer());
+  }
+};
+
+// Persistent GEMM over the tiles of many transforms.
+template <int MODE, int N>
+__global__ void __launch_bounds__(kThreads, kCtasPerSm<N>) mixed_gemm_group_kernel(const Args* __restrict__ targs,
+                                                                                   const int4* __restrict__ items,
+                                                                                   int nitems,
+                                                                                   unsigned long long* __restrict__ done) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  const Bars B = gemm_bars<N>(sm);
+  const unsigned tmem = gemm_cta_setup<N>(B);
+  const GroupSrc<MODE> src{targs, items, nitems, done};
+  gemm_tiles<MODE, N>(src, sm, B, tmem);
   gemm_cta_teardown<N>(tmem);
 }
 
@@ -755,24 +854,35 @@ static int ensure_table(const shtb_plan* cp, cudaStream_t st) {
   return SHTB_OK;
 }
 
+static int sm_count() {
+  int dev = 0, n = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  return n;
+}
+
+// ntiles tiles per block of N/2 fields; persistent CTAs, at most the resident number.
 template <int MODE, int N>
-static int launch_gemm(const shtb_plan* p, const Args& a, dim3 grid, cudaStream_t st) {
+static int launch_gemm(const shtb_plan* p, const Args& a, int ntiles, int nz, int ntp, cudaStream_t st) {
   auto kern = mixed_gemm_kernel<MODE, N>;
   const int smem = Smem<N>::kBytes;
   SHTB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "mixed smem attr");
+  const int total = ntiles * nz;
+  const int grid = std::max(1, std::min(total, sm_count() * kCtasPerSm<N>));
   prof_begin(st);
-  kern<<<grid, kThreads, smem, st>>>(a);
+  kern<<<grid, kThreads, smem, st>>>(a, total, nz, ntp);
   SHTB_LAUNCHED(MODE == 0 ? "tc gemm synthesis kernel" : "tc gemm analysis kernel");
   return SHTB_OK;
 }
 
+// ntiles: tiles per block of fields (synthesis: orders x pair tiles x 2, analysis:
+// degree tiles x 2); ntp: pair tiles per order (synthesis).
 template <int MODE>
-static int dispatch_gemm(const shtb_plan* p, const Args& a, int nf, dim3 grid_xy, cudaStream_t st) {
-  if (nf > 32) { dim3 g(grid_xy.x, grid_xy.y, (nf + 63) / 64); return launch_gemm<MODE, 128>(p, a, g, st); }
-  if (nf > 16) { dim3 g(grid_xy.x, grid_xy.y, 1); return launch_gemm<MODE, 64>(p, a, g, st); }
-  if (nf > 8) { dim3 g(grid_xy.x, grid_xy.y, 1); return launch_gemm<MODE, 32>(p, a, g, st); }
-  dim3 g(grid_xy.x, grid_xy.y, 1);
-  return launch_gemm<MODE, 16>(p, a, g, st);
+static int dispatch_gemm(const shtb_plan* p, const Args& a, int nf, int ntiles, int ntp, cudaStream_t st) {
+  if (nf > 32) return launch_gemm<MODE, 128>(p, a, ntiles, (nf + 63) / 64, ntp, st);
+  if (nf > 16) return launch_gemm<MODE, 64>(p, a, ntiles, 1, ntp, st);
+  if (nf > 8) return launch_gemm<MODE, 32>(p, a, ntiles, 1, ntp, st);
+  return launch_gemm<MODE, 16>(p, a, ntiles, 1, ntp, st);
 }
 
 // Clears whole order columns the analysis GEMM does not visit (m not a multiple of
@@ -813,8 +923,8 @@ int mixed_synthesis(const shtb_plan* p, const void* alm, void* f, int nf, int lt
   prof_begin(st);
   mixed_pack_kernel<<<dim3(mlim / p->mres + 1, nf), 256, 0, st>>>(a);
   SHTB_LAUNCHED("tc gemm B packing kernel");
-  dim3 g(2 * ((p->npair + kM - 1) / kM), mlim / p->mres + 1);
-  if ((rc = dispatch_gemm<0>(p, a, nf, g, st))) return rc;
+  const int ntp = (p->npair + kM - 1) / kM;
+  if ((rc = dispatch_gemm<0>(p, a, nf, 2 * ntp * (mlim / p->mres + 1), ntp, st))) return rc;
   return launch_fft_syn<float, float>(p, work, (float*)f, nullptr, 1, nf, mlim, p->phi_inv_scale / p->nlon, 0, 0, st);
 }
 
@@ -857,8 +967,7 @@ int mixed_analysis(const shtb_plan* p, const void* f, void* alm, int nf, int ltr
   a.lend = ltr;
   a.lcap = ltr;
   a.tiles = p->d_mx_tiles;
-  dim3 g(2 * (unsigned)tl.size(), 1);
-  if ((rc = dispatch_gemm<1>(p, a, nf, g, st))) return rc;
+  if ((rc = dispatch_gemm<1>(p, a, nf, 2 * (int)tl.size(), 0, st))) return rc;
   if (p->mres > 1 || mlim < p->mmax) {
     dim3 zg(p->mmax + 1, nf);
     prof_begin(st);
