@@ -148,12 +148,12 @@ __device__ __forceinline__ void mma_tf32_ts(unsigned tmem_d, unsigned tmem_a, un
 
 // Store this thread's 8 hi values at columns taddr.. and 8 lo values at taddr+8.. of
 // its TMEM lane, then wait for the stores.
+// Two 8-column TMEM stores (hi at taddr, lo at taddr + 8); the caller waits (tcgen05.wait::st).
 __device__ __forceinline__ void tmem_st8x2(unsigned taddr, const float4& h0, const float4& h1, const float4& l0,
                                            const float4& l1) {
   asm volatile(
       "tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%2, %3, %4, %5, %6, %7, %8, %9};\n\t"
-      "tcgen05.st.sync.aligned.32x32b.x8.b32 [%1], {%10, %11, %12, %13, %14, %15, %16, %17};\n\t"
-      "tcgen05.wait::st.sync.aligned;" ::"r"(taddr),
+      "tcgen05.st.sync.aligned.32x32b.x8.b32 [%1], {%10, %11, %12, %13, %14, %15, %16, %17};" ::"r"(taddr),
       "r"(taddr + 8), "r"(__float_as_uint(h0.x)), "r"(__float_as_uint(h0.y)), "r"(__float_as_uint(h0.z)),
       "r"(__float_as_uint(h0.w)), "r"(__float_as_uint(h1.x)), "r"(__float_as_uint(h1.y)), "r"(__float_as_uint(h1.z)),
       "r"(__float_as_uint(h1.w)), "r"(__float_as_uint(l0.x)), "r"(__float_as_uint(l0.y)), "r"(__float_as_uint(l0.z)),
@@ -247,13 +247,13 @@ struct Smem {
   static constexpr int kSt = (N == 128) ? 4 : (N == 64) ? 6 : (N == 32) ? 8 : 4;
   static constexpr int kFull = 16;   // per-chunk split barriers
   static constexpr int kStA = (N == 16) ? 8 : 16;   // two 16-column CTAs share an SM's TMEM
+  static constexpr int kSlotCh = kStA / kChunk;     // chunks whose split A tiles TMEM holds
   static constexpr int kRel = 16;   // chunk-release barriers (>= kSt and kStA, see the tile roles below)
   static constexpr int kBar = kSt * kStage;
-  // barriers: full[kFull], ldfull[kSt], rel[kRel], acce[2]; then the splitters' slot->chunk
-  // maps (256 x kStA ints), TMEM slot, abort flag
-  static constexpr int kBytes = kBar + (kFull + kSt + kRel + 2) * 8 + 256 * kStA * 4 + 16;
+  // barriers: full[kFull], ldfull[kSt], rel[kRel], acce[2]; then TMEM slot, abort flag
+  static constexpr int kBytes = kBar + (kFull + kSt + kRel + 2) * 8 + 16;
   // TMEM: chunk accumulators H0 [0, N) and H1 [N, 2N); A slot s: hi at 2N + 16 s, lo at
-  // 2N + 16 s + 8
+  // 2N + 16 s + 8; K-step s of chunk gc uses slot (gc % kSlotCh) kChunk + s
   static constexpr int kTmemA = 2 * N;
   static constexpr int kTmemNeed = 2 * N + 16 * kStA;
   static constexpr int kTmemCols = kTmemNeed <= 32 ? 32 : kTmemNeed <= 64 ? 64 : kTmemNeed <= 128 ? 128
@@ -276,7 +276,6 @@ struct TileCoord {
 // Shared-memory barriers of a GEMM CTA (initialised once per CTA).
 struct Bars {
   unsigned long long *full, *ldfull, *rel, *acce;
-  unsigned* slot_chunk;    // [256][kStA] the same for TMEM A slots (one row per splitter thread)
   unsigned* tmem_slot;
   volatile int* abort_flag;
 };
@@ -289,8 +288,7 @@ __device__ __forceinline__ Bars gemm_bars(unsigned char* sm) {
   B.ldfull = B.full + S::kFull;   // [kSt] bulk copies of the stage landed
   B.rel = B.ldfull + S::kSt;      // [kRel] MMAs of chunk q done (q % kRel)
   B.acce = B.rel + S::kRel;       // [2] TMEM chunk buffer b drained by the promotion warps
-  B.slot_chunk = reinterpret_cast<unsigned*>(B.acce + 2);
-  B.tmem_slot = B.slot_chunk + 256 * S::kStA;
+  B.tmem_slot = reinterpret_cast<unsigned*>(B.acce + 2);
   B.abort_flag = reinterpret_cast<volatile int*>(B.tmem_slot + 1);
   return B;
 }
@@ -308,8 +306,8 @@ template <int N>
 __device__ __forceinline__ unsigned gemm_cta_setup(const Bars& B) {
   const int tid = threadIdx.x, warp = tid >> 5;
   if (tid == 0) {
-    // one arrival per splitter warp and K-step of a full chunk (4 warps x kChunk)
-    for (int s = 0; s < Smem<N>::kFull; ++s) mbar_init(&B.full[s], 4 * kChunk);
+    // two arrivals per splitter warp and chunk (8 warps x 2 = 16)
+    for (int s = 0; s < Smem<N>::kFull; ++s) mbar_init(&B.full[s], 16);
     for (int s = 0; s < Smem<N>::kSt; ++s) mbar_init(&B.ldfull[s], 1);
     for (int s = 0; s < Smem<N>::kRel; ++s) mbar_init(&B.rel[s], 1);
     for (int b = 0; b < 2; ++b) mbar_init(&B.acce[b], 8);   // one arrival per promotion warp
@@ -341,9 +339,9 @@ __device__ __forceinline__ void gemm_cta_teardown(unsigned tmem) {
 //
 // A CTA runs a sequence of tiles (tile i = blockIdx.x, blockIdx.x + gridDim.x, ...), and
 // each role walks that sequence on its own: the loader and splitters run ahead into the
-// next tile while the promotion warps still drain and store the previous one. ks0 and
-// c0, counted identically by every role, number the K-steps and chunks of the tiles
-// before the current one and fix every stage index, TMEM slot and barrier phase.
+// next tile while the promotion warps still drain and store the previous one. c0,
+// counted identically by every role, numbers the chunks of the tiles before the current
+// one and fixes every stage index, TMEM slot and barrier phase.
 //
 // Synchronisation: chunk gc (kChunk K-steps, fewer at the end of a tile) occupies
 // shared-memory stage gc % kSt. The MMA issuer waits for all K-steps of a chunk to be
@@ -352,8 +350,7 @@ __device__ __forceinline__ void gemm_cta_teardown(unsigned tmem) {
 // rel[gc % kRel]. Each mbarrier wait costs a few hundred cycles even when the phase has
 // completed, so the MMA issuer waits on two barriers per chunk only.
 // That one barrier releases the chunk's stage (loader), its TMEM A slots (splitters)
-// and its accumulator (promotion warps); the splitters look up the chunk of a slot's
-// previous K-step in a small per-thread map. kRel >= kSt, kStA keeps a waiter from ever
+// and its accumulator (promotion warps). kRel >= kSt, kSlotCh keeps a waiter from ever
 // seeing a barrier two phases ahead.
 struct TileInfo {
   int m, nks, nch;
@@ -427,41 +424,44 @@ __device__ __forceinline__ bool loader_tile(const Args& a, const TileCoord& tc, 
 }
 
 // Splitter thread t of group sgp rounds row t of the A tile into TMEM lane t (its warp's
-// quadrant) for the K-steps g with g % 2 == sgp.
+// quadrant) for the K-steps s = sgp, sgp + 2 of each chunk. Every splitter warp arrives
+// on the chunk's barrier once with count 2 (its two K-step places), whatever the chunk's
+// length, after waiting for the chunk's stage: that bounds how far it runs ahead.
 template <int MODE, int N>
 __device__ __forceinline__ bool splitter_tile(const Args& a, const TileInfo& T, unsigned char* sm, const Bars& B,
-                                              unsigned tmem, unsigned ks0, unsigned c0) {
-  const unsigned astr = (unsigned)T.arows * kK * 4;   // A tile image bytes per K-step
+                                              unsigned tmem, unsigned c0) {
   using S = Smem<N>;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, t = tid & 127, sgp = warp >> 2;
-  const unsigned ta_lane = tmem + ((unsigned)(32 * (warp & 3)) << 16);
+  const unsigned ta_lane = tmem + ((unsigned)(32 * (warp & 3)) << 16) + S::kTmemA;
   const int o0 = tile_off(t, 0), o1 = tile_off(t, 1);
-  unsigned* my_slots = B.slot_chunk + (sgp * 128 + t) * S::kStA;
-  for (int ks = ((ks0 & 1) == (unsigned)sgp) ? 0 : 1; ks < T.nks; ks += 2) {
-    const unsigned g = ks0 + ks, gc = c0 + ks / kChunk;
-    const int ba = g % S::kStA;
+  const unsigned astr = (unsigned)T.arows * kK * 4;   // A tile image bytes per K-step
+  for (int c = 0; c < T.nch; ++c) {
+    const unsigned gc = c0 + c;
+    const int nk = min(kChunk, T.nks - c * kChunk);
     bool ok = mbar_wait(&B.ldfull[gc % S::kSt], (gc / S::kSt) & 1, B.abort_flag, a.err);
-    if (ok && g >= S::kStA) {
-      const unsigned q = my_slots[ba];
+    if (ok && sgp < nk && gc >= S::kSlotCh) {
+      const unsigned q = gc - S::kSlotCh;   // the chunk that last used these TMEM slots
       ok = mbar_wait(&B.rel[q % S::kRel], (q / S::kRel) & 1, B.abort_flag, a.err);
     }
     // the warp leaves together (the TMEM stores below are warp-collective)
     if (!__all_sync(0xffffffffu, ok)) return false;
-    my_slots[ba] = c0 + ks / kChunk;
-    // the MMAs that last read TMEM slot ba have completed
+    // the MMAs that last read these TMEM slots have completed
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const unsigned char* Ah = sm + (size_t)(gc % S::kSt) * S::kStage + (ks % kChunk) * astr;
-    const float4 x0 = *reinterpret_cast<const float4*>(Ah + o0);
-    const float4 x1 = *reinterpret_cast<const float4*>(Ah + o1);
-    float4 h, l, h1, l1;
-    split4(x0, h, l);
-    split4(x1, h1, l1);
-    tmem_st8x2(ta_lane + (unsigned)(S::kTmemA + 16 * ba), h, h1, l, l1);
+    const unsigned char* As = sm + (size_t)(gc % S::kSt) * S::kStage;
+    const unsigned slot0 = ta_lane + 16u * (gc % S::kSlotCh) * kChunk;
+    for (int s = sgp; s < nk; s += 2) {
+      const unsigned char* Ah = As + s * astr;
+      const float4 x0 = *reinterpret_cast<const float4*>(Ah + o0);
+      const float4 x1 = *reinterpret_cast<const float4*>(Ah + o1);
+      float4 h, l, h1, l1;
+      split4(x0, h, l);
+      split4(x1, h1, l1);
+      tmem_st8x2(slot0 + 16u * s, h, h1, l, l1);
+    }
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncwarp();   // one arrival per warp: 128 arrivals on one word serialize
-    // the last K-step of a short chunk also arrives for the missing ones
-    const int nk = min(kChunk, T.nks - (ks / kChunk) * kChunk);
-    if (lane == 0) mbar_arrive_cnt(&B.full[gc % S::kFull], (ks % kChunk == nk - 1) ? 1 + kChunk - nk : 1);
+    if (lane == 0) mbar_arrive_cnt(&B.full[gc % S::kFull], 2);
   }
   return true;
 }
@@ -469,7 +469,7 @@ __device__ __forceinline__ bool splitter_tile(const Args& a, const TileInfo& T, 
 // One thread issues the MMAs, a chunk at a time, and commits once per chunk.
 template <int MODE, int N>
 __device__ __forceinline__ bool mma_tile(const Args& a, const TileInfo& T, unsigned char* sm, const Bars& B,
-                                         unsigned tmem, unsigned ks0, unsigned c0) {
+                                         unsigned tmem, unsigned c0) {
   using S = Smem<N>;
   const unsigned idesc = idesc_tf32<N>();
   const unsigned long long bh0 = sdesc(sm + S::kStageA), bl0 = sdesc(sm + S::kStageA + kChunk * S::kTileB);
@@ -487,17 +487,16 @@ __device__ __forceinline__ bool mma_tile(const Args& a, const TileInfo& T, unsig
     // sum is still small, and the hi*hi products last.
     const unsigned dH = tmem + bb * N;
     const unsigned long long sc = (unsigned long long)(gc % S::kSt) * kStageDesc;
+    const unsigned slot0 = tmem + S::kTmemA + 16u * (gc % S::kSlotCh) * kChunk;
     for (int ks = k0; ks < k1; ++ks) {
-      const unsigned g = ks0 + ks;
       const unsigned long long so = sc + (ks - k0) * kstepDesc;
-      const unsigned ah = tmem + S::kTmemA + 16 * (g % S::kStA), al = ah + 8;
+      const unsigned ah = slot0 + 16u * (ks - k0), al = ah + 8;
       mma_tf32_ts(dH, ah, bl0 + so, idesc, ks == k0 ? 0u : 1u);
       mma_tf32_ts(dH, al, bh0 + so, idesc, 1u);
     }
     for (int ks = k0; ks < k1; ++ks) {
-      const unsigned g = ks0 + ks;
       const unsigned long long so = sc + (ks - k0) * kstepDesc;
-      mma_tf32_ts(dH, tmem + S::kTmemA + 16 * (g % S::kStA), bh0 + so, idesc, 1u);
+      mma_tf32_ts(dH, slot0 + 16u * (ks - k0), bh0 + so, idesc, 1u);
     }
     mma_commit(&B.rel[gc % S::kRel]);
   }
@@ -589,7 +588,7 @@ __device__ __forceinline__ void gemm_tiles(const Src& src, unsigned char* sm, co
   const bool loader = (warp == 17 && lane == 0), splitter = warp < 8, mma = (warp == 8 && lane == 0),
              promo = (warp >= 9 && warp <= 16);
   if (!(loader || splitter || mma || promo)) return;
-  unsigned ks0 = 0, c0 = 0;
+  unsigned c0 = 0;
   for (int i = blockIdx.x; i < src.n; i += gridDim.x) {
     const Args& a = src.args(i);
     const TileCoord tc = src.coord(i);
@@ -598,14 +597,13 @@ __device__ __forceinline__ void gemm_tiles(const Src& src, unsigned char* sm, co
     if (loader)
       ok = loader_tile<MODE, N>(a, tc, T, sm, B, c0);
     else if (splitter)
-      ok = splitter_tile<MODE, N>(a, T, sm, B, tmem, ks0, c0);
+      ok = splitter_tile<MODE, N>(a, T, sm, B, tmem, c0);
     else if (mma)
-      ok = mma_tile<MODE, N>(a, T, sm, B, tmem, ks0, c0);
+      ok = mma_tile<MODE, N>(a, T, sm, B, tmem, c0);
     else
       ok = promo_tile<MODE, N>(a, tc, T, B, tmem, c0);
     if (!ok) break;
     if (promo) src.tile_done(i);
-    ks0 += T.nks;
     c0 += T.nch;
   }
 }
