@@ -71,9 +71,8 @@ struct FFTJob {
   T* g0;                                  // grid (synthesis out / analysis in), component 0
   T* g1;                                  // component 1 when ncomp == 2
   int ncomp, mlim, use_w, spow;
-  int wtile;                              // analysis: 1 = write W as the GEMM's B tile images,
-  int nf;                                 //   TF32 hi at W and lo at W + wlo (floats), nf fields
-  size_t wlo;
+  int wtile;                              // analysis: 1 = write W as the GEMM's B tile images
+  int nf;                                 //   (FP32), nf fields
   double scale;                           // synthesis: grid factor; analysis: weight factor
   const typename V2<T>::type* tw;
   const typename V2<T>::type* twp;
@@ -294,11 +293,7 @@ __device__ __forceinline__ void fft_ana_body(const FFTJob<T>& J, int p0, int k, 
       const size_t o[4] = {b0 + btile_off(2 * fl, kk), b0 + btile_off(2 * fl + 1, kk), b1 + btile_off(2 * fl, kk),
                            b1 + btile_off(2 * fl + 1, kk)};
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const float hi = tf32_round(v[q]);
-        Wf[o[q]] = hi;
-        Wf[J.wlo + o[q]] = tf32_round(v[q] - hi);
-      }
+      for (int q = 0; q < 4; ++q) Wf[o[q]] = v[q];
     } else {
       const size_t base = ((size_t)k * P.nm + im) * 2 * npair + p0 + h;
       W[base] = E;
@@ -314,10 +309,7 @@ __device__ __forceinline__ void fft_ana_body(const FFTJob<T>& J, int p0, int k, 
       const int kk = p & 7, fl = k & 63;
       for (int par = 0; par < 2; ++par) {
         const size_t b = btile_base(im, par, p, k, npair, J.nf);
-        for (int c = 0; c < 2; ++c) {
-          Wf[b + btile_off(2 * fl + c, kk)] = 0.f;
-          Wf[J.wlo + b + btile_off(2 * fl + c, kk)] = 0.f;
-        }
+        for (int c = 0; c < 2; ++c) Wf[b + btile_off(2 * fl + c, kk)] = 0.f;
       }
     }
   }
@@ -355,7 +347,7 @@ __global__ void __launch_bounds__(512) fft_group_kernel(const FFTJob<T>* __restr
   }
 }
 
-// Floats of one analysis B tile image (the lo image follows the hi image).
+// Floats of the analysis B tile images.
 size_t fft_btile_floats(const shtb_plan* p, int nf) {
   return (size_t)p->nm * 2 * ((p->npair + 7) / 8) * btile_nfp(nf) * 16;
 }
@@ -379,7 +371,6 @@ static FFTJob<T> fft_job(const shtb_plan* p, const int* perm, const typename V2<
   J.spow = spow;
   J.wtile = wtile;
   J.nf = nf;
-  J.wlo = wtile ? fft_btile_floats(p, nf) : 0;
   J.scale = scale;
   J.tw = std::is_same<T, double>::value ? (const V*)p->d_tw64 : (const V*)p->d_tw32;
   J.twp = std::is_same<T, double>::value ? (const V*)p->d_twp64 : (const V*)p->d_twp32;

@@ -76,7 +76,7 @@ __device__ __forceinline__ float tf32_round(float x) {
   return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
 }
 
-// B operand tile images of the mixed-precision GEMMs: one region of nfp x 16 floats per
+// B operand tile images (FP32) of the mixed-precision GEMMs: one region of nfp x 16 floats per
 // K-step (nfp = fields rounded up to 4, so tiles have whole 8-row core-matrix groups);
 // fields in blocks of 64 (1024 floats), block rows 2f (real) and 2f+1 (imaginary) in the
 // K-major no-swizzle core-matrix order, 8 K values per row. btile_off gives the float

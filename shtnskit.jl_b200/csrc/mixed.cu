@@ -51,8 +51,8 @@ struct Args {
   const long long* seg;      // [2*nm+1] first table row of segment (im, parity); rows hold npp pairs
   int npp;
   const float2* cin;         // synthesis: coefficients (input of the B packing)
-  float* bhi;                // B tile images, TF32 hi and lo (synthesis: packed coefficients,
-  float* blo;                //   analysis: written by the FFT)
+  float* bimg;               // B tile images, FP32 (synthesis: packed coefficients, analysis:
+                             //   written by the FFT); split into TF32 hi/lo in shared memory
   float2* Wout;              // synthesis: Fourier buffer
   float2* cout;              // analysis: coefficients
   long long ld_k;            // coefficient field stride (complex elements)
@@ -357,6 +357,7 @@ struct TileInfo {
   long long sg, ln;   // table segment start and rows of (im, par)
   int arows;          // rows of the A tile image (128, fewer in the last analysis tile)
   unsigned bstr;      // bytes from one K-step's B tile to the next in a stage
+  unsigned bbytes;    // bytes of one K-step's B tile image (this CTA's fields)
 };
 
 template <int MODE>
@@ -371,12 +372,13 @@ __device__ __forceinline__ TileInfo tile_info(const Args& a, const TileCoord& tc
   // B images of consecutive K-steps are contiguous when all fields fit one 64-field block
   const int nfp = btile_nfp(a.nf);
   T.bstr = (nfp <= 64) ? (unsigned)nfp * 64 : (unsigned)(kM / 2) * 64;
+  T.bbytes = (unsigned)min(64, nfp - tc.kb) * 64;
   return T;
 }
 
 // One thread fills the shared-memory ring, kSt chunks ahead, with one bulk copy per
-// operand and chunk (the FP32 A tile images and the pre-split B tile images, hi and lo)
-// when the B images of the chunk are contiguous, one per K-step for B otherwise.
+// operand and chunk (the FP32 A and B tile images; B lands in the B_hi area and is split
+// in place) when the B images of the chunk are contiguous, one per K-step for B otherwise.
 template <int MODE, int N>
 __device__ __forceinline__ bool loader_tile(const Args& a, const TileCoord& tc, const TileInfo& T, unsigned char* sm,
                                             const Bars& B, unsigned c0) {
@@ -390,11 +392,9 @@ __device__ __forceinline__ bool loader_tile(const Args& a, const TileCoord& tc, 
   // B tile images: region rb + ks of nfp x 16 floats, this CTA's block of 64 fields
   const int nfp = btile_nfp(a.nf);
   const long long rb = (MODE == 0) ? T.sg / kK : (long long)(tc.im * 2 + tc.par) * ((npair + kK - 1) / kK);
-  const long long boff = rb * nfp * 16 + (long long)(tc.kb >> 6) * 1024;
-  const unsigned bbytes = (unsigned)min(64, nfp - tc.kb) * 64;
+  const float* bsrc = a.bimg + rb * nfp * 16 + (long long)(tc.kb >> 6) * 1024;
+  const unsigned bbytes = T.bbytes;
   const bool bcontig = nfp <= 64;
-  const float* bh = a.bhi + boff;
-  const float* bl = a.blo + boff;
   int* err = a.err;
   for (int c = 0; c < T.nch; ++c) {
     const unsigned gc = c0 + c;
@@ -405,26 +405,22 @@ __device__ __forceinline__ bool loader_tile(const Args& a, const TileCoord& tc, 
     }
     const int k0 = c * kChunk, nk = min(kChunk, T.nks - k0);
     unsigned char* sa = sm + (size_t)st * S::kStage;
-    unsigned char* sbh = sa + S::kStageA;
-    unsigned char* sbl = sbh + kChunk * S::kTileB;
+    unsigned char* sb = sa + S::kStageA;
     unsigned long long* bar = &B.ldfull[st];
-    mbar_expect_tx(bar, (unsigned)nk * (abytes + 2 * bbytes));
+    mbar_expect_tx(bar, (unsigned)nk * (abytes + bbytes));
     bulk_g2s(sa, a0 + (long long)k0 * T.arows * kK, nk * abytes, bar);
     if (bcontig) {
-      bulk_g2s(sbh, bh + (long long)k0 * nfp * 16, nk * bbytes, bar);
-      bulk_g2s(sbl, bl + (long long)k0 * nfp * 16, nk * bbytes, bar);
+      bulk_g2s(sb, bsrc + (long long)k0 * nfp * 16, nk * bbytes, bar);
     } else {
-      for (int s = 0; s < nk; ++s) {
-        bulk_g2s(sbh + s * S::kTileB, bh + (long long)(k0 + s) * nfp * 16, bbytes, bar);
-        bulk_g2s(sbl + s * S::kTileB, bl + (long long)(k0 + s) * nfp * 16, bbytes, bar);
-      }
+      for (int s = 0; s < nk; ++s) bulk_g2s(sb + s * S::kTileB, bsrc + (long long)(k0 + s) * nfp * 16, bbytes, bar);
     }
   }
   return true;
 }
 
 // Splitter thread t of group sgp rounds row t of the A tile into TMEM lane t (its warp's
-// quadrant) for the K-steps s = sgp, sgp + 2 of each chunk. Every splitter warp arrives
+// quadrant) for the K-steps s = sgp, sgp + 2 of each chunk, and splits those K-steps' B
+// tiles in shared memory (hi in place, lo into the B_lo area). Every splitter warp arrives
 // on the chunk's barrier once with count 2 (its two K-step places), whatever the chunk's
 // length, after waiting for the chunk's stage: that bounds how far it runs ahead.
 template <int MODE, int N>
@@ -447,7 +443,7 @@ __device__ __forceinline__ bool splitter_tile(const Args& a, const TileInfo& T, 
     if (!__all_sync(0xffffffffu, ok)) return false;
     // the MMAs that last read these TMEM slots have completed
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const unsigned char* As = sm + (size_t)(gc % S::kSt) * S::kStage;
+    unsigned char* As = sm + (size_t)(gc % S::kSt) * S::kStage;
     const unsigned slot0 = ta_lane + 16u * (gc % S::kSlotCh) * kChunk;
     for (int s = sgp; s < nk; s += 2) {
       const unsigned char* Ah = As + s * astr;
@@ -457,8 +453,18 @@ __device__ __forceinline__ bool splitter_tile(const Args& a, const TileInfo& T, 
       split4(x0, h, l);
       split4(x1, h1, l1);
       tmem_st8x2(slot0 + 16u * s, h, h1, l, l1);
+      float4* bh = reinterpret_cast<float4*>(As + S::kStageA + s * T.bstr);
+      float4* bl = reinterpret_cast<float4*>(As + S::kStageA + kChunk * S::kTileB + s * T.bstr);
+      for (int i = t; i < (int)(T.bbytes >> 4); i += 128) {
+        float4 bx = bh[i], hb, lb;
+        split4(bx, hb, lb);
+        bh[i] = hb;
+        bl[i] = lb;
+      }
     }
     asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+    // the B halves written here are read by the MMAs (async proxy)
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncwarp();   // one arrival per warp: 128 arrivals on one word serialize
     if (lane == 0) mbar_arrive_cnt(&B.full[gc % S::kFull], 2);
@@ -609,7 +615,7 @@ __device__ __forceinline__ void gemm_tiles(const Src& src, unsigned char* sm, co
 }
 
 // Synthesis B tile images: the coefficients of order im, field k, times the per-(l, m)
-// factors, split into TF32 hi/lo. Rows are the degrees l = m + par + 2j of one parity
+// factors, in FP32 (the GEMM splits them). Rows are the degrees l = m + par + 2j of one parity
 // (region seg(im, par)/8 + j/8 of the images); every row of the segment is written,
 // zero beyond lend, so the GEMM's last K-step of each segment reads zeros there.
 __device__ __forceinline__ void pack_order(const Args& a, int im, int k) {
@@ -634,11 +640,8 @@ __device__ __forceinline__ void pack_order(const Args& a, int im, int k) {
       const long long base = (sg / kK + j / kK) * nfp * 16 + (long long)(k >> 6) * 1024;
       const int kk = j & 7;
       const long long o0 = base + btile_off(2 * fl, kk), o1 = base + btile_off(2 * fl + 1, kk);
-      const float hx = tf32_round(v.x), hy = tf32_round(v.y);
-      a.bhi[o0] = hx;
-      a.bhi[o1] = hy;
-      a.blo[o0] = tf32_round(v.x - hx);
-      a.blo[o1] = tf32_round(v.y - hy);
+      a.bimg[o0] = v.x;
+      a.bimg[o1] = v.y;
     }
   }
 }
@@ -810,7 +813,7 @@ static long long table_segments(const shtb_plan* p, std::vector<long long>* seg)
 static size_t align256(size_t v) { return (v + 255) / 256 * 256; }
 
 // Synthesis workspace: Fourier buffer [f][nm][2][npair] (float2), then the B tile
-// images hi and lo (table rows x nfp x 2 floats each).
+// images (table rows x nfp x 2 floats).
 static size_t syn_w_bytes(const shtb_plan* p, int nf) { return align256((size_t)nf * p->nm * 2 * p->npair * 8); }
 static size_t syn_img_bytes(const shtb_plan* p, int nf) {
   return align256((size_t)table_segments(p, nullptr) * btile_nfp(nf) * 2 * 4);
@@ -912,8 +915,7 @@ int mixed_synthesis(const shtb_plan* p, const void* alm, void* f, int nf, int lt
   Args a = base_args(p);
   a.cin = (const float2*)alm;
   a.Wout = (float2*)work;
-  a.bhi = (float*)((char*)work + syn_w_bytes(p, nf));
-  a.blo = (float*)((char*)a.bhi + syn_img_bytes(p, nf));
+  a.bimg = (float*)((char*)work + syn_w_bytes(p, nf));
   a.sc_mode = p->d_scale ? 1 : 0;
   a.nf = nf;
   a.lend = ltr;
@@ -927,8 +929,8 @@ int mixed_synthesis(const shtb_plan* p, const void* alm, void* f, int nf, int lt
 }
 
 size_t mixed_workspace_bytes(const shtb_plan* p, int op, int nf) {
-  if (op == SHTB_OP_SYNTHESIS) return syn_w_bytes(p, nf) + 2 * syn_img_bytes(p, nf);
-  return align256(2 * fft_btile_floats(p, nf) * 4);
+  if (op == SHTB_OP_SYNTHESIS) return syn_w_bytes(p, nf) + syn_img_bytes(p, nf);
+  return align256(fft_btile_floats(p, nf) * 4);
 }
 
 int mixed_analysis(const shtb_plan* p, const void* f, void* alm, int nf, int ltr, void* work, cudaStream_t st) {
@@ -957,8 +959,7 @@ int mixed_analysis(const shtb_plan* p, const void* f, void* alm, int nf, int ltr
   }
   Args a = base_args(p);
   a.tab = p->d_tab_ana;
-  a.bhi = (float*)work;
-  a.blo = (float*)work + fft_btile_floats(p, nf);
+  a.bimg = (float*)work;
   a.cout = (float2*)alm;
   a.sc_mode = p->d_scale ? 2 : 0;
   a.nf = nf;
@@ -988,13 +989,11 @@ void mixed_fill_args(const shtb_plan* p, int mode, const void* in, void* out, in
   if (mode == 0) {
     a.cin = (const float2*)in;
     a.Wout = (float2*)out;
-    a.bhi = (float*)((char*)out + syn_w_bytes(p, nf));
-    a.blo = (float*)((char*)a.bhi + syn_img_bytes(p, nf));
+    a.bimg = (float*)((char*)out + syn_w_bytes(p, nf));
     a.sc_mode = p->d_scale ? 1 : 0;
   } else {
     a.tab = p->d_tab_ana;
-    a.bhi = (float*)const_cast<void*>(in);
-    a.blo = (float*)const_cast<void*>(in) + fft_btile_floats(p, nf);
+    a.bimg = (float*)const_cast<void*>(in);
     a.cout = (float2*)out;
     a.sc_mode = p->d_scale ? 2 : 0;
   }
