@@ -397,7 +397,7 @@ static bool fft_generic(const shtb_plan* p) {
   bool g = p->fft.direct;
   for (int i = 0; i < p->fft.nrad; ++i) {
     const int r = p->fft.rad[i];
-    g = g || !(r == 2 || r == 3 || r == 4 || r == 5 || r == 8);
+    g = g || !(r == 2 || r == 3 || r == 4 || r == 5 || r == 8 || r == 16);
   }
   return g;
 }

@@ -8,7 +8,7 @@
 // E/O and forms X_N = E + O, X_S = E - O.
 //
 // The transform is an in-place decimation-in-frequency mixed-radix FFT
-// (radices 8, 4, 2, 3, 5 and generic odd radices up to 13): every pass updates
+// (radices 16, 8, 4, 2, 3, 5 and generic odd radices up to 13): every pass updates
 // disjoint groups of r elements where they lie, so one shared buffer and one
 // barrier per pass suffice for any thread count. The result comes out in
 // mixed-radix digit-reversed order; callers read bin k at position rev[k]
@@ -106,6 +106,36 @@ __device__ __forceinline__ void dft_small(V* u, int dir, const V* __restrict__ t
     u[1] = cadd(e[1], o1);   u[5] = csub(e[1], o1);
     u[2] = cadd(e[2], o2);   u[6] = csub(e[2], o2);
     u[3] = cadd(e[3], o3);   u[7] = csub(e[3], o3);
+  } else if constexpr (RADIX == 16) {
+    // 16 = 4 x 4: DFT4 over n1 of x[4 n1 + n2], twiddle W16^(n2 k1), DFT4 over n2;
+    // X[k1 + 4 k2] lands in u[k1 + 4 k2]
+    V a[4][4];
+#pragma unroll
+    for (int n2 = 0; n2 < 4; ++n2) {
+      V t[4] = {u[n2], u[n2 + 4], u[n2 + 8], u[n2 + 12]};
+      dft_small<T, V, 4>(t, dir, tw, twstep, 4);
+#pragma unroll
+      for (int k1 = 0; k1 < 4; ++k1) a[n2][k1] = t[k1];
+    }
+    // W16^e = exp(dir 2 pi i e / 16) for e = n2 k1 in {1, 2, 3, 4, 6, 9}
+    const T c1 = (T)0.92387953251128675613, s1 = (T)0.38268343236508977173, r2 = (T)0.70710678118654752440;
+    const T sd = dir > 0 ? (T)1 : (T)-1;
+    V w1, w2, w3, w6, w9;
+    w1.x = c1;  w1.y = sd * s1;
+    w2.x = r2;  w2.y = sd * r2;
+    w3.x = s1;  w3.y = sd * c1;
+    w6.x = -r2; w6.y = sd * r2;
+    w9.x = -c1; w9.y = -sd * s1;
+    a[1][1] = cmul(a[1][1], w1); a[1][2] = cmul(a[1][2], w2); a[1][3] = cmul(a[1][3], w3);
+    a[2][1] = cmul(a[2][1], w2); a[2][2] = crot(a[2][2], dir); a[2][3] = cmul(a[2][3], w6);
+    a[3][1] = cmul(a[3][1], w3); a[3][2] = cmul(a[3][2], w6); a[3][3] = cmul(a[3][3], w9);
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+      V t[4] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1]};
+      dft_small<T, V, 4>(t, dir, tw, twstep, 4);
+#pragma unroll
+      for (int k2 = 0; k2 < 4; ++k2) u[k1 + 4 * k2] = t[k2];
+    }
   } else {
     V out[RADIX];
 #pragma unroll
@@ -237,6 +267,7 @@ __device__ void fft_rows(V* X, V* scratch, int F, int S, const FFTDesc& fd, cons
       case 4: dif_pass<T, V, 4>(X, F, N, S, Ns, 4, tw, tp, mr, ms, dir, sh); break;
       case 5: dif_pass<T, V, 5>(X, F, N, S, Ns, 5, tw, tp, mr, ms, dir, sh); break;
       case 8: dif_pass<T, V, 8>(X, F, N, S, Ns, 8, tw, tp, mr, ms, dir, sh); break;
+      case 16: dif_pass<T, V, 16>(X, F, N, S, Ns, 16, tw, tp, mr, ms, dir, sh); break;
       default:
         if constexpr (GENERIC) dif_pass<T, V, 13>(X, F, N, S, Ns, r, tw, tp, mr, ms, dir, sh);
         break;

@@ -130,7 +130,9 @@ static bool factor_fft(int n, FFTDesc& d) {
   d.nrad = 0;
   d.direct = false;
   int k = n;
-  // prefer radix 8 and 4, then 2, 3, 5, 7 and small odd primes up to 16
+  // prefer radix 16, 8 and 4, then 2, 3, 5, 7 and small odd primes up to 16: fewer
+  // passes over shared memory
+  while (k % 16 == 0 && d.nrad < 24) { d.rad[d.nrad++] = 16; k /= 16; }
   while (k % 8 == 0 && d.nrad < 24) { d.rad[d.nrad++] = 8; k /= 8; }
   while (k % 4 == 0 && d.nrad < 24) { d.rad[d.nrad++] = 4; k /= 4; }
   while (k % 2 == 0 && d.nrad < 24) { d.rad[d.nrad++] = 2; k /= 2; }
