@@ -85,6 +85,61 @@ __device__ __forceinline__ size_t btile_base(int im, int par, int p, int k, int 
   return (((size_t)im * 2 + par) * nks8 + (p >> 3)) * (size_t)btile_nfp(nf) * 16 + (size_t)(k >> 6) * 1024;
 }
 
+// First DIF pass (radix R, span N/R) read straight from the grid: group (row h, j)
+// takes longitudes j + q span of latitude pair p0 + h as z = f_north + i f_south.
+// Consecutive threads take consecutive rows, so a warp's loads for one q cover whole
+// 32-byte runs of latitudes.
+template <typename T, typename V, int R, int H>
+__device__ __forceinline__ void dif_first_from_grid(V* X, int S, int N, const T* __restrict__ in, int nlat, int p0,
+                                                    int hv, const V* __restrict__ twp, int sh) {
+  const int span = N / R;
+  for (int b = threadIdx.x; b < H * span; b += blockDim.x) {
+    const int h = b % H, j = b / H;
+    const int pair = p0 + h, south = nlat - 1 - pair;
+    const bool vn = h < hv, vs = vn && south != pair;
+    V u[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const size_t off = (size_t)(j + q * span) * nlat;
+      u[q].x = vn ? in[off + pair] : (T)0;
+      u[q].y = vs ? in[off + south] : (T)0;
+    }
+    dft_small<T, V, R>(u, -1, nullptr, 0, R);
+    if (j != 0) {
+#pragma unroll
+      for (int q = 1; q < R; ++q) u[q] = cmul(u[q], twp[(q - 1) * span + j]);
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q) X[h * S + fft_pad(j + q * span, sh)] = u[q];
+  }
+}
+
+// Last DIF pass (radix R, span 1) written straight to the grid: group (row h, block)
+// holds the storage positions block R + q, i.e. longitudes rinv[block R + q]; the
+// per-pair factor g[h] is applied on the way out.
+template <typename T, typename V, int R, int H>
+__device__ __forceinline__ void dif_last_to_grid(const V* X, int S, int N, T* __restrict__ out, int nlat, int p0,
+                                                 int hv, const int* __restrict__ rinv, const T* g, int sh) {
+  const int ngrp = N / R;
+  for (int b = threadIdx.x; b < H * ngrp; b += blockDim.x) {
+    const int h = b % H, blk = b / H;
+    V u[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) u[q] = X[h * S + fft_pad(blk * R + q, sh)];
+    dft_small<T, V, R>(u, +1, nullptr, 0, R);
+    if (h < hv) {
+      const int pair = p0 + h, south = nlat - 1 - pair;
+      const T gh = g[h];
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        T* row = out + (size_t)rinv[blk * R + q] * nlat;
+        row[pair] = u[q].x * gh;
+        if (south != pair) row[south] = u[q].y * gh;
+      }
+    }
+  }
+}
+
 // Latitude pairs p0 .. p0+H-1 of field k.
 template <typename T, int H, bool GENERIC>
 __device__ __forceinline__ void fft_syn_body(const FFTJob<T>& J, int p0, int k, unsigned char* smem_raw) {
@@ -160,10 +215,22 @@ __device__ __forceinline__ void fft_syn_body(const FFTJob<T>& J, int p0, int k, 
     }
   }
   __syncthreads();
-  fft_rows<T, V, GENERIC>(Z, scratch, H, S, fd, tw, twp, +1);
   T* out = (ncomp == 2 && (k & 1)) ? out1 : out0;
   const size_t kk = (ncomp == 2) ? (size_t)(k >> 1) : (size_t)k;
   const size_t fbase = kk * (size_t)nlat * N;
+  if (const int rl = fft_fusable_radix(fd, fd.nrad - 1)) {
+    // all passes but the last in shared memory; the last one writes the grid
+    fft_rows<T, V, GENERIC>(Z, scratch, H, S, fd, tw, twp, +1, 0, fd.nrad - 1);
+    T* o = out + fbase;
+    switch (rl) {
+      case 16: dif_last_to_grid<T, V, 16, H>(Z, S, N, o, nlat, p0, hv, rinv, gfac, sh); break;
+      case 8: dif_last_to_grid<T, V, 8, H>(Z, S, N, o, nlat, p0, hv, rinv, gfac, sh); break;
+      case 4: dif_last_to_grid<T, V, 4, H>(Z, S, N, o, nlat, p0, hv, rinv, gfac, sh); break;
+      default: dif_last_to_grid<T, V, 2, H>(Z, S, N, o, nlat, p0, hv, rinv, gfac, sh); break;
+    }
+    return;
+  }
+  fft_rows<T, V, GENERIC>(Z, scratch, H, S, fd, tw, twp, +1);
   constexpr int L = Vec16<T>::n;
   const bool vec = (H % L == 0) && (hv == H) && (nlat % L == 0);
   constexpr int QU = 4;   // longitudes per thread per round; their rinv entries load together
@@ -232,6 +299,19 @@ __device__ __forceinline__ void fft_ana_body(const FFTJob<T>& J, int p0, int k, 
   const size_t kk = (ncomp == 2) ? (size_t)(k >> 1) : (size_t)k;
   const size_t fbase = kk * (size_t)nlat * N;
   for (int h = threadIdx.x; h < H; h += blockDim.x) wfac[h] = (h < hv) ? pair_factor<T>(P, p0 + h, wscale, use_w, spow) : (T)0;
+  if (const int r0 = fft_fusable_radix(fd, 0)) {
+    // the first pass reads the grid; the remaining passes run in shared memory
+    __syncthreads();   // wfac
+    const T* src = in + fbase;
+    switch (r0) {
+      case 16: dif_first_from_grid<T, V, 16, H>(Z, S, N, src, nlat, p0, hv, twp + fd.twoff[0], sh); break;
+      case 8: dif_first_from_grid<T, V, 8, H>(Z, S, N, src, nlat, p0, hv, twp + fd.twoff[0], sh); break;
+      case 4: dif_first_from_grid<T, V, 4, H>(Z, S, N, src, nlat, p0, hv, twp + fd.twoff[0], sh); break;
+      default: dif_first_from_grid<T, V, 2, H>(Z, S, N, src, nlat, p0, hv, twp + fd.twoff[0], sh); break;
+    }
+    __syncthreads();
+    fft_rows<T, V, GENERIC>(Z, scratch, H, S, fd, tw, twp, -1, 1);
+  } else {
   constexpr int L = Vec16<T>::n;
   const bool vec = (H % L == 0) && (hv == H) && (nlat % L == 0);
   for (int j = threadIdx.x; j < N; j += blockDim.x) {
@@ -270,6 +350,7 @@ __device__ __forceinline__ void fft_ana_body(const FFTJob<T>& J, int p0, int k, 
   }
   __syncthreads();
   fft_rows<T, V, GENERIC>(Z, scratch, H, S, fd, tw, twp, -1);
+  }
   const int nmu = mlim / P.mres + 1;
   for (int idx = threadIdx.x; idx < nmu * H; idx += blockDim.x) {
     const int im = idx / H, h = idx - im * H;

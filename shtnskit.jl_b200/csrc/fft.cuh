@@ -51,6 +51,12 @@ __host__ __device__ inline int fft_row_stride(int n, int sh) { return n + (n >> 
 // Skew of a row of complex elements of celem bytes: the plan's choice for FP32 (8-byte
 // elements); FP64 rows (16-byte elements) measured fastest with i + i/8 at every length.
 __host__ __device__ inline int fft_padsh(const FFTDesc& fd, size_t celem) { return celem == 8 ? fd.padsh : 3; }
+// Radix of pass s when the grid I/O can take it over (power-of-two radices), else 0.
+__host__ __device__ inline int fft_fusable_radix(const FFTDesc& fd, int s) {
+  if (fd.direct || fd.nrad < 2) return 0;
+  const int r = fd.rad[s];
+  return (r == 2 || r == 4 || r == 8 || r == 16) ? r : 0;
+}
 
 // In-register DFT of RADIX points in direction dir. Generic odd radices use the
 // twiddle table tw[t] = exp(-2 pi i t / N) with step twstep = N / radix.
@@ -226,11 +232,13 @@ __device__ __forceinline__ void dif_pass(V* X, int F, int N, int S, int Ns, int 
   __syncthreads();
 }
 
-// Full in-place FFT of F rows (natural-order input; output bin k at rev[k]).
-// `scratch` (same size as X) is used only in direct mode (a prime factor above 13).
+// Full in-place FFT of F rows (natural-order input; output bin k at rev[k]), or its
+// passes s0 .. s1-1 only (s1 < 0: to the end) when the caller fuses the first or the
+// last pass with its global loads or stores. `scratch` (same size as X) is used only in
+// direct mode (a prime factor above 13).
 template <typename T, typename V, bool GENERIC>
 __device__ void fft_rows(V* X, V* scratch, int F, int S, const FFTDesc& fd, const V* __restrict__ tw,
-                         const V* __restrict__ twp, int dir) {
+                         const V* __restrict__ twp, int dir, int s0 = 0, int s1 = -1) {
   const int N = fd.n, sh = fft_padsh(fd, sizeof(V));
   if (GENERIC && fd.direct) {
     // O(N^2) DFT into scratch, written at natural positions (rev = identity in direct mode)
@@ -257,7 +265,9 @@ __device__ void fft_rows(V* X, V* scratch, int F, int S, const FFTDesc& fd, cons
     return;
   }
   int Ns = N;
-  for (int s = 0; s < fd.nrad; ++s) {
+  for (int s = 0; s < s0; ++s) Ns /= fd.rad[s];
+  const int send = s1 < 0 ? fd.nrad : s1;
+  for (int s = s0; s < send; ++s) {
     const int r = fd.rad[s];
     const V* tp = twp + fd.twoff[s];
     const unsigned mr = fd.mrow[s], ms = fd.mspan[s];
