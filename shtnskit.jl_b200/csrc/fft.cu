@@ -352,7 +352,47 @@ __device__ __forceinline__ void fft_ana_body(const FFTJob<T>& J, int p0, int k, 
   fft_rows<T, V, GENERIC>(Z, scratch, H, S, fd, tw, twp, -1);
   }
   const int nmu = mlim / P.mres + 1;
+  if constexpr (H % 4 == 0) {
+    if (J.wtile && hv == H) {
+      // B tile images, four pairs per thread: a K-slot quad of rows 2f and 2f+1 is one
+      // 32-byte run, written as two 16-byte stores per parity
+      float* Wf = reinterpret_cast<float*>(W);
+      const int fl = k & 63;
+      constexpr int NQ = H / 4;
+      for (int idx = threadIdx.x; idx < nmu * NQ; idx += blockDim.x) {
+        const int im = idx / NQ, qd = idx - im * NQ;
+        const int m = im * P.mres;
+        const int pm = fft_pad(rev[m], sh), pc = fft_pad(rev[m == 0 ? 0 : N - m], sh);
+        float4 ex, ey, ox, oy;
+        float* e0 = &ex.x; float* e1 = &ey.x; float* q0 = &ox.x; float* q1 = &oy.x;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int h = 4 * qd + u;
+          const V Zm = Z[h * S + pm];
+          V Zc = Z[h * S + pc];
+          Zc.y = -Zc.y;
+          const V sum = cadd(Zm, Zc), d = csub(Zm, Zc);
+          V XN, XS;
+          XN.x = sum.x * (T)0.5; XN.y = sum.y * (T)0.5;
+          XS.x = d.y * (T)0.5;   XS.y = -d.x * (T)0.5;
+          const T wt = wfac[h];
+          const V E = cscale(cadd(XN, XS), wt), O = cscale(csub(XN, XS), wt);
+          e0[u] = (float)E.x; e1[u] = (float)E.y; q0[u] = (float)O.x; q1[u] = (float)O.y;
+        }
+        const int p = p0 + 4 * qd, kk = p & 7;
+        float* d0 = Wf + btile_base(im, 0, p, k, npair, J.nf) + btile_off(2 * fl, kk);
+        float* d1 = Wf + btile_base(im, 1, p, k, npair, J.nf) + btile_off(2 * fl, kk);
+        reinterpret_cast<float4*>(d0)[0] = ex;   // row 2f
+        reinterpret_cast<float4*>(d0)[1] = ey;   // row 2f+1 (next 16 bytes)
+        reinterpret_cast<float4*>(d1)[0] = ox;
+        reinterpret_cast<float4*>(d1)[1] = oy;
+      }
+    }
+  }
   for (int idx = threadIdx.x; idx < nmu * H; idx += blockDim.x) {
+    if constexpr (H % 4 == 0) {
+      if (J.wtile && hv == H) break;
+    }
     const int im = idx / H, h = idx - im * H;
     if (h >= hv) continue;
     const int m = im * P.mres;
@@ -405,7 +445,13 @@ __global__ void __launch_bounds__(512) fft_syn_kernel(const __grid_constant__ FF
 template <typename T, int H, bool GENERIC>
 __global__ void __launch_bounds__(512) fft_ana_kernel(const __grid_constant__ FFTJob<T> J) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  fft_ana_body<T, H, GENERIC>(J, blockIdx.x * H, blockIdx.y, smem_raw);
+  // B tile image output: blockIdx.x = field, blockIdx.y = pair block, so the fields' CTAs
+  // that fill one B tile region (all fields of 8 pairs) run together and its lines
+  // complete in L2; Fourier-buffer output: blockIdx.x = pair block, blockIdx.y = field.
+  if (J.wtile)
+    fft_ana_body<T, H, GENERIC>(J, blockIdx.y * H, blockIdx.x, smem_raw);
+  else
+    fft_ana_body<T, H, GENERIC>(J, blockIdx.x * H, blockIdx.y, smem_raw);
 }
 
 // Persistent FFTs over many independent transforms: CTA i runs items i, i + gridDim.x,
@@ -508,6 +554,7 @@ static int launch_ana_h(const shtb_plan* p, const T* in0, const T* in1, int ncom
   auto kern = fft_generic(p) ? fft_ana_kernel<T, H, true> : fft_ana_kernel<T, H, false>;
   SHTB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "fft smem attr");
   dim3 grid((p->npair + H - 1) / H, nfw);
+  if (wtile) grid = dim3(nfw, (p->npair + H - 1) / H);
   const FFTJob<T> J = fft_job<T>(p, p->d_rev, nullptr, (V*)W, const_cast<T*>(in0), const_cast<T*>(in1), ncomp, mlim,
                                  wscale, use_w, spow, wtile, nfw);
   prof_begin(st);
