@@ -130,6 +130,42 @@ int shtb_analysis_sphtor(const shtb_plan* plan, const void* Vt, const void* Vp, 
                          void* work, size_t work_bytes, void* stream);
 
 /*
+ * Vector transforms with divergence/vorticity spectra on the spectral side, the diagonal
+ * factor applied where the coefficients enter (synthesis) or leave (analysis) the Legendre
+ * stage instead of in a separate pass:
+ *   shtb_synthesis_divvort(div, vort) = synthesis_sphtor(spheroidal_from_divergence(div),
+ *                                                        toroidal_from_vorticity(vort))
+ *   shtb_analysis_divvort(Vt, Vp)     = (divergence_from_spheroidal(S), vorticity_from_toroidal(T))
+ *                                       with (S, T) = analysis_sphtor(Vt, Vp)
+ * (src/sphtor_transforms.jl:771-783, :817-831, :865-877, :911-925 composed with
+ * :162-241 / :252-289). No single reference entry point; arguments, workspace
+ * (SHTB_OP_SYNTHESIS_SPHTOR / SHTB_OP_ANALYSIS_SPHTOR) and errors as the sphtor calls. FP64.
+ */
+int shtb_synthesis_divvort(const shtb_plan* plan, const void* div, const void* vort, void* Vt, void* Vp,
+                           int nfields, int ltr, int dtype, int precision,
+                           void* work, size_t work_bytes, void* stream);
+int shtb_analysis_divvort(const shtb_plan* plan, const void* Vt, const void* Vp, void* div, void* vort,
+                          int nfields, int ltr, int dtype, int precision,
+                          void* work, size_t work_bytes, void* stream);
+
+/*
+ * Diagonal spectral operators on dense (lmax+1, mmax+1) coefficients of nfields fields
+ * (dtype SHTB_F64: complex double, SHTB_F32: complex float), no workspace:
+ *   SHTB_SPEC_NEG_LL      out = -l(l+1) in: divergence_from_spheroidal!,
+ *                         vorticity_from_toroidal! (src/sphtor_transforms.jl:771-783, :865-877),
+ *                         laplacian_kernel! / gpu_apply_laplacian! (ext/GPUCommon.jl:1501-1512,
+ *                         ext/SHTnsKitGPUExt.jl:2382-2389)
+ *   SHTB_SPEC_INV_NEG_LL  out = -(in / (l(l+1))): spheroidal_from_divergence!,
+ *                         toroidal_from_vorticity! (src/sphtor_transforms.jl:817-831, :911-925)
+ * Entries with m % mres != 0 or l < max(1, m) are written as zero. out may be in itself;
+ * otherwise the two must not overlap.
+ */
+#define SHTB_SPEC_NEG_LL     0
+#define SHTB_SPEC_INV_NEG_LL 1
+int shtb_spectral_op(const shtb_plan* plan, int op, const void* in, void* out, int nfields, int dtype,
+                     void* stream);
+
+/*
  * Adjoints (Zygote convention g = 2 dL/d(conj a)), FP64 only, real spatial cotangents.
  *   shtb_synthesis_adjoint:        ybar (grid)  -> abar (coefficients)
  *   shtb_analysis_adjoint:         abar         -> fbar (grid, real projection)

@@ -424,6 +424,42 @@ def analysis_sphtor(cfg: Config, Vt: np.ndarray, Vp: np.ndarray, ltr: int | None
 
 
 # ---------------------------------------------------------------------------
+# Dense diagonal spectral operators, src/sphtor_transforms.jl:771-783 (δ = −l(l+1) S),
+# :817-831 (S = −δ/(l(l+1))), :865-877 / :911-925 (vorticity/toroidal, same maps);
+# ext/GPUCommon.jl:1501-1512 (laplacian_kernel!, the same map as the divergence).
+# Entries with m % mres != 0 or l < max(1, m) become zero.
+# ---------------------------------------------------------------------------
+
+def _spectral_mask(cfg: Config, shape):
+    l = np.arange(cfg.lmax + 1).reshape(-1, 1)
+    m = np.arange(cfg.mmax + 1).reshape(1, -1)
+    valid = (m % cfg.mres == 0) & (l >= np.maximum(1, m))
+    return valid.reshape(valid.shape + (1,) * (len(shape) - 2)), l.reshape(l.shape + (1,) * (len(shape) - 2))
+
+
+def neg_ll(cfg: Config, a: np.ndarray) -> np.ndarray:
+    """divergence_from_spheroidal / vorticity_from_toroidal / laplacian: −l(l+1)·a."""
+    a = np.asarray(a)
+    valid, l = _spectral_mask(cfg, a.shape)
+    ll = (l * (l + 1)).astype(a.real.dtype)
+    out = np.empty_like(a)
+    out.real = np.where(valid, -ll * a.real, 0)
+    out.imag = np.where(valid, -ll * a.imag, 0)
+    return out
+
+
+def inv_neg_ll(cfg: Config, a: np.ndarray) -> np.ndarray:
+    """spheroidal_from_divergence / toroidal_from_vorticity: −(a / (l(l+1))), componentwise."""
+    a = np.asarray(a)
+    valid, l = _spectral_mask(cfg, a.shape)
+    ll = np.maximum(l * (l + 1), 1).astype(a.real.dtype)
+    out = np.empty_like(a)
+    out.real = np.where(valid, -(a.real / ll), 0)
+    out.imag = np.where(valid, -(a.imag / ll), 0)
+    return out
+
+
+# ---------------------------------------------------------------------------
 # Adjoints (Zygote convention g = 2 ∂L/∂ā), src/core_transforms.jl:477-652,
 # src/sphtor_transforms.jl:385-452
 # ---------------------------------------------------------------------------

@@ -297,6 +297,31 @@ extern "C" int shtb_analysis_sphtor(const shtb_plan* p, const void* Vt, const vo
                       (cudaStream_t)stream);
 }
 
+// Divergence/vorticity spectra: S = -div / (l(l+1)) enters the sphtor synthesis as the
+// factor -1 / (l(l+1)) of the pre-combine kernel; div = -l(l+1) S leaves the analysis as
+// the factor -1 in place of its 1 / (l(l+1)).
+extern "C" int shtb_synthesis_divvort(const shtb_plan* p, const void* D, const void* Z, void* Vt, void* Vp, int nf,
+                                      int ltr, int dtype, int precision, void* work, size_t wb, void* stream) {
+  int rc = check_common(p, nf, &ltr, dtype, precision, work, wb, SHTB_OP_SYNTHESIS_SPHTOR);
+  if (rc) return rc;
+  if ((rc = check_ptrs({D, Z, Vt, Vp}))) return rc;
+  if (precision != SHTB_PREC_FP64) return set_error(SHTB_ERR_UNSUPPORTED, "vector transforms run on the FP64 path");
+  Factors F{nullptr, p->d_scale, p->d_scale ? 1 : 0, -1.0, -1.0};
+  return vec_synthesis(p, D, Z, Vt, Vp, nf, ltr, F, 1, p->phi_inv_scale / p->nlon, 0, p->robert ? 0 : 1, work,
+                       (cudaStream_t)stream);
+}
+
+extern "C" int shtb_analysis_divvort(const shtb_plan* p, const void* Vt, const void* Vp, void* D, void* Z, int nf,
+                                     int ltr, int dtype, int precision, void* work, size_t wb, void* stream) {
+  int rc = check_common(p, nf, &ltr, dtype, precision, work, wb, SHTB_OP_ANALYSIS_SPHTOR);
+  if (rc) return rc;
+  if ((rc = check_ptrs({D, Z, Vt, Vp}))) return rc;
+  if (precision != SHTB_PREC_FP64) return set_error(SHTB_ERR_UNSUPPORTED, "vector transforms run on the FP64 path");
+  Factors F{nullptr, p->d_scale, p->d_scale ? 2 : 0, -1.0, -1.0};
+  return vec_analysis(p, Vt, Vp, D, Z, nf, ltr, F, 0, p->ana_scale, 1, p->robert ? 2 : 1, work,
+                      (cudaStream_t)stream);
+}
+
 // ---------------------------------------------------------------------------
 // adjoints (src/core_transforms.jl:477-652, src/sphtor_transforms.jl:385-452)
 // ---------------------------------------------------------------------------

@@ -34,6 +34,9 @@ SHTB_OP_ANALYSIS = 1
 SHTB_OP_SYNTHESIS_SPHTOR = 2
 SHTB_OP_ANALYSIS_SPHTOR = 3
 
+SHTB_SPEC_NEG_LL = 0
+SHTB_SPEC_INV_NEG_LL = 1
+
 
 class BackendUnavailableError(RuntimeError):
     """Mirror of SHTnsKit's ``BackendUnavailableError(operation, detail)`` (src/devices.jl:20-26)."""
@@ -70,6 +73,9 @@ SIGNATURES = {
     "shtb_analysis": (_I, [_P, _P, _P, _I, _I, _I, _I, _P, _SZ, _P]),
     "shtb_synthesis_sphtor": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _P, _SZ, _P]),
     "shtb_analysis_sphtor": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _P, _SZ, _P]),
+    "shtb_synthesis_divvort": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _P, _SZ, _P]),
+    "shtb_analysis_divvort": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _P, _SZ, _P]),
+    "shtb_spectral_op": (_I, [_P, _I, _P, _P, _I, _I, _P]),
     "shtb_synthesis_adjoint": (_I, [_P, _P, _P, _I, _P, _SZ, _P]),
     "shtb_analysis_adjoint": (_I, [_P, _P, _P, _I, _P, _SZ, _P]),
     "shtb_synthesis_sphtor_adjoint": (_I, [_P, _P, _P, _P, _P, _I, _P, _SZ, _P]),

@@ -514,6 +514,153 @@ def analysis_sphtor_batch(cfg: SHTConfig, Vt, Vp, *, use_rfft: bool = False, lca
     return _sphtor_anal(cfg, Vt, Vp, True, use_rfft, lcap)
 
 
+# ---------------------------------------------------------------------------
+# diagonal spectral operators and divergence/vorticity spectra
+# ---------------------------------------------------------------------------
+
+def _spectral_op(name, op, cfg, src, out):
+    a = _as_tensor(src)
+    if not a.is_complex():
+        a = a.to(torch.complex128)
+    if a.dim() not in (2, 3) or a.shape[0] != cfg.lmax + 1 or a.shape[1] != cfg.mmax + 1:
+        raise DimensionMismatch("spectral input dims")
+    if a.dtype not in (torch.complex64, torch.complex128):
+        raise ArgumentError(f"{name}: complex64 or complex128 coefficients expected")
+    dev = _device_index(src) if out is None else _device_index(src, out)
+    a = to_device(a, a.dtype, dev)
+    if out is None:
+        o = julia_empty(tuple(a.shape), a.dtype, a.device)
+    else:
+        o = out
+        if not isinstance(o, torch.Tensor) or not o.is_cuda or tuple(o.shape) != tuple(a.shape):
+            raise DimensionMismatch(f"{name}: output dims")
+        if o.dtype != a.dtype or not is_julia_dense(o):
+            raise ArgumentError(f"{name}: output must be a column-major {a.dtype} device array")
+    nf = a.shape[2] if a.dim() == 3 else 1
+    plan = cfg.plan(dev)
+    dcode = _lib.SHTB_F64 if a.dtype == torch.complex128 else _lib.SHTB_F32
+    with torch.cuda.device(dev):
+        rc = _lib.load().shtb_spectral_op(plan.handle, op, _ptr(a), _ptr(o), nf, dcode, _stream(dev))
+    _lib.check(rc, name)
+    return o
+
+
+def divergence_from_spheroidal(cfg: SHTConfig, Slm):
+    """δ_lm = −l(l+1) S_lm, zero for l < max(1, m) and m off the mres lattice
+    (src/sphtor_transforms.jl:744-783). Coefficients (lmax+1, mmax+1[, nfields])."""
+    return _spectral_op("divergence_from_spheroidal", _lib.SHTB_SPEC_NEG_LL, cfg, Slm, None)
+
+
+def divergence_from_spheroidal_into(cfg: SHTConfig, out, Slm):
+    """``divergence_from_spheroidal!``: writes into ``out``, which may be ``Slm`` itself."""
+    return _spectral_op("divergence_from_spheroidal!", _lib.SHTB_SPEC_NEG_LL, cfg, Slm, out)
+
+
+def spheroidal_from_divergence(cfg: SHTConfig, dlm):
+    """S_lm = −δ_lm / (l(l+1)) for l ≥ max(1, m), else zero (src/sphtor_transforms.jl:790-831)."""
+    return _spectral_op("spheroidal_from_divergence", _lib.SHTB_SPEC_INV_NEG_LL, cfg, dlm, None)
+
+
+def spheroidal_from_divergence_into(cfg: SHTConfig, out, dlm):
+    """``spheroidal_from_divergence!``: writes into ``out``, which may be ``dlm`` itself."""
+    return _spectral_op("spheroidal_from_divergence!", _lib.SHTB_SPEC_INV_NEG_LL, cfg, dlm, out)
+
+
+def vorticity_from_toroidal(cfg: SHTConfig, Tlm):
+    """ζ_lm = −l(l+1) T_lm (src/sphtor_transforms.jl:838-877)."""
+    return _spectral_op("vorticity_from_toroidal", _lib.SHTB_SPEC_NEG_LL, cfg, Tlm, None)
+
+
+def vorticity_from_toroidal_into(cfg: SHTConfig, out, Tlm):
+    """``vorticity_from_toroidal!``: writes into ``out``, which may be ``Tlm`` itself."""
+    return _spectral_op("vorticity_from_toroidal!", _lib.SHTB_SPEC_NEG_LL, cfg, Tlm, out)
+
+
+def toroidal_from_vorticity(cfg: SHTConfig, zlm):
+    """T_lm = −ζ_lm / (l(l+1)) (src/sphtor_transforms.jl:884-925)."""
+    return _spectral_op("toroidal_from_vorticity", _lib.SHTB_SPEC_INV_NEG_LL, cfg, zlm, None)
+
+
+def toroidal_from_vorticity_into(cfg: SHTConfig, out, zlm):
+    """``toroidal_from_vorticity!``: writes into ``out``, which may be ``zlm`` itself."""
+    return _spectral_op("toroidal_from_vorticity!", _lib.SHTB_SPEC_INV_NEG_LL, cfg, zlm, out)
+
+
+def gpu_apply_laplacian(cfg: SHTConfig, coeffs):
+    """``gpu_apply_laplacian!``: in place, a_lm ← −l(l+1) a_lm on a device array (zero for
+    l < max(1, m) and m off the mres lattice; ext/GPUCommon.jl:1501-1512,
+    ext/SHTnsKitGPUExt.jl:2382-2389). Returns ``coeffs``."""
+    if not isinstance(coeffs, torch.Tensor) or not coeffs.is_cuda:
+        raise ArgumentError("gpu_apply_laplacian!: coefficients must be a device array")
+    return _spectral_op("gpu_apply_laplacian!", _lib.SHTB_SPEC_NEG_LL, cfg, coeffs, coeffs)
+
+
+def _divvort_synth(cfg, D, Z, batched, lcap):
+    d, z = _as_tensor(D), _as_tensor(Z)
+    for a, nm in ((d, "div"), (z, "vort")):
+        if a.dim() != (3 if batched else 2) or a.shape[0] != cfg.lmax + 1 or a.shape[1] != cfg.mmax + 1:
+            raise DimensionMismatch(f"{nm} dims")
+    ltr = _lcap(cfg, lcap)
+    dev = _device_index(D, Z)
+    d = to_device(d if d.is_complex() else d.to(torch.complex128), torch.complex128, dev)
+    z = to_device(z if z.is_complex() else z.to(torch.complex128), torch.complex128, dev)
+    d3 = d if batched else d.unsqueeze(2)
+    z3 = z if batched else z.unsqueeze(2)
+    nf = d3.shape[2]
+    vt = julia_empty((cfg.nlat, cfg.nlon, nf), torch.float64, d3.device)
+    vp = julia_empty((cfg.nlat, cfg.nlon, nf), torch.float64, d3.device)
+    plan = cfg.plan(dev)
+    ws, nb = _workspace(plan, _lib.SHTB_OP_SYNTHESIS_SPHTOR, nf, _lib.SHTB_F64, _lib.SHTB_PREC_FP64, dev)
+    with torch.cuda.device(dev):
+        rc = _lib.load().shtb_synthesis_divvort(plan.handle, _ptr(d3), _ptr(z3), _ptr(vt), _ptr(vp), nf, ltr,
+                                                _lib.SHTB_F64, _lib.SHTB_PREC_FP64, _ptr(ws), nb, _stream(dev))
+    _lib.check(rc, "synthesis_divvort")
+    return (vt, vp) if batched else (vt[:, :, 0], vp[:, :, 0])
+
+
+def _divvort_anal(cfg, Vt, Vp, batched, lcap):
+    a, b = _as_tensor(Vt), _as_tensor(Vp)
+    for v, nm in ((a, "Vt"), (b, "Vp")):
+        if v.is_complex() or v.dim() != (3 if batched else 2) or v.shape[0] != cfg.nlat or v.shape[1] != cfg.nlon:
+            raise DimensionMismatch(f"{nm} dims")
+    ltr = _lcap(cfg, lcap)
+    dev = _device_index(Vt, Vp)
+    a3 = to_device(a, torch.float64, dev)
+    b3 = to_device(b, torch.float64, dev)
+    a3 = a3 if batched else a3.unsqueeze(2)
+    b3 = b3 if batched else b3.unsqueeze(2)
+    nf = a3.shape[2]
+    D = julia_empty((cfg.lmax + 1, cfg.mmax + 1, nf), torch.complex128, a3.device)
+    Z = julia_empty((cfg.lmax + 1, cfg.mmax + 1, nf), torch.complex128, a3.device)
+    plan = cfg.plan(dev)
+    ws, nb = _workspace(plan, _lib.SHTB_OP_ANALYSIS_SPHTOR, nf, _lib.SHTB_F64, _lib.SHTB_PREC_FP64, dev)
+    with torch.cuda.device(dev):
+        rc = _lib.load().shtb_analysis_divvort(plan.handle, _ptr(a3), _ptr(b3), _ptr(D), _ptr(Z), nf, ltr,
+                                               _lib.SHTB_F64, _lib.SHTB_PREC_FP64, _ptr(ws), nb, _stream(dev))
+    _lib.check(rc, "analysis_divvort")
+    return (D, Z) if batched else (D[:, :, 0], Z[:, :, 0])
+
+
+def synthesis_divvort(cfg: SHTConfig, div, vort, *, lcap: int | None = None):
+    """``synthesis_sphtor(cfg, spheroidal_from_divergence(cfg, div), toroidal_from_vorticity(cfg, vort))``
+    in one pass: the −1/(l(l+1)) factor is applied as the coefficients enter the Legendre stage."""
+    return _divvort_synth(cfg, div, vort, False, lcap)
+
+
+def analysis_divvort(cfg: SHTConfig, Vt, Vp, *, lcap: int | None = None):
+    """``(divergence_from_spheroidal(S), vorticity_from_toroidal(T))`` of ``analysis_sphtor(cfg, Vt, Vp)``
+    in one pass: the −l(l+1) factor is applied as the coefficients leave the Legendre stage."""
+    return _divvort_anal(cfg, Vt, Vp, False, lcap)
+
+
+def synthesis_divvort_batch(cfg: SHTConfig, div, vort, *, lcap: int | None = None):
+    return _divvort_synth(cfg, div, vort, True, lcap)
+
+
+def analysis_divvort_batch(cfg: SHTConfig, Vt, Vp, *, lcap: int | None = None):
+    return _divvort_anal(cfg, Vt, Vp, True, lcap)
+
+
 def synthesis_qst(cfg: SHTConfig, Qlm, Slm, Tlm, *, real_output: bool = True, use_rfft: bool = False,
                   lcap: int | None = None):
     """Radial/spheroidal/toroidal synthesis to ``(Vr, Vt, Vp)`` (src/qst_transforms.jl:112-135):

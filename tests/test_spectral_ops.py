@@ -1,0 +1,47 @@
+"""CPU: the oracle's dense diagonal spectral operators against the reference's own
+test cases for them (test/parity/operators.jl:92-131, :205-216; test/parity/sphtor_full.jl:
+290-340): mres = 2 with adversarial storage in forbidden columns, l = 0 cleared, the
+Laplacian kernel on a dense ramp equal to the divergence map, and the inverse recovering
+the input on the valid entries."""
+import numpy as np
+
+from oracle import sht_oracle as so
+
+
+def test_divergence_map_and_inverse_mres2():
+    cfg = so.create_gauss_config(6, 8, mres=2)
+    rng = np.random.default_rng(0xD1A6)
+    a = (rng.standard_normal((7, 7)) + 1j * rng.standard_normal((7, 7))).astype(np.complex64)
+    d = so.neg_ll(cfg, a)
+    assert d.dtype == np.complex64
+    assert np.all(d[:, 1] == 0) and d[0, 0] == 0          # column m = 1 is forbidden with mres = 2
+    for m in range(0, 7, 2):
+        for l in range(max(1, m), 7):
+            assert d[l, m] == np.complex64(-(l * (l + 1))) * a[l, m]
+    back = so.inv_neg_ll(cfg, d)
+    expected = a.copy()
+    for m in range(7):
+        for l in range(7):
+            if m % 2 or l < max(1, m):
+                expected[l, m] = 0
+    assert np.allclose(back, expected, rtol=1e-6, atol=0)
+
+
+def test_laplacian_ramp_equals_divergence():
+    cfg = so.create_gauss_config(5, 6, mmax=4)
+    dense = (np.arange(1, 6 * 5 + 1).reshape(5, 6).T).astype(np.complex128)   # CT.(1:N), column-major
+    lap = so.neg_ll(cfg, dense)
+    for m in range(5):
+        for l in range(6):
+            want = -(l * (l + 1)) * dense[l, m] if l >= max(1, m) else 0
+            assert lap[l, m] == want
+
+
+def test_batched_trailing_field_axis():
+    cfg = so.create_gauss_config(9, 10)
+    rng = np.random.default_rng(3)
+    a = rng.standard_normal((10, 10, 3)) + 1j * rng.standard_normal((10, 10, 3))
+    d = so.neg_ll(cfg, a)
+    for k in range(3):
+        assert np.array_equal(d[:, :, k], so.neg_ll(cfg, a[:, :, k]))
+    assert np.array_equal(so.inv_neg_ll(cfg, a)[:, :, 1], so.inv_neg_ll(cfg, a[:, :, 1]))
