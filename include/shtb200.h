@@ -130,6 +130,24 @@ int shtb_analysis_sphtor(const shtb_plan* plan, const void* Vt, const void* Vp, 
                          void* work, size_t work_bytes, void* stream);
 
 /*
+ * Scalar transforms on coefficients in the packed LM layout of SHTns: per field a vector of
+ * nlm = sum over m = 0, mres, ..., mmax of (lmax - m + 1) complex values, order m's block
+ * starting at LM_index(0, m) = (im (2 lmax + 2 - (im + 1) mres)) / 2 (src/layout.jl:88-162),
+ * fields nlm apart. The gather/scatter is the transform's own coefficient addressing, not a
+ * separate pass.
+ *   shtb_synthesis_packed  synthesis_packed / synthesis_packed_l (src/transforms.jl:144-155,
+ *                          :209-227); ltr < lmax ignores the packed coefficients above ltr
+ *   shtb_analysis_packed   analysis_packed / analysis_packed_l (src/transforms.jl:125-136,
+ *                          :183-203); coefficients above ltr come out zero
+ * Arguments, workspace (SHTB_OP_SYNTHESIS / SHTB_OP_ANALYSIS), precisions and errors as
+ * shtb_synthesis / shtb_analysis.
+ */
+int shtb_synthesis_packed(const shtb_plan* plan, const void* qlm, void* f, int nfields, int ltr,
+                          int dtype, int precision, void* work, size_t work_bytes, void* stream);
+int shtb_analysis_packed(const shtb_plan* plan, const void* f, void* qlm, int nfields, int ltr,
+                         int dtype, int precision, void* work, size_t work_bytes, void* stream);
+
+/*
  * Vector transforms with divergence/vorticity spectra on the spectral side, the diagonal
  * factor applied where the coefficients enter (synthesis) or leave (analysis) the Legendre
  * stage instead of in a separate pass:

@@ -424,6 +424,48 @@ def analysis_sphtor(cfg: Config, Vt: np.ndarray, Vp: np.ndarray, ltr: int | None
 
 
 # ---------------------------------------------------------------------------
+# Packed LM layout, src/layout.jl:88-101 (nlm_calc), :143-162 (LM_index), :282-339
+# (unpack_lm / pack_lm); also decodes the packed golden fixtures. Packed transforms,
+# src/transforms.jl:125-155 and :183-227. Trailing axes (fields) pass through.
+# ---------------------------------------------------------------------------
+
+def nlm_calc(lmax: int, mmax: int, mres: int) -> int:
+    return 0 if mmax > lmax else sum(lmax - m + 1 for m in range(0, mmax + 1, mres))
+
+
+def lm_index(lmax: int, mres: int, l: int, m: int) -> int:
+    im = m // mres
+    return ((im * (2 * lmax + 2 - (im + 1) * mres)) >> 1) + l
+
+
+def pack_lm(cfg: Config, A: np.ndarray) -> np.ndarray:
+    A = np.asarray(A)
+    q = np.zeros((nlm_calc(cfg.lmax, cfg.mmax, cfg.mres),) + A.shape[2:], dtype=A.dtype)
+    for m in range(0, cfg.mmax + 1, cfg.mres):
+        b = lm_index(cfg.lmax, cfg.mres, m, m)
+        q[b:b + cfg.lmax - m + 1] = A[m:, m]
+    return q
+
+
+def unpack_lm(cfg: Config, q: np.ndarray) -> np.ndarray:
+    q = np.asarray(q)
+    A = np.zeros((cfg.lmax + 1, cfg.mmax + 1) + q.shape[1:], dtype=q.dtype)
+    for m in range(0, cfg.mmax + 1, cfg.mres):
+        b = lm_index(cfg.lmax, cfg.mres, m, m)
+        A[m:, m] = q[b:b + cfg.lmax - m + 1]
+    return A
+
+
+def synthesis_packed(cfg: Config, q: np.ndarray, ltr: int | None = None) -> np.ndarray:
+    """vec(synthesis(unpack_lm(q))) with degrees above ltr dropped."""
+    return synthesis(cfg, unpack_lm(cfg, q), ltr=ltr).reshape(-1, order="F")
+
+
+def analysis_packed(cfg: Config, v: np.ndarray, ltr: int | None = None) -> np.ndarray:
+    return pack_lm(cfg, analysis(cfg, np.asarray(v).reshape(cfg.nlat, cfg.nlon, order="F"), ltr=ltr))
+
+
+# ---------------------------------------------------------------------------
 # Dense diagonal spectral operators, src/sphtor_transforms.jl:771-783 (δ = −l(l+1) S),
 # :817-831 (S = −δ/(l(l+1))), :865-877 / :911-925 (vorticity/toroidal, same maps);
 # ext/GPUCommon.jl:1501-1512 (laplacian_kernel!, the same map as the divergence).
@@ -596,32 +638,6 @@ def synthesis_sphtor_batch(cfg, S, T, real_output=True):
 def analysis_sphtor_batch(cfg, Vt, Vp):
     outs = [analysis_sphtor(cfg, Vt[:, :, k], Vp[:, :, k]) for k in range(Vt.shape[2])]
     return np.stack([o[0] for o in outs], axis=2), np.stack([o[1] for o in outs], axis=2)
-
-
-# ---------------------------------------------------------------------------
-# Packed LM order (SHTns; src/layout.jl:143-215) for decoding fixtures
-# ---------------------------------------------------------------------------
-
-def lm_index(lmax: int, mres: int, l: int, m: int) -> int:
-    im = m // mres
-    return ((im * (2 * lmax + 2 - (im + 1) * mres)) >> 1) + l
-
-
-def unpack_lm(cfg: Config, q: np.ndarray) -> np.ndarray:
-    A = np.zeros((cfg.lmax + 1, cfg.mmax + 1), dtype=np.asarray(q).dtype)
-    for m in range(0, cfg.mmax + 1, cfg.mres):
-        for l in range(m, cfg.lmax + 1):
-            A[l, m] = q[lm_index(cfg.lmax, cfg.mres, l, m)]
-    return A
-
-
-def pack_lm(cfg: Config, A: np.ndarray) -> np.ndarray:
-    n = sum(cfg.lmax - m + 1 for m in range(0, cfg.mmax + 1, cfg.mres))
-    q = np.zeros(n, dtype=A.dtype)
-    for m in range(0, cfg.mmax + 1, cfg.mres):
-        for l in range(m, cfg.lmax + 1):
-            q[lm_index(cfg.lmax, cfg.mres, l, m)] = A[l, m]
-    return q
 
 
 def balanced_m_order(mmax: int, mres: int = 1) -> list[int]:

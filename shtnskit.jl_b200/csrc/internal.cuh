@@ -86,6 +86,19 @@ __host__ __device__ inline int btile_off(int row, int kk) {
   return (row >> 3) * 64 + (kk >> 2) * 32 + (row & 7) * 4 + (kk & 3);
 }
 
+// Start of order m's block in the packed LM layout of SHTns (src/layout.jl:143-162):
+// LM_index(l, m) = lm_base(m) + l with im = m / mres.
+__host__ __device__ inline long long lm_base(int lmax, int mres, int m) {
+  const long long im = m / mres;
+  return (im * (2LL * lmax + 2 - (im + 1) * mres)) >> 1;
+}
+// Number of packed LM coefficients (nlm_calc, src/layout.jl:88-101).
+__host__ __device__ inline long long lm_count(int lmax, int mmax, int mres) {
+  long long s = 0;
+  for (int m = 0; m <= mmax && m <= lmax; m += mres) s += lmax - m + 1;
+  return s;
+}
+
 // floor(v / d) for v * d < 2^32 with the multiplier m = floor(2^32 / d) + 1 (m = 0 means d = 1)
 __host__ __device__ inline unsigned magic_div_mul(unsigned d) {
   return d <= 1 ? 0u : (unsigned)((1ull << 32) / d + 1);

@@ -10,6 +10,8 @@ namespace shtb {
 
 // Coefficient-side operands of the Legendre stage. Element (l, im, k) lives at
 //   ptr[k * ld_k + base(im) + l],  base(im) = packed ? off[im] - m : m * ld_m.
+// packed: 0 dense (lmax+1, mmax+1) columns of stride ld_m; 1 the plan's internal packed
+// (im, l <= lrec) layout; 2 the SHTns LM layout (lm_base). ld_k: field stride.
 struct CoefSrc {
   const double2* ptr;
   long long ld_k, ld_m;

@@ -88,7 +88,8 @@ __global__ void __launch_bounds__(NT) leg_syn64_kernel(PlanDev P, CoefSrc src, F
       accE[t][f] = make_double2(0.0, 0.0);
       accO[t][f] = make_double2(0.0, 0.0);
     }
-  const long long cbase = src.packed ? (poff - m) : (long long)m * src.ld_m;
+  const long long cbase = src.packed == 1 ? (poff - m)
+                          : src.packed == 2 ? lm_base(P.lmax, P.mres, m) : (long long)m * src.ld_m;
   for (int lc = lbeg; lc <= lend; lc += LC) {
     __syncthreads();
     for (int idx = threadIdx.x; idx < LC * FB; idx += NT) {
@@ -355,8 +356,9 @@ __global__ void __launch_bounds__(256, 1) leg_ana64_kernel(PlanDev P, const doub
     }
   }
 
-  const long long dbase = dst.packed ? (poff - m) : (long long)m * dst.ld_m;
-  const int lcap = dst.packed ? lend : min(lend, P.lmax);
+  const long long dbase = dst.packed == 1 ? (poff - m)
+                          : dst.packed == 2 ? lm_base(P.lmax, P.mres, m) : (long long)m * dst.ld_m;
+  const int lcap = dst.packed == 1 ? lend : min(lend, P.lmax);
   if (ks == 0) {
 #pragma unroll
     for (int i = 0; i < TRP; ++i) {

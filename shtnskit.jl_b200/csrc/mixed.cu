@@ -62,7 +62,13 @@ struct Args {
   int nf, lend, lcap;
   const int2* tiles;         // analysis tiles (im, j0)
   int* err;
+  int cpacked;               // coefficients in the packed LM layout (field stride ld_k = nlm)
 };
+
+// First coefficient of order m of one field: dense column m, or the order's packed LM block.
+__device__ __forceinline__ long long coef_col(const Args& a, int m) {
+  return a.cpacked ? lm_base(a.P.lmax, a.P.mres, m) : (long long)m * (a.P.lmax + 1);
+}
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -564,15 +570,16 @@ __device__ __forceinline__ bool promo_tile(const Args& a, const TileCoord& tc, c
     if (l <= a.lcap) {
       const float s = coef_factor(a, l, m);
       const long long ld = a.ld_k;
-      float2* c = a.cout + (long long)kf0 * ld + (long long)m * (P.lmax + 1) + l;
+      float2* c = a.cout + (long long)kf0 * ld + coef_col(a, m) + l;
 #pragma unroll
       for (int qq = 0; qq < N / 4; ++qq)
         if (qq < nq) c[qq * ld] = make_float2(acc[2 * qq] * s, acc[2 * qq + 1] * s);
     }
   }
-  if (MODE == 1 && tc.j0 == 0) {
+  if (MODE == 1 && tc.j0 == 0 && !a.cpacked) {
     // The first tile of each order also clears that order's degrees l < m and
-    // lcap < l <= lmax; the two parity tiles take half of the fields each.
+    // lcap < l <= lmax (dense layout; a packed output is cleared before the call); the
+    // two parity tiles take half of the fields each.
     const int pt = tid - 9 * 32;
     const int nfl = min(N / 2, nf - kb), hf = (nfl + 1) / 2;
     const int f0 = par ? hf : 0, f1 = par ? nfl : hf;
@@ -622,7 +629,7 @@ __device__ __forceinline__ void pack_order(const Args& a, int im, int k) {
   const PlanDev& P = a.P;
   const int m = im * P.mres;
   const int nfp = btile_nfp(a.nf), fl = k & 63;
-  const float2* c = a.cin + (long long)k * a.ld_k + (long long)m * (P.lmax + 1);
+  const float2* c = a.cin + (long long)k * a.ld_k + coef_col(a, m);
   for (int par = 0; par < 2; ++par) {
     const long long sg = a.seg[2 * im + par];
     const int R = (int)(a.seg[2 * im + par + 1] - sg);
@@ -908,12 +915,17 @@ static Args base_args(const shtb_plan* p) {
   return a;
 }
 
-int mixed_synthesis(const shtb_plan* p, const void* alm, void* f, int nf, int ltr, void* work, cudaStream_t st) {
+int mixed_synthesis(const shtb_plan* p, const void* alm, void* f, int nf, int ltr, void* work, cudaStream_t st,
+                    int packed) {
   int rc = ensure_table(p, st);
   if (rc) return rc;
   const int mlim = std::min(p->mmax, ltr);
   Args a = base_args(p);
   a.cin = (const float2*)alm;
+  if (packed) {
+    a.cpacked = 1;
+    a.ld_k = lm_count(p->lmax, p->mmax, p->mres);
+  }
   a.Wout = (float2*)work;
   a.bimg = (float*)((char*)work + syn_w_bytes(p, nf));
   a.sc_mode = p->d_scale ? 1 : 0;
@@ -933,10 +945,14 @@ size_t mixed_workspace_bytes(const shtb_plan* p, int op, int nf) {
   return align256(fft_btile_floats(p, nf) * 4);
 }
 
-int mixed_analysis(const shtb_plan* p, const void* f, void* alm, int nf, int ltr, void* work, cudaStream_t st) {
+int mixed_analysis(const shtb_plan* p, const void* f, void* alm, int nf, int ltr, void* work, cudaStream_t st,
+                   int packed) {
   int rc = ensure_table(p, st);
   if (rc) return rc;
   const int mlim = std::min(p->mmax, ltr);
+  const long long nlm = lm_count(p->lmax, p->mmax, p->mres);
+  if (packed && ltr < p->lmax)   // degrees above ltr are no tile's output
+    SHTB_TRY_CUDA(cudaMemsetAsync(alm, 0, (size_t)nlm * nf * sizeof(float2), st), "packed output clear");
   if ((rc = launch_fft_ana<float, float>(p, (const float*)f, nullptr, 1, work, nf, mlim, p->ana_scale, 1, 0, st, 1)))
     return rc;
   // analysis tiles: 128 degrees of each parity per tile
@@ -966,8 +982,12 @@ int mixed_analysis(const shtb_plan* p, const void* f, void* alm, int nf, int ltr
   a.lend = ltr;
   a.lcap = ltr;
   a.tiles = p->d_mx_tiles;
+  if (packed) {
+    a.cpacked = 1;
+    a.ld_k = nlm;
+  }
   if ((rc = dispatch_gemm<1>(p, a, nf, 2 * (int)tl.size(), 0, st))) return rc;
-  if (p->mres > 1 || mlim < p->mmax) {
+  if (!packed && (p->mres > 1 || mlim < p->mmax)) {
     dim3 zg(p->mmax + 1, nf);
     prof_begin(st);
     zero_columns_kernel32<<<zg, 256, 0, st>>>(p->dev, (float2*)alm, a.ld_k, mlim);

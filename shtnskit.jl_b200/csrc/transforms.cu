@@ -206,42 +206,74 @@ static Factors fac_none() { return Factors{nullptr, nullptr, 0, 1.0, 1.0}; }
 
 // Mixed-precision entry points live in mixed.cu.
 namespace shtb {
-int mixed_synthesis(const shtb_plan* p, const void* alm, void* f, int nf, int ltr, void* work, cudaStream_t st);
-int mixed_analysis(const shtb_plan* p, const void* f, void* alm, int nf, int ltr, void* work, cudaStream_t st);
+int mixed_synthesis(const shtb_plan* p, const void* alm, void* f, int nf, int ltr, void* work, cudaStream_t st,
+                    int packed);
+int mixed_analysis(const shtb_plan* p, const void* f, void* alm, int nf, int ltr, void* work, cudaStream_t st,
+                   int packed);
 }
 
 // ---------------------------------------------------------------------------
 // scalar
 // ---------------------------------------------------------------------------
-extern "C" int shtb_synthesis(const shtb_plan* p, const void* alm, void* f, int nf, int ltr, int dtype,
-                              int precision, void* work, size_t wb, void* stream) {
+// packed = 1: coefficients in the SHTns LM layout (nlm per field) instead of dense columns.
+static int scalar_synthesis(const shtb_plan* p, const void* alm, void* f, int nf, int ltr, int dtype, int precision,
+                            void* work, size_t wb, void* stream, int packed) {
   int rc = check_common(p, nf, &ltr, dtype, precision, work, wb, SHTB_OP_SYNTHESIS);
   if (rc) return rc;
   if ((rc = check_ptrs({alm, f}))) return rc;
   cudaStream_t st = (cudaStream_t)stream;
   const int mlim = std::min(p->mmax, ltr);
-  if (precision == SHTB_PREC_MIXED) return mixed_synthesis(p, alm, f, nf, ltr, work, st);
-  CoefSrc src{(const double2*)alm, (long long)(p->lmax + 1) * (p->mmax + 1), (long long)(p->lmax + 1), 0};
+  if (precision == SHTB_PREC_MIXED) return mixed_synthesis(p, alm, f, nf, ltr, work, st, packed);
+  CoefSrc src = packed ? CoefSrc{(const double2*)alm, lm_count(p->lmax, p->mmax, p->mres), 0, 2}
+                       : CoefSrc{(const double2*)alm, (long long)(p->lmax + 1) * (p->mmax + 1), (long long)(p->lmax + 1), 0};
   Factors F{p->dev.cfac, p->d_scale, p->d_scale ? 1 : 0, 1.0, 1.0};
   if ((rc = launch_leg_syn64(p, src, F, work, nf, ltr, mlim, st))) return rc;
   return launch_fft_syn<double, double>(p, work, (double*)f, nullptr, 1, nf, mlim, p->phi_inv_scale / p->nlon, 0, 0, st);
 }
 
-extern "C" int shtb_analysis(const shtb_plan* p, const void* f, void* alm, int nf, int ltr, int dtype,
-                             int precision, void* work, size_t wb, void* stream) {
+static int scalar_analysis(const shtb_plan* p, const void* f, void* alm, int nf, int ltr, int dtype, int precision,
+                           void* work, size_t wb, void* stream, int packed) {
   int rc = check_common(p, nf, &ltr, dtype, precision, work, wb, SHTB_OP_ANALYSIS);
   if (rc) return rc;
   if ((rc = check_ptrs({alm, f}))) return rc;
   cudaStream_t st = (cudaStream_t)stream;
   const int mlim = std::min(p->mmax, ltr);
-  if (precision == SHTB_PREC_MIXED) return mixed_analysis(p, f, alm, nf, ltr, work, st);
+  if (precision == SHTB_PREC_MIXED) return mixed_analysis(p, f, alm, nf, ltr, work, st, packed);
   if ((rc = launch_fft_ana<double, double>(p, (const double*)f, nullptr, 1, work, nf, mlim, p->ana_scale, 1, 0, st)))
     return rc;
-  CoefSink dst{(double2*)alm, (long long)(p->lmax + 1) * (p->mmax + 1), (long long)(p->lmax + 1), 0};
   Factors F{p->dev.cfac, p->d_scale, p->d_scale ? 2 : 0, 1.0, 1.0};
+  if (packed) {
+    // every order's block is written for l <= ltr; degrees above ltr and orders above it start cleared
+    const long long nlm = lm_count(p->lmax, p->mmax, p->mres);
+    if (ltr < p->lmax)
+      SHTB_TRY_CUDA(cudaMemsetAsync(alm, 0, (size_t)nlm * nf * sizeof(double2), st), "packed output clear");
+    CoefSink dst{(double2*)alm, nlm, 0, 2};
+    return launch_leg_ana64(p, work, nf, ltr, mlim, dst, F, 0, st);
+  }
+  CoefSink dst{(double2*)alm, (long long)(p->lmax + 1) * (p->mmax + 1), (long long)(p->lmax + 1), 0};
   if ((rc = launch_leg_ana64(p, work, nf, ltr, mlim, dst, F, 1, st))) return rc;
   if (p->mres > 1 || mlim < p->mmax) return launch_zero_columns64(p, (double2*)alm, nf, mlim, st);
   return SHTB_OK;
+}
+
+extern "C" int shtb_synthesis(const shtb_plan* p, const void* alm, void* f, int nf, int ltr, int dtype,
+                              int precision, void* work, size_t wb, void* stream) {
+  return scalar_synthesis(p, alm, f, nf, ltr, dtype, precision, work, wb, stream, 0);
+}
+
+extern "C" int shtb_analysis(const shtb_plan* p, const void* f, void* alm, int nf, int ltr, int dtype,
+                             int precision, void* work, size_t wb, void* stream) {
+  return scalar_analysis(p, f, alm, nf, ltr, dtype, precision, work, wb, stream, 0);
+}
+
+extern "C" int shtb_synthesis_packed(const shtb_plan* p, const void* qlm, void* f, int nf, int ltr, int dtype,
+                                     int precision, void* work, size_t wb, void* stream) {
+  return scalar_synthesis(p, qlm, f, nf, ltr, dtype, precision, work, wb, stream, 1);
+}
+
+extern "C" int shtb_analysis_packed(const shtb_plan* p, const void* f, void* qlm, int nf, int ltr, int dtype,
+                                    int precision, void* work, size_t wb, void* stream) {
+  return scalar_analysis(p, f, qlm, nf, ltr, dtype, precision, work, wb, stream, 1);
 }
 
 // ---------------------------------------------------------------------------

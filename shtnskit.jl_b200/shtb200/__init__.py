@@ -13,7 +13,9 @@ from .transforms import (  # noqa: F401
     spheroidal_from_divergence, spheroidal_from_divergence_into, synthesis, synthesis_batch, synthesis_divvort,
     synthesis_divvort_batch, synthesis_into, synthesis_qst, synthesis_qst_batch, synthesis_sphtor,
     synthesis_sphtor_batch, to_device, to_host, toroidal_from_vorticity, toroidal_from_vorticity_into,
-    vorticity_from_toroidal, vorticity_from_toroidal_into,
+    vorticity_from_toroidal, vorticity_from_toroidal_into, LM_index, nlm_calc, pack_lm, unpack_lm,
+    synthesis_packed, synthesis_packed_l, analysis_packed, analysis_packed_l, synthesis_packed_batch,
+    analysis_packed_batch,
 )
 
 __version__ = "0.1.0"

@@ -73,6 +73,8 @@ SIGNATURES = {
     "shtb_analysis": (_I, [_P, _P, _P, _I, _I, _I, _I, _P, _SZ, _P]),
     "shtb_synthesis_sphtor": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _P, _SZ, _P]),
     "shtb_analysis_sphtor": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _P, _SZ, _P]),
+    "shtb_synthesis_packed": (_I, [_P, _P, _P, _I, _I, _I, _I, _P, _SZ, _P]),
+    "shtb_analysis_packed": (_I, [_P, _P, _P, _I, _I, _I, _I, _P, _SZ, _P]),
     "shtb_synthesis_divvort": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _P, _SZ, _P]),
     "shtb_analysis_divvort": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _P, _SZ, _P]),
     "shtb_spectral_op": (_I, [_P, _I, _P, _P, _I, _I, _P]),

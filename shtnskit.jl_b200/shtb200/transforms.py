@@ -515,6 +515,144 @@ def analysis_sphtor_batch(cfg: SHTConfig, Vt, Vp, *, use_rfft: bool = False, lca
 
 
 # ---------------------------------------------------------------------------
+# packed LM layout (SHTns order: m blocks of l = m..lmax, src/layout.jl:88-339)
+# ---------------------------------------------------------------------------
+
+def nlm_calc(lmax: int, mmax: int, mres: int) -> int:
+    """Number of packed coefficients (src/layout.jl:88-101)."""
+    if lmax < 0 or mmax < 0 or mres < 1:
+        raise ArgumentError("invalid sizes")
+    if mmax > lmax:
+        return 0
+    return sum(lmax - m + 1 for m in range(0, mmax + 1, mres))
+
+
+def LM_index(lmax: int, mres: int, l: int, m: int) -> int:
+    """0-based packed index of (l, m) (src/layout.jl:143-162)."""
+    if m < 0:
+        raise ArgumentError("m must be ≥ 0 for packed layout")
+    if m % mres:
+        raise ArgumentError("m must be a multiple of mres")
+    if not (m <= l <= lmax):
+        raise ArgumentError("require m ≤ l ≤ lmax")
+    im = m // mres
+    return ((im * (2 * lmax + 2 - (im + 1) * mres)) >> 1) + l
+
+
+def _lm_gather_index(cfg: SHTConfig, device) -> torch.Tensor:
+    """Dense column-major offsets l + (lmax+1) m of the packed entries, in packed order."""
+    idx = [l + (cfg.lmax + 1) * m for m in range(0, cfg.mmax + 1, cfg.mres) for l in range(m, cfg.lmax + 1)]
+    return torch.tensor(idx, dtype=torch.long, device=device)
+
+
+def pack_lm(cfg: SHTConfig, A):
+    """Dense (lmax+1, mmax+1) coefficients to the packed LM vector (src/layout.jl:315-339);
+    orders off the mres lattice are skipped."""
+    a = _as_tensor(A)
+    _check_coeff_shape(cfg, a, False)
+    dev = _device_index(A)
+    a = to_device(a if a.is_complex() else a.to(torch.complex128), a.dtype if a.is_complex() else torch.complex128, dev)
+    flat = a.permute(1, 0).reshape(-1)                    # column-major memory order
+    return flat[_lm_gather_index(cfg, a.device)].contiguous()
+
+
+def unpack_lm(cfg: SHTConfig, Qlm):
+    """Packed LM vector to dense (lmax+1, mmax+1) coefficients, zero where the packed layout
+    has no entry (src/layout.jl:282-307)."""
+    q = _as_tensor(Qlm)
+    if q.dim() != 1 or q.shape[0] != cfg.nlm:
+        raise DimensionMismatch(f"Qlm must have length {cfg.nlm}")
+    dev = _device_index(Qlm)
+    q = q.to(torch.device("cuda", dev))
+    if not q.is_complex():
+        q = q.to(torch.complex128)
+    out = julia_empty((cfg.lmax + 1, cfg.mmax + 1), q.dtype, q.device)
+    out.zero_()
+    out.permute(1, 0).reshape(-1)[_lm_gather_index(cfg, q.device)] = q
+    return out
+
+
+def _packed_synth(cfg, Qlm, batched, lcap, precision):
+    q = _as_tensor(Qlm)
+    if q.dim() != (2 if batched else 1) or q.shape[0] != cfg.nlm:
+        raise DimensionMismatch(f"Qlm must have length {cfg.nlm}")
+    ltr = _lcap(cfg, lcap)
+    prec = _prec_code(precision)
+    rt, ct, dcode = _types(prec)
+    dev = _device_index(Qlm)
+    q = to_device(q if q.is_complex() else q.to(ct), ct, dev)
+    q2 = q if batched else q.unsqueeze(1)
+    nf = q2.shape[1]
+    f = julia_empty((cfg.nlat, cfg.nlon, nf), rt, q2.device)
+    plan = cfg.plan(dev)
+    ws, nb = _workspace(plan, _lib.SHTB_OP_SYNTHESIS, nf, dcode, prec, dev)
+    with torch.cuda.device(dev):
+        rc = _lib.load().shtb_synthesis_packed(plan.handle, _ptr(q2), _ptr(f), nf, ltr, dcode, prec, _ptr(ws), nb,
+                                               _stream(dev))
+    _lib.check(rc, "synthesis_packed")
+    flat = f.permute(2, 1, 0).reshape(nf, cfg.nlat * cfg.nlon).permute(1, 0)   # vec(f) per field
+    return flat if batched else flat[:, 0]
+
+
+def _packed_anal(cfg, Vr, batched, lcap, precision):
+    v = _as_tensor(Vr)
+    if v.is_complex() or v.dim() != (2 if batched else 1) or v.shape[0] != cfg.nlat * cfg.nlon:
+        raise DimensionMismatch(f"Vr must have length {cfg.nlat * cfg.nlon}")
+    ltr = _lcap(cfg, lcap)
+    prec = _prec_code(precision)
+    rt, ct, dcode = _types(prec)
+    dev = _device_index(Vr)
+    v = to_device(v, rt, dev)
+    v2 = v if batched else v.unsqueeze(1)
+    nf = v2.shape[1]
+    grid = v2.permute(1, 0).reshape(nf, cfg.nlon, cfg.nlat).permute(2, 1, 0)   # (nlat, nlon, nf), column-major
+    if not is_julia_dense(grid):
+        g = julia_empty((cfg.nlat, cfg.nlon, nf), rt, v2.device)
+        g.copy_(grid)
+        grid = g
+    q = julia_empty((cfg.nlm, nf), ct, v2.device)
+    plan = cfg.plan(dev)
+    ws, nb = _workspace(plan, _lib.SHTB_OP_ANALYSIS, nf, dcode, prec, dev)
+    with torch.cuda.device(dev):
+        rc = _lib.load().shtb_analysis_packed(plan.handle, _ptr(grid), _ptr(q), nf, ltr, dcode, prec, _ptr(ws), nb,
+                                              _stream(dev))
+    _lib.check(rc, "analysis_packed")
+    return q if batched else q[:, 0]
+
+
+def synthesis_packed(cfg: SHTConfig, Qlm, *, precision: str = "fp64"):
+    """Packed LM coefficients (length nlm) to the flattened real grid vec(f), length nlat·nlon
+    (src/transforms.jl:144-155)."""
+    return _packed_synth(cfg, Qlm, False, None, precision)
+
+
+def synthesis_packed_l(cfg: SHTConfig, Qlm, ltr: int, *, precision: str = "fp64"):
+    """``synthesis_packed`` using degrees l ≤ ltr only (src/transforms.jl:209-227)."""
+    return _packed_synth(cfg, Qlm, False, ltr, precision)
+
+
+def analysis_packed(cfg: SHTConfig, Vr, *, precision: str = "fp64"):
+    """Flattened real grid (length nlat·nlon) to packed LM coefficients (src/transforms.jl:125-136)."""
+    return _packed_anal(cfg, Vr, False, None, precision)
+
+
+def analysis_packed_l(cfg: SHTConfig, Vr, ltr: int, *, precision: str = "fp64"):
+    """``analysis_packed`` truncated to l ≤ ltr; the other packed entries are zero
+    (src/transforms.jl:183-203)."""
+    return _packed_anal(cfg, Vr, False, ltr, precision)
+
+
+def synthesis_packed_batch(cfg: SHTConfig, Qlm, *, lcap: int | None = None, precision: str = "fp64"):
+    """Fields along the trailing axis: (nlm, nfields) -> (nlat·nlon, nfields)."""
+    return _packed_synth(cfg, Qlm, True, lcap, precision)
+
+
+def analysis_packed_batch(cfg: SHTConfig, Vr, *, lcap: int | None = None, precision: str = "fp64"):
+    """(nlat·nlon, nfields) -> (nlm, nfields)."""
+    return _packed_anal(cfg, Vr, True, lcap, precision)
+
+
+# ---------------------------------------------------------------------------
 # diagonal spectral operators and divergence/vorticity spectra
 # ---------------------------------------------------------------------------
 

@@ -108,3 +108,54 @@ def test_divvort_batch_roundtrip_and_lcap():
     vt_l, vp_l = sht.synthesis_divvort(cfg, D[:, :, 0], Z[:, :, 0], lcap=ltr)
     vt_ref, _ = so.synthesis_sphtor(ocfg, so.inv_neg_ll(ocfg, D[:, :, 0]), so.inv_neg_ll(ocfg, Z[:, :, 0]), ltr=ltr)
     assert rel_l2(host(vt_l), vt_ref) <= TOL64
+
+
+# ---------------------------------------------------------------- packed LM layout
+PACKED_CASES = [dict(lmax=31, nlat=32), dict(lmax=47, nlat=50, mres=2, mmax=40),
+                dict(lmax=20, nlat=22, nlon=45, mmax=12)]
+
+
+@pytest.mark.parametrize("case", PACKED_CASES, ids=["l31", "l47-mres2", "l20-mmax12"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_packed_equals_dense_bitwise(case, precision):
+    """The packed entry points address the coefficients differently but compute the same
+    values: bit-identical to pack_lm / unpack_lm around the dense transforms."""
+    c = dict(case)
+    lmax, nlat = c.pop("lmax"), c.pop("nlat")
+    cfg = sht.create_gauss_config(lmax, nlat, **c)
+    ocfg = so.create_gauss_config(lmax, nlat, **c)
+    A = rand_alm(lmax, cfg.mmax, seed=41, mres=cfg.mres)
+    if precision == "mixed":
+        A = A.astype(np.complex64)
+    q = so.pack_lm(ocfg, A)
+    f_dense = host(sht.synthesis(cfg, A, precision=precision))
+    v = host(sht.synthesis_packed(cfg, q, precision=precision))
+    assert np.array_equal(v, f_dense.reshape(-1, order="F"))
+    g = np.random.default_rng(42).standard_normal((nlat, cfg.nlon))
+    if precision == "mixed":
+        g = g.astype(np.float32)
+    a_dense = host(sht.analysis(cfg, g, precision=precision))
+    qa = host(sht.analysis_packed(cfg, g.reshape(-1, order="F"), precision=precision))
+    assert np.array_equal(qa, so.pack_lm(ocfg, a_dense))
+    for ltr in (0, lmax // 3):
+        vl = host(sht.synthesis_packed_l(cfg, q, ltr, precision=precision))
+        assert np.array_equal(vl, host(sht.synthesis(cfg, A, lcap=ltr, precision=precision)).reshape(-1, order="F"))
+        ql = host(sht.analysis_packed_l(cfg, g.reshape(-1, order="F"), ltr, precision=precision))
+        assert np.array_equal(ql, so.pack_lm(ocfg, host(sht.analysis(cfg, g, lcap=ltr, precision=precision))))
+
+
+def test_packed_vs_oracle_and_batch():
+    cfg = sht.create_gauss_config(40, 42, mres=2)
+    ocfg = so.create_gauss_config(40, 42, mres=2)
+    A = rand_alm(40, 40, 3, seed=43, mres=2)
+    Q = so.pack_lm(ocfg, A)
+    V = host(sht.synthesis_packed_batch(cfg, Q))
+    assert V.shape == (42 * cfg.nlon, 3)
+    for k in range(3):
+        assert rel_l2(V[:, k], so.synthesis_packed(ocfg, Q[:, k])) <= TOL64
+    back = host(sht.analysis_packed_batch(cfg, V))
+    assert rel_l2(back, Q) <= TOL64
+    assert np.array_equal(host(sht.pack_lm(cfg, A[:, :, 0])), Q[:, 0])
+    assert np.array_equal(host(sht.unpack_lm(cfg, Q[:, 1])), so.unpack_lm(ocfg, Q[:, 1]))
+    with pytest.raises(DimensionMismatch):
+        sht.synthesis_packed(cfg, Q[:-1, 0])

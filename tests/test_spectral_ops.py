@@ -45,3 +45,32 @@ def test_batched_trailing_field_axis():
     for k in range(3):
         assert np.array_equal(d[:, :, k], so.neg_ll(cfg, a[:, :, k]))
     assert np.array_equal(so.inv_neg_ll(cfg, a)[:, :, 1], so.inv_neg_ll(cfg, a[:, :, 1]))
+
+
+def test_packed_lm_layout():
+    """LM_index walks the m blocks of l = m..lmax contiguously (src/layout.jl:143-162), and
+    pack/unpack invert each other on the stored entries."""
+    for lmax, mmax, mres in ((4, 4, 2), (9, 6, 3), (12, 12, 1)):
+        cfg = so.create_gauss_config(lmax, lmax + 2, mmax=mmax, mres=mres)
+        idx = [so.lm_index(lmax, mres, l, m) for m in range(0, mmax + 1, mres) for l in range(m, lmax + 1)]
+        assert idx == list(range(so.nlm_calc(lmax, mmax, mres)))
+        rng = np.random.default_rng(lmax)
+        A = rng.standard_normal((lmax + 1, mmax + 1)) + 1j * rng.standard_normal((lmax + 1, mmax + 1))
+        q = so.pack_lm(cfg, A)
+        back = so.unpack_lm(cfg, q)
+        for m in range(mmax + 1):
+            for l in range(lmax + 1):
+                assert back[l, m] == (A[l, m] if (m % mres == 0 and l >= m) else 0)
+    assert so.lm_index(4, 2, 2, 2) == 5 and so.lm_index(4, 2, 4, 4) == 8
+
+
+def test_packed_transforms_oracle_roundtrip():
+    cfg = so.create_gauss_config(15, 16)
+    rng = np.random.default_rng(8)
+    A = rng.standard_normal((16, 16)) + 1j * rng.standard_normal((16, 16))
+    A = np.tril(A)
+    A[:, 0] = A[:, 0].real
+    q = so.pack_lm(cfg, A)
+    v = so.synthesis_packed(cfg, q)
+    assert v.shape == (16 * cfg.nlon,)
+    assert np.allclose(so.analysis_packed(cfg, v), q, rtol=0, atol=1e-12)
