@@ -192,3 +192,20 @@ def test_in_place_and_errors():
         sht.analysis(cfg, np.zeros((16, 32)), lcap=16)
     with pytest.raises(sht.ArgumentError):
         sht.analysis(cfg, np.zeros((16, 32)), fft_scratch=np.zeros((16, 32), complex))
+
+
+@pytest.mark.parametrize("nf", [40, 64, 70])
+def test_wide_batches_fp64_and_mixed(nf):
+    """Batches past 32 and 64 fields take the widest kernel shapes (128-column FP64
+    analysis tiles, N = 128 GEMM tiles, several 64-field blocks)."""
+    cfg, ocfg = both(31, 32)
+    a = rand_alm(31, 31, nf, seed=51)
+    f_ref = so.synthesis_batch(ocfg, a)
+    assert rel_l2(host(sht.synthesis_batch(cfg, a)), f_ref) <= TOL64
+    g = np.random.default_rng(52).standard_normal((32, cfg.nlon, nf))
+    b_ref = so.analysis_batch(ocfg, g)
+    assert rel_l2(host(sht.analysis_batch(cfg, g)), b_ref) <= TOL64
+    f32 = host(sht.synthesis_batch(cfg, a.astype(np.complex64), precision="mixed"))
+    assert rel_l2(f32, so.synthesis_batch(ocfg, a.astype(np.complex64).astype(np.complex128))) <= 1e-6
+    b32 = host(sht.analysis_batch(cfg, g.astype(np.float32), precision="mixed"))
+    assert rel_l2(b32, so.analysis_batch(ocfg, g.astype(np.float32).astype(np.float64))) <= 1e-6
