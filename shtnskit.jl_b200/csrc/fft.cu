@@ -178,7 +178,8 @@ __device__ __forceinline__ void fft_syn_body(const FFTJob<T>& J, int p0, int k, 
   __syncthreads();
   const int nmu = mlim / P.mres + 1;
   // one (im, pair) item per thread; consecutive threads read consecutive pairs of one m
-  constexpr int U = 16;   // all of a thread's (order, pair) items for H = 8: their loads overlap
+  // FP32: all of a thread's (order, pair) items for H = 8 in flight together; FP64 keeps 4 (registers)
+  constexpr int U = sizeof(T) == 4 ? 16 : 4;
   for (int base0 = threadIdx.x; base0 < nmu * H; base0 += blockDim.x * U) {
     V Ev[U], Ov[U];
 #pragma unroll
