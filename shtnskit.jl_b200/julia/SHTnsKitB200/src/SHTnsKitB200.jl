@@ -175,6 +175,60 @@ SHTnsKit.synthesis_batch(cfg::SHTnsKit.SHTConfig, alm::CuArray{<:Complex,3}; lca
 SHTnsKit.analysis_batch(cfg::SHTnsKit.SHTConfig, f::CuArray{<:Real,3}; lcap::Int=cfg.lmax, kwargs...) =
     _analysis(cfg, f; lcap)
 
+# ---------------------------------------------------------------- packed LM layout (src/transforms.jl:125-227)
+function _synthesis_packed(cfg, Q::CuVector{Complex{T}}, lcap::Int) where {T<:Union{Float32,Float64}}
+    length(Q) == cfg.nlm || throw(DimensionMismatch("Qlm must have length $(cfg.nlm)"))
+    f = CuArray{T}(undef, cfg.nlat, cfg.nlon)
+    p = plan(cfg)
+    ws = workspace(p, OP_SYN, 1, dtype_of(T), prec_of(T))
+    check(ccall((:shtb_synthesis_packed, LIB), Cint,
+                (Ptr{Cvoid}, CuPtr{Cvoid}, CuPtr{Cvoid}, Cint, Cint, Cint, Cint, CuPtr{Cvoid}, Csize_t, Ptr{Cvoid}),
+                p.ptr, Q, f, 1, lcap, dtype_of(T), prec_of(T), ws, sizeof(ws), stream()), :synthesis_packed)
+    return vec(f)
+end
+
+function _analysis_packed(cfg, Vr::CuVector{T}, lcap::Int) where {T<:Union{Float32,Float64}}
+    length(Vr) == cfg.nlat * cfg.nlon || throw(DimensionMismatch("Vr must have length $(cfg.nlat * cfg.nlon)"))
+    Q = CuArray{Complex{T}}(undef, cfg.nlm)
+    p = plan(cfg)
+    ws = workspace(p, OP_ANA, 1, dtype_of(T), prec_of(T))
+    check(ccall((:shtb_analysis_packed, LIB), Cint,
+                (Ptr{Cvoid}, CuPtr{Cvoid}, CuPtr{Cvoid}, Cint, Cint, Cint, Cint, CuPtr{Cvoid}, Csize_t, Ptr{Cvoid}),
+                p.ptr, Vr, Q, 1, lcap, dtype_of(T), prec_of(T), ws, sizeof(ws), stream()), :analysis_packed)
+    return Q
+end
+
+SHTnsKit.synthesis_packed(cfg::SHTnsKit.SHTConfig, Q::CuVector{<:Complex}) = _synthesis_packed(cfg, Q, cfg.lmax)
+SHTnsKit.synthesis_packed_l(cfg::SHTnsKit.SHTConfig, Q::CuVector{<:Complex}, ltr::Integer) =
+    _synthesis_packed(cfg, Q, Int(ltr))
+SHTnsKit.analysis_packed(cfg::SHTnsKit.SHTConfig, Vr::CuVector{<:Real}) = _analysis_packed(cfg, Vr, cfg.lmax)
+SHTnsKit.analysis_packed_l(cfg::SHTnsKit.SHTConfig, Vr::CuVector{<:Real}, ltr::Integer) =
+    _analysis_packed(cfg, Vr, Int(ltr))
+
+# ---------------------------------------------------------------- diagonal spectral operators
+# (src/sphtor_transforms.jl:744-930, ext/GPUCommon.jl:1501-1512); `out` may be `in` itself
+const SPEC_NEG_LL = Cint(0)
+const SPEC_INV_NEG_LL = Cint(1)
+function _spectral_op!(cfg, op::Cint, out::CuMatrix{Complex{T}}, in::CuMatrix{Complex{T}}) where {T<:Union{Float32,Float64}}
+    expected = (cfg.lmax + 1, cfg.mmax + 1)
+    size(in) == expected || throw(DimensionMismatch("spectral input dims"))
+    size(out) == size(in) || throw(DimensionMismatch("spectral output dims"))
+    check(ccall((:shtb_spectral_op, LIB), Cint,
+                (Ptr{Cvoid}, Cint, CuPtr{Cvoid}, CuPtr{Cvoid}, Cint, Cint, Ptr{Cvoid}),
+                plan(cfg).ptr, op, in, out, 1, dtype_of(T), stream()), :spectral_op)
+    return out
+end
+SHTnsKit.divergence_from_spheroidal!(cfg::SHTnsKit.SHTConfig, d::CuMatrix, S::CuMatrix) = _spectral_op!(cfg, SPEC_NEG_LL, d, S)
+SHTnsKit.vorticity_from_toroidal!(cfg::SHTnsKit.SHTConfig, z::CuMatrix, T::CuMatrix) = _spectral_op!(cfg, SPEC_NEG_LL, z, T)
+SHTnsKit.spheroidal_from_divergence!(cfg::SHTnsKit.SHTConfig, S::CuMatrix, d::CuMatrix) = _spectral_op!(cfg, SPEC_INV_NEG_LL, S, d)
+SHTnsKit.toroidal_from_vorticity!(cfg::SHTnsKit.SHTConfig, T::CuMatrix, z::CuMatrix) = _spectral_op!(cfg, SPEC_INV_NEG_LL, T, z)
+SHTnsKit.divergence_from_spheroidal(cfg::SHTnsKit.SHTConfig, S::CuMatrix) = _spectral_op!(cfg, SPEC_NEG_LL, similar(S), S)
+SHTnsKit.vorticity_from_toroidal(cfg::SHTnsKit.SHTConfig, T::CuMatrix) = _spectral_op!(cfg, SPEC_NEG_LL, similar(T), T)
+SHTnsKit.spheroidal_from_divergence(cfg::SHTnsKit.SHTConfig, d::CuMatrix) = _spectral_op!(cfg, SPEC_INV_NEG_LL, similar(d), d)
+SHTnsKit.toroidal_from_vorticity(cfg::SHTnsKit.SHTConfig, z::CuMatrix) = _spectral_op!(cfg, SPEC_INV_NEG_LL, similar(z), z)
+SHTnsKit.gpu_apply_laplacian!(cfg::SHTnsKit.SHTConfig, a::CuMatrix; device=SHTnsKit.GPU()) =
+    _spectral_op!(cfg, SPEC_NEG_LL, a, a)
+
 # ---------------------------------------------------------------- adjoint kernels behind the rrules
 function _adjoint(sym::Symbol, op::Cint, cfg, ins::Tuple, outs::Tuple, nf)
     p = plan(cfg)
