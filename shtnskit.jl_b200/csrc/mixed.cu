@@ -130,16 +130,6 @@ __device__ __forceinline__ unsigned idesc_tf32() {
   return (1u << 4) | (2u << 7) | (2u << 10) | ((unsigned)(N >> 3) << 17) | ((unsigned)(kM >> 4) << 24);
 }
 
-__device__ __forceinline__ void mma_tf32(unsigned tmem_d, unsigned long long a, unsigned long long b, unsigned idesc,
-                                         unsigned accum) {
-  const unsigned z = 0;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-      :
-      : "r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(accum), "r"(z), "r"(z), "r"(z), "r"(z));
-}
 // A from TMEM (M = 128 lanes x 8 columns of TF32), B from shared memory.
 __device__ __forceinline__ void mma_tf32_ts(unsigned tmem_d, unsigned tmem_a, unsigned long long b, unsigned idesc,
                                             unsigned accum) {
@@ -152,9 +142,8 @@ __device__ __forceinline__ void mma_tf32_ts(unsigned tmem_d, unsigned tmem_a, un
       : "r"(tmem_d), "r"(tmem_a), "l"(b), "r"(idesc), "r"(accum), "r"(z), "r"(z), "r"(z), "r"(z));
 }
 
-// Store this thread's 8 hi values at columns taddr.. and 8 lo values at taddr+8.. of
-// its TMEM lane, then wait for the stores.
-// Two 8-column TMEM stores (hi at taddr, lo at taddr + 8); the caller waits (tcgen05.wait::st).
+// This thread's 8 hi values at columns taddr.. and 8 lo values at taddr + 8.. of its TMEM
+// lane; the caller waits for the stores (tcgen05.wait::st).
 __device__ __forceinline__ void tmem_st8x2(unsigned taddr, const float4& h0, const float4& h1, const float4& l0,
                                            const float4& l1) {
   asm volatile(
