@@ -74,3 +74,19 @@ def test_packed_transforms_oracle_roundtrip():
     v = so.synthesis_packed(cfg, q)
     assert v.shape == (16 * cfg.nlon,)
     assert np.allclose(so.analysis_packed(cfg, v), q, rtol=0, atol=1e-12)
+
+
+def test_mirror_lm_index_matches_oracle_and_rejects():
+    """The host mirror's LM_index / nlm_calc (no GPU) against the oracle, and the reference's
+    argument errors (src/layout.jl:143-162)."""
+    import pytest
+    import shtb200 as sht
+    for lmax, mmax, mres in ((7, 7, 1), (10, 8, 2), (12, 9, 3)):
+        assert sht.nlm_calc(lmax, mmax, mres) == so.nlm_calc(lmax, mmax, mres)
+        for m in range(0, mmax + 1, mres):
+            for l in range(m, lmax + 1):
+                assert sht.LM_index(lmax, mres, l, m) == so.lm_index(lmax, mres, l, m)
+    assert sht.nlm_calc(3, 5, 1) == 0
+    for bad in ((4, 2, 3, 1), (4, 1, 1, 2), (4, 1, 5, 1), (4, 1, -1, -1)):
+        with pytest.raises(sht.ArgumentError):
+            sht.LM_index(*bad)
