@@ -30,20 +30,35 @@
 // short chunks keep that bias below 1e-6 relative at any lmax.
 // Every mbarrier wait is bounded (2 s of %globaltimer); a timeout sets the
 // plan's error word and the CTA drains and exits.
+#include <cuda_fp16.h>
+
 #include <climits>
 #include <cstring>
 
 #include "kernels.cuh"
+
+#ifndef SHTB_MIXED_F16
+#define SHTB_MIXED_F16 1
+#endif
 
 namespace shtb {
 namespace mx {
 
 constexpr int kM = 128;          // UMMA M
 constexpr int kK = 8;            // TF32 K per instruction
-constexpr int kChunk = 4;          // K-steps accumulated in TMEM before promotion
+#ifndef SHTB_F16_CHUNK
+#define SHTB_F16_CHUNK 8
+#endif
+#ifndef SHTB_PROMO_FULLWAIT
+#define SHTB_PROMO_FULLWAIT 1
+#endif
 constexpr int kThreads = 576;       // 8 splitter warps, 1 MMA warp, 8 promotion warps, 1 loader warp
 constexpr int kTileBytesA = kM * kK * 4;  // 4 KB
 constexpr unsigned long long kWaitNs = 2000000000ull;
+constexpr bool kF16 = SHTB_MIXED_F16 != 0;   // fp16x3 (kind::f16, K = 16) instead of 3xTF32
+constexpr int kChunk = kF16 ? SHTB_F16_CHUNK : 4;   // FP32 K-steps accumulated in TMEM before promotion
+constexpr int kScR = 16;                      // ring of per-chunk B column scales (fp16x3)
+constexpr int kSegRows = kF16 ? 16 : 8;       // table segment padding (degrees)
 
 struct Args {
   PlanDev P;
@@ -157,6 +172,73 @@ __device__ __forceinline__ void tmem_st8x2(unsigned taddr, const float4& h0, con
       : "memory");
 }
 
+template <int N>
+__device__ __forceinline__ unsigned idesc_f16() {
+  // F32 accumulate, A/B F16, both K-major, N>>3 at bit 17, M>>4 at bit 24
+  return (1u << 4) | ((unsigned)(N >> 3) << 17) | ((unsigned)(kM >> 4) << 24);
+}
+
+// A from TMEM (M = 128 lanes x 8 columns of f16 pairs: K = 16), B from shared memory.
+__device__ __forceinline__ void mma_f16_ts(unsigned tmem_d, unsigned tmem_a, unsigned long long b, unsigned idesc,
+                                           unsigned accum) {
+  const unsigned z = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+      :
+      : "r"(tmem_d), "r"(tmem_a), "l"(b), "r"(idesc), "r"(accum), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+
+// A and B from shared memory (K = 16).
+__device__ __forceinline__ void mma_f16_ss(unsigned tmem_d, unsigned long long a, unsigned long long b, unsigned idesc,
+                                           unsigned accum) {
+  const unsigned z = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+      :
+      : "r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(accum), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+
+// This thread's 8 hi words at columns taddr.. and 8 lo words at taddr + 8.. of its TMEM
+// lane; the caller waits for the stores (tcgen05.wait::st).
+__device__ __forceinline__ void tmem_st8x2u(unsigned taddr, const unsigned* h, const unsigned* l) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%2, %3, %4, %5, %6, %7, %8, %9};\n\t"
+      "tcgen05.st.sync.aligned.32x32b.x8.b32 [%1], {%10, %11, %12, %13, %14, %15, %16, %17};" ::"r"(taddr),
+      "r"(taddr + 8), "r"(h[0]), "r"(h[1]), "r"(h[2]), "r"(h[3]), "r"(h[4]), "r"(h[5]), "r"(h[6]), "r"(h[7]),
+      "r"(l[0]), "r"(l[1]), "r"(l[2]), "r"(l[3]), "r"(l[4]), "r"(l[5]), "r"(l[6]), "r"(l[7])
+      : "memory");
+}
+
+__device__ __forceinline__ unsigned h2_bits(__half2 h) {
+  unsigned u;
+  memcpy(&u, &h, 4);
+  return u;
+}
+
+// (a, b) = hi + lo as f16 pairs (a in the low half): hi rounded to nearest, lo the
+// remainders (exact in FP32) rounded to nearest.
+__device__ __forceinline__ void split_h2(float a, float b, unsigned& hi, unsigned& lo) {
+  const __half2 h = __floats2half2_rn(a, b);
+  const float2 hf = __half22float2(h);
+  hi = h2_bits(h);
+  lo = h2_bits(__floats2half2_rn(a - hf.x, b - hf.y));
+}
+
+// fp16x3: the table holds P * 2^s with s the largest exponent <= 14 such that
+// 2^s sqrt(2 (2L + 1) / (4 pi)) <= 2^15, L = lmax + 1. |P_l^m| <= sqrt((2l + 1) / (4 pi)),
+// so every scaled value and its f16 hi part stay below 2^15 (f16 maximum 65504) with a
+// factor sqrt(2) to spare.
+__device__ __forceinline__ int f16_table_exp(int lmax) {
+  const long long q = 2LL * (lmax + 1) + 1;
+  int s = 14;
+  while (s > 0 && (q << (2 * s)) > 6746518852LL) --s;   // floor(2^31 pi)
+  return s;
+}
+
 __device__ __forceinline__ void mma_commit(unsigned long long* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                : "memory");
@@ -232,29 +314,35 @@ __device__ __forceinline__ float coef_factor(const Args& a, int l, int m) {
 template <int N>
 struct Smem {
   static constexpr int kTileB = N * kK * 4;
-  // One stage holds a chunk: kChunk K-steps of A as loaded (FP32), then of B_hi and B_lo
-  // (one parity class per CTA), each operand filled by one bulk copy; the split A tiles
-  // live in TMEM.
+  // One stage holds a chunk: kChunk K-steps of A as loaded (FP32), then of B (one parity
+  // class per CTA), each operand filled by one bulk copy; the split A tiles live in TMEM.
+  // 3xTF32 splits B into the B_hi place and a B_lo area after it; fp16x3 converts each
+  // pair of FP32 B tiles in place into an f16 hi tile and an f16 lo tile of the same size.
   static constexpr int kStageA = kChunk * kTileBytesA;
-  static constexpr int kStage = kChunk * (kTileBytesA + 2 * kTileB);
-  // Ring depth: 192 KB of stages per CTA (80 KB for the two 16-column CTAs of an SM),
-  // 16 per-chunk split barriers and 16 TMEM slots for the split A tiles.
-  static constexpr int kSt = (N == 128) ? 4 : (N == 64) ? 6 : (N == 32) ? 8 : 4;
+  static constexpr int kStage = kChunk * (kTileBytesA + (kF16 ? 1 : 2) * kTileB);
+  // Ring depth: up to 192 KB of stages per CTA (92 KB for each of the two 16-column CTAs
+  // of an SM), 16 per-chunk split barriers and 16 TMEM slots for the split A tiles.
+  static constexpr int kSt = ((N == 16) ? 94208 : 196608) / kStage < 14 ? ((N == 16) ? 94208 : 196608) / kStage : 14;
   static constexpr int kFull = 16;   // per-chunk split barriers
   static constexpr int kStA = (N == 16) ? 8 : 16;   // two 16-column CTAs share an SM's TMEM
-  static constexpr int kSlotCh = kStA / kChunk;     // chunks whose split A tiles TMEM holds
+  static constexpr int kSlotCols = 16 * (kF16 ? kChunk / 2 : kChunk);   // TMEM columns of a chunk's A slots
+  static constexpr int kSlotCh = 16 * kStA / kSlotCols;                   // chunks whose split A tiles TMEM holds
   static constexpr int kRel = 16;   // chunk-release barriers (>= kSt and kStA, see the tile roles below)
   static constexpr int kBar = kSt * kStage;
-  // barriers: full[kFull], ldfull[kSt], rel[kRel], acce[2]; then TMEM slot, abort flag
-  static constexpr int kBytes = kBar + (kFull + kSt + kRel + 2) * 8 + 16;
+  // barriers: full[kFull], ldfull[kSt], rel[kRel], acce[2]; then TMEM slot, abort flag;
+  // fp16x3 then keeps the FP32 column scales of the last kScR chunks
+  static constexpr int kScOff = (kBar + (kFull + kSt + kRel + 2) * 8 + 16 + 15) & ~15;
+  static constexpr int kBytes = kF16 ? kScOff + kScR * N * 4 : kBar + (kFull + kSt + kRel + 2) * 8 + 16;
   // TMEM: chunk accumulators H0 [0, N) and H1 [N, 2N); A slot s: hi at 2N + 16 s, lo at
-  // 2N + 16 s + 8; K-step s of chunk gc uses slot (gc % kSlotCh) kChunk + s
+  // 2N + 16 s + 8, one slot per K-step (3xTF32) or f16 K-step (fp16x3); the slots of
+  // chunk gc start at column 2N + kSlotCols (gc % kSlotCh)
   static constexpr int kTmemA = 2 * N;
-  static constexpr int kTmemNeed = 2 * N + 16 * kStA;
+  static constexpr int kTmemNeed = kF16 ? 2 * N : 2 * N + 16 * kStA;   // fp16x3 reads A from shared memory
   static constexpr int kTmemCols = kTmemNeed <= 32 ? 32 : kTmemNeed <= 64 ? 64 : kTmemNeed <= 128 ? 128
                                    : kTmemNeed <= 256 ? 256 : 512;
   static_assert(kTmemNeed <= 512, "TMEM columns");
   static_assert(kSt <= kRel && kStA <= kRel, "release barriers");
+  static_assert(kSt + 2 <= kScR && kSt + 2 <= kFull, "scale ring: a chunk's scales outlive its promotion");
 };
 
 // Narrow tiles (N = 16: up to 8 fields) leave the tensor core mostly idle, so two CTAs
@@ -273,6 +361,7 @@ struct Bars {
   unsigned long long *full, *ldfull, *rel, *acce;
   unsigned* tmem_slot;
   volatile int* abort_flag;
+  float* fsc;   // fp16x3: [kScR][N] factors 2^-(row scale + table scale) of chunk gc % kScR
 };
 
 template <int N>
@@ -285,6 +374,7 @@ __device__ __forceinline__ Bars gemm_bars(unsigned char* sm) {
   B.acce = B.rel + S::kRel;       // [2] TMEM chunk buffer b drained by the promotion warps
   B.tmem_slot = reinterpret_cast<unsigned*>(B.acce + 2);
   B.abort_flag = reinterpret_cast<volatile int*>(B.tmem_slot + 1);
+  B.fsc = reinterpret_cast<float*>(sm + S::kScOff);
   return B;
 }
 
@@ -402,8 +492,9 @@ __device__ __forceinline__ bool loader_tile(const Args& a, const TileCoord& tc, 
     unsigned char* sa = sm + (size_t)st * S::kStage;
     unsigned char* sb = sa + S::kStageA;
     unsigned long long* bar = &B.ldfull[st];
-    mbar_expect_tx(bar, (unsigned)nk * (abytes + bbytes));
-    bulk_g2s(sa, a0 + (long long)k0 * T.arows * kK, nk * abytes, bar);
+    const int na = kF16 ? (nk + 1) & ~1 : nk;   // fp16x3: A tiles come in hi/lo pairs
+    mbar_expect_tx(bar, (unsigned)na * abytes + (unsigned)nk * bbytes);
+    bulk_g2s(sa, a0 + (long long)k0 * T.arows * kK, na * abytes, bar);
     if (bcontig) {
       bulk_g2s(sb, bsrc + (long long)k0 * nfp * 16, nk * bbytes, bar);
     } else {
@@ -439,7 +530,7 @@ __device__ __forceinline__ bool splitter_tile(const Args& a, const TileInfo& T, 
     // the MMAs that last read these TMEM slots have completed
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     unsigned char* As = sm + (size_t)(gc % S::kSt) * S::kStage;
-    const unsigned slot0 = ta_lane + 16u * (gc % S::kSlotCh) * kChunk;
+    const unsigned slot0 = ta_lane + S::kSlotCols * (gc % S::kSlotCh);
     for (int s = sgp; s < nk; s += 2) {
       const unsigned char* Ah = As + s * astr;
       const float4 x0 = *reinterpret_cast<const float4*>(Ah + o0);
@@ -467,15 +558,96 @@ __device__ __forceinline__ bool splitter_tile(const Args& a, const TileInfo& T, 
   return true;
 }
 
+// fp16x3 splitters. The table already holds A as f16 hi/lo tile pairs (P 2^s, below
+// 2^15): FP32 K-steps 2g and 2g+1 of a chunk form f16 K-step g (K = 16), whose hi tile
+// takes the place of FP32 tile 2g and lo tile that of 2g + 1. The 256 splitter threads
+// convert B the same way, kTpr threads per row: each row of the chunk is scaled by the
+// power of two 2^e that brings its largest magnitude into [2^14, 2^15), split into f16
+// hi + lo and written in place (the same core-matrix byte order: 16-byte rows of 8 f16
+// values). The factor 2^-(e + s) that undoes both scales goes to the chunk's entry of the
+// scale ring. A missing odd K-step at the end of a tile converts as zeros.
+template <int MODE, int N>
+__device__ __forceinline__ bool splitter_tile_f16(const Args& a, const TileInfo& T, unsigned char* sm, const Bars& B,
+                                                  unsigned c0) {
+  using S = Smem<N>;
+  constexpr int kTpr = (256 / N < 8) ? 256 / N : 8;   // threads per B row
+  constexpr int kPieces = 2 * kChunk;                 // 16-byte pieces of a B row per chunk
+  constexpr int kG = (kTpr > 4) ? kTpr / 4 : 1;       // f16 K-steps per conversion pass
+  constexpr int kPp = 4 * kG / kTpr;                  // pieces per thread and pass
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int nrows = (int)(T.bbytes >> 5);             // B rows loaded (2 per field)
+  const int r = tid / kTpr, v = tid % kTpr;
+  const bool rowok = tid < N * kTpr && r < nrows;
+  const int sa = f16_table_exp(a.P.lmax);
+  for (int c = 0; c < T.nch; ++c) {
+    const unsigned gc = c0 + c;
+    const int nk = min(kChunk, T.nks - c * kChunk), nk2 = (nk + 1) >> 1;
+    const bool ok = mbar_wait(&B.ldfull[gc % S::kSt], (gc / S::kSt) & 1, B.abort_flag, a.err);
+    if (!__all_sync(0xffffffffu, ok)) return false;
+    // B row r: piece u = 2 st + khalf of FP32 tile st holds k = 4 u .. 4 u + 3 of the chunk.
+    // Pass 1: the row's largest magnitude (a thread's pieces u = v, v + kTpr, ...).
+    unsigned char* Bs = sm + (size_t)(gc % S::kSt) * S::kStage + S::kStageA;
+    unsigned mx = 0;
+#pragma unroll
+    for (int u = v; u < kPieces; u += kTpr) {
+      if (rowok && (u >> 1) < nk) {
+        const float4 x = *reinterpret_cast<const float4*>(Bs + (u >> 1) * T.bstr + tile_off(r, u & 1));
+        mx = max(mx, max(max(__float_as_uint(x.x) & 0x7fffffffu, __float_as_uint(x.y) & 0x7fffffffu),
+                         max(__float_as_uint(x.z) & 0x7fffffffu, __float_as_uint(x.w) & 0x7fffffffu)));
+      }
+    }
+#pragma unroll
+    for (int o = 1; o < kTpr; o <<= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    // max * 2^e in [2^14, 2^15) (e at most 100: rows below 2^-86 keep the f16 subnormal steps)
+    const int e = min(141 - (int)(mx >> 23), 100);
+    const float su = __int_as_float((e + 127) << 23);
+    // Pass 2, kG f16 K-steps at a time: their pieces are read before any of them is
+    // overwritten (a row's threads share a warp).
+    for (int g0 = 0; 2 * g0 < nk; g0 += kG) {
+      float4 xb[kPp];
+#pragma unroll
+      for (int j = 0; j < kPp; ++j) {
+        const int u = 4 * g0 + v + j * kTpr, st = u >> 1;
+        xb[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (rowok && u < 4 * (g0 + kG) && st < nk)
+          xb[j] = *reinterpret_cast<const float4*>(Bs + st * T.bstr + tile_off(r, u & 1));
+      }
+      __syncwarp();
+      if (rowok) {
+#pragma unroll
+        for (int j = 0; j < kPp; ++j) {
+          const int u = 4 * g0 + v + j * kTpr, st = u >> 1;
+          if (u < 4 * (g0 + kG) && st < 2 * nk2) {
+            unsigned h0, l0, h1, l1;
+            split_h2(xb[j].x * su, xb[j].y * su, h0, l0);
+            split_h2(xb[j].z * su, xb[j].w * su, h1, l1);
+            unsigned char* d = Bs + (st & ~1) * T.bstr + tile_off(r, st & 1) + (u & 1) * 8;
+            *reinterpret_cast<uint2*>(d) = make_uint2(h0, h1);
+            *reinterpret_cast<uint2*>(d + T.bstr) = make_uint2(l0, l1);
+          }
+        }
+      }
+      __syncwarp();
+    }
+    if (rowok && v == 0) B.fsc[(gc % kScR) * N + r] = __int_as_float((127 - e - sa) << 23);
+    // the B tiles written here are read by the MMAs (async proxy)
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncwarp();
+    if (lane == 0) mbar_arrive_cnt(&B.full[gc % S::kFull], 2);
+  }
+  return true;
+}
+
 // One thread issues the MMAs, a chunk at a time, and commits once per chunk.
 template <int MODE, int N>
 __device__ __forceinline__ bool mma_tile(const Args& a, const TileInfo& T, unsigned char* sm, const Bars& B,
                                          unsigned tmem, unsigned c0) {
   using S = Smem<N>;
-  const unsigned idesc = idesc_tf32<N>();
+  const unsigned idesc = idesc_tf32<N>(), idesc16 = idesc_f16<N>();
   const unsigned long long bh0 = sdesc(sm + S::kStageA), bl0 = sdesc(sm + S::kStageA + kChunk * S::kTileB);
   constexpr unsigned long long kStageDesc = S::kStage >> 4;   // descriptor address step per stage
   const unsigned long long kstepDesc = T.bstr >> 4;          // and per K-step within a stage
+  const unsigned long long a0 = sdesc(sm), akDesc = ((unsigned)T.arows * kK * 4) >> 4;   // A tiles (fp16x3)
   for (int c = 0; c < T.nch; ++c) {
     const unsigned gc = c0 + c;
     const int bb = gc & 1;
@@ -488,16 +660,29 @@ __device__ __forceinline__ bool mma_tile(const Args& a, const TileInfo& T, unsig
     // sum is still small, and the hi*hi products last.
     const unsigned dH = tmem + bb * N;
     const unsigned long long sc = (unsigned long long)(gc % S::kSt) * kStageDesc;
-    const unsigned slot0 = tmem + S::kTmemA + 16u * (gc % S::kSlotCh) * kChunk;
-    for (int ks = k0; ks < k1; ++ks) {
-      const unsigned long long so = sc + (ks - k0) * kstepDesc;
-      const unsigned ah = slot0 + 16u * (ks - k0), al = ah + 8;
-      mma_tf32_ts(dH, ah, bl0 + so, idesc, ks == k0 ? 0u : 1u);
-      mma_tf32_ts(dH, al, bh0 + so, idesc, 1u);
-    }
-    for (int ks = k0; ks < k1; ++ks) {
-      const unsigned long long so = sc + (ks - k0) * kstepDesc;
-      mma_tf32_ts(dH, slot0 + 16u * (ks - k0), bh0 + so, idesc, 1u);
+    const unsigned slot0 = tmem + S::kTmemA + S::kSlotCols * (gc % S::kSlotCh);
+    if constexpr (kF16) {
+      // f16 K-step g: A and B hi over FP32 tile 2g, lo over tile 2g + 1, both in the stage
+      const int nk2 = (k1 - k0 + 1) >> 1;
+      const unsigned long long ast = a0 + sc;
+      for (int g = 0; g < nk2; ++g) {
+        const unsigned long long ah = ast + 2 * g * akDesc, bh = bh0 + sc + 2 * g * kstepDesc;
+        mma_f16_ss(dH, ah, bh + kstepDesc, idesc16, g == 0 ? 0u : 1u);
+        mma_f16_ss(dH, ah + akDesc, bh, idesc16, 1u);
+      }
+      for (int g = 0; g < nk2; ++g)
+        mma_f16_ss(dH, ast + 2 * g * akDesc, bh0 + sc + 2 * g * kstepDesc, idesc16, 1u);
+    } else {
+      for (int ks = k0; ks < k1; ++ks) {
+        const unsigned long long so = sc + (ks - k0) * kstepDesc;
+        const unsigned ah = slot0 + 16u * (ks - k0), al = ah + 8;
+        mma_tf32_ts(dH, ah, bl0 + so, idesc, ks == k0 ? 0u : 1u);
+        mma_tf32_ts(dH, al, bh0 + so, idesc, 1u);
+      }
+      for (int ks = k0; ks < k1; ++ks) {
+        const unsigned long long so = sc + (ks - k0) * kstepDesc;
+        mma_tf32_ts(dH, slot0 + 16u * (ks - k0), bh0 + so, idesc, 1u);
+      }
     }
     mma_commit(&B.rel[gc % S::kRel]);
   }
@@ -524,16 +709,31 @@ __device__ __forceinline__ bool promo_tile(const Args& a, const TileCoord& tc, c
   for (int c = 0; c < T.nch; ++c) {
     const unsigned gc = c0 + c;
     const int bb = gc & 1;
+    // fp16x3: the chunk's column scales, written by the splitters before they arrived on
+    // full (complete long before the chunk's MMAs are)
+    if (kF16 && SHTB_PROMO_FULLWAIT && ok) ok = mbar_wait(&B.full[gc % S::kFull], (gc / S::kFull) & 1, B.abort_flag, a.err);
     if (ok) ok = mbar_wait(&B.rel[gc % S::kRel], (gc / S::kRel) & 1, B.abort_flag, a.err);
     ok = __all_sync(0xffffffffu, ok);   // warp-uniform: the TMEM loads are warp-collective
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const unsigned dH = tmem + lane_base + bb * N + h * (N / 2);
+    const float4* fs = reinterpret_cast<const float4*>(B.fsc + (gc % kScR) * N + h * (N / 2));
 #pragma unroll
     for (int i = 0; i < N / 2; i += kLd) {
       float v[kLd];
       tmem_ld<kLd>(dH + i, v);
+      if constexpr (kF16) {
 #pragma unroll
-      for (int u = 0; u < kLd; ++u) acc[i + u] += v[u];
+        for (int u = 0; u < kLd; u += 4) {
+          const float4 f = fs[(i + u) >> 2];   // exact powers of two: fma rounds once, like the add
+          acc[i + u] = fmaf(v[u], f.x, acc[i + u]);
+          acc[i + u + 1] = fmaf(v[u + 1], f.y, acc[i + u + 1]);
+          acc[i + u + 2] = fmaf(v[u + 2], f.z, acc[i + u + 2]);
+          acc[i + u + 3] = fmaf(v[u + 3], f.w, acc[i + u + 3]);
+        }
+      } else {
+#pragma unroll
+        for (int u = 0; u < kLd; ++u) acc[i + u] += v[u];
+      }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncwarp();
@@ -599,7 +799,7 @@ __device__ __forceinline__ void gemm_tiles(const Src& src, unsigned char* sm, co
     if (loader)
       ok = loader_tile<MODE, N>(a, tc, T, sm, B, c0);
     else if (splitter)
-      ok = splitter_tile<MODE, N>(a, T, sm, B, tmem, c0);
+      ok = kF16 ? splitter_tile_f16<MODE, N>(a, T, sm, B, c0) : splitter_tile<MODE, N>(a, T, sm, B, tmem, c0);
     else if (mma)
       ok = mma_tile<MODE, N>(a, T, sm, B, tmem, c0);
     else
@@ -758,6 +958,7 @@ __global__ void mixed_table_kernel(PlanDev P, float* __restrict__ tabS, float* _
   const int l0 = P.l0[(size_t)im * P.npair + pair];
   const double2 r01 = P.r01[(size_t)im * P.npair + pair];
   const int pt = pair / kM, pr = pair % kM, pk = pair % kK, pks = pair / kK;
+  const float asc = kF16 ? (float)(1 << f16_table_exp(P.lmax)) : 1.f;   // exact scaling
   double ra = 0.0, rb = 0.0;
   for (int l = m; l <= P.lrec; ++l) {
     double r;
@@ -772,13 +973,28 @@ __global__ void mixed_table_kernel(PlanDev P, float* __restrict__ tabS, float* _
     const int par = (l - m) & 1, j = (l - m) >> 1;
     const long long sg = seg[2 * im + par];
     const int R = (int)(seg[2 * im + par + 1] - sg);
-    const float v = (float)(P.cfac[poff + (l - m)] * r);
+    const float v = (float)(P.cfac[poff + (l - m)] * r) * asc;
+    const int jt = j / kM, rr = j % kM, rows = min(kM, R - jt * kM);
+    if constexpr (kF16) {
+      // f16 hi/lo of P 2^s: K-step pair (2g, 2g + 1) of the FP32 layout holds the hi and lo
+      // tiles of f16 K-step g, element k16 of a row at byte tile_off(row, k16 / 8) + 2 (k16 % 8)
+      const __half h = __float2half_rn(v), lo = __float2half_rn(v - __half2float(h));
+      const int js = j % 16, ps = pair % 16;
+      unsigned char* ds = reinterpret_cast<unsigned char*>(tabS + sg * npp) +
+                          ((long long)pt * (R / kK) + 2 * (j / 16)) * kTileBytesA + tile_off(pr, js >> 3) + 2 * (js & 7);
+      unsigned char* da = reinterpret_cast<unsigned char*>(tabA + sg * npp + (long long)jt * kM * npp) +
+                          (long long)(2 * (pair / 16)) * rows * kK * 4 + tile_off(rr, ps >> 3) + 2 * (ps & 7);
+      *reinterpret_cast<__half*>(ds) = h;
+      *reinterpret_cast<__half*>(ds + kTileBytesA) = lo;
+      *reinterpret_cast<__half*>(da) = h;
+      *reinterpret_cast<__half*>(da + rows * kK * 4) = lo;
+      continue;
+    }
     // synthesis: tile (pt, j/8), row pr, K slot j%8
     const int k = j % kK;
     tabS[sg * npp + ((long long)pt * (R / kK) + j / kK) * (kM * kK) + (pr >> 3) * 64 + (k >> 2) * 32 + (pr & 7) * 4 +
          (k & 3)] = v;
     // analysis: tile (j/128, pair/8) of rows = min(128, R - 128 (j/128)), row j%128, K slot pair%8
-    const int jt = j / kM, rr = j % kM, rows = min(kM, R - jt * kM);
     tabA[sg * npp + (long long)jt * kM * npp + (long long)pks * rows * kK + (rr >> 3) * 64 + (pk >> 2) * 32 +
          (rr & 7) * 4 + (pk & 3)] = v;
   }
@@ -789,7 +1005,8 @@ __global__ void mixed_table_kernel(PlanDev P, float* __restrict__ tabS, float* _
 using namespace mx;
 
 // Segment starts of the P table: rows (degrees m+par, m+par+2, .., lrec) of every
-// (order, parity), each segment padded to a multiple of 8 rows. Returns the row count.
+// (order, parity), each segment padded to a multiple of kSegRows rows (one f16 K-step of
+// 16 degrees, or one TF32 K-step of 8). Returns the row count.
 static long long table_segments(const shtb_plan* p, std::vector<long long>* seg) {
   const int nm = p->nm, LR = p->lrec;
   if (seg) seg->assign(2 * nm + 1, 0);
@@ -799,7 +1016,7 @@ static long long table_segments(const shtb_plan* p, std::vector<long long>* seg)
     for (int par = 0; par < 2; ++par) {
       if (seg) (*seg)[2 * im + par] = rows;
       const int cnt = (LR - m - par >= 0) ? (LR - m - par) / 2 + 1 : 0;
-      rows += (cnt + kK - 1) / kK * kK;
+      rows += (cnt + kSegRows - 1) / kSegRows * kSegRows;
     }
   }
   if (seg) (*seg)[2 * nm] = rows;
