@@ -131,7 +131,7 @@ static int group_launch_stages(shtb_group* g, int op, cudaStream_t st) {
     group_start_kernel<<<1, 256, 0, st>>>(g->d_done, g->n, g->d_t0);
     count_launch();
     SHTB_TRY_CUDA(cudaGetLastError(), "group start marker");
-    if ((rc = launch_pack_group(g->d_args_syn, g->d_items_pack, g->n_pack, std::min(g->n_pack, 8 * g->nsm), st)))
+    if ((rc = launch_pack_group(g->d_args_syn, g->d_items_pack, g->n_pack, std::min(g->n_pack, 24 * g->nsm), st)))
       return rc;
     if ((rc = launch_gemm_group(0, g->d_args_syn, g->d_items_syn, g->n_syn, g->gemm_ctas_syn, nullptr, st))) return rc;
     if ((rc = launch_fft_group_f32(1, g->fft_h, g->generic, g->d_jobs_syn, g->d_items_fft, g->n_fft, g->fft_ctas,

@@ -70,17 +70,13 @@ struct FFTDesc {
   unsigned mspan[24];      // the same for the group span Ns / rad[s]
 };
 
-// Round to the nearest TF32 value, ties away from zero: add half a TF32 ulp to the
-// magnitude bits and clear the 13 low mantissa bits (finite inputs).
-__device__ __forceinline__ float tf32_round(float x) {
-  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
-}
-
-// B operand tile images (FP32) of the mixed-precision GEMMs: one region of nfp x 16 floats per
+// B operand tile images of the mixed-precision GEMMs: one region of nfp x 16 floats per
 // K-step (nfp = fields rounded up to 4, so tiles have whole 8-row core-matrix groups);
 // fields in blocks of 64 (1024 floats), block rows 2f (real) and 2f+1 (imaginary) in the
 // K-major no-swizzle core-matrix order, 8 K values per row. btile_off gives the float
-// offset of (row, K slot kk) inside a block.
+// offset of (row, K slot kk) inside a block. The analysis images hold FP32 values (from the
+// FFT); the synthesis images hold f16 hi/lo tile pairs in the same bytes (16 K values per
+// row and region, hi in even regions, lo in odd ones).
 __host__ __device__ inline int btile_nfp(int nf) { return (nf + 3) & ~3; }
 __host__ __device__ inline int btile_off(int row, int kk) {
   return (row >> 3) * 64 + (kk >> 2) * 32 + (row & 7) * 4 + (kk & 3);

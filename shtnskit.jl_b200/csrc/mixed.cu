@@ -3,31 +3,34 @@
 // Per order m both directions are dense GEMMs over one parity class of degrees:
 //   synthesis  E[pair, col] = sum_j  P[m+2j,   pair] * a[m+2j,   col]    (O: degrees m+2j+1)
 //   analysis   a[m+2j, col] = sum_pair P[m+2j, pair] * E[pair, col]      (O likewise)
-// with col = (field, re|im). Each GEMM runs as tcgen05.mma kind::tf32 with FP32
-// accumulation in TMEM, using the 3xTF32 split x = hi + lo (both rounded to
-// nearest TF32): x*y ~ hi_x hi_y + hi_x lo_y + lo_x hi_y.
+// with col = (field, re|im). Each GEMM runs as tcgen05.mma kind::f16 (K = 16, A and B f16)
+// with FP32 accumulation in TMEM, on the split x = hi + lo of both operands into f16
+// values (hi rounded to nearest, lo = the rounded remainder: 22 significant bits):
+// x*y ~ hi_x hi_y + hi_x lo_y + lo_x hi_y. f16 has 5 exponent bits, so both operands are
+// scaled by powers of two first: P by 2^s for the whole plan (its largest values near
+// 2^15), B per row by 2^e so that the row's largest magnitude lies in [2^14, 2^15) (per
+// segment in the synthesis, per chunk in the analysis); the promotion undoes both exactly.
 //
-// P comes from a per-plan FP32 table of P_l^m(x_pair), l = m..lmax+1, grouped by
-// (m, parity) into segments of R rows (degrees, padded to a multiple of 8) by npp
-// latitude pairs (padded to a multiple of 128). The table is written once by
-// mixed_table_kernel from the FP64 recurrence (extended-range seeds and FP64
-// recurrence coefficients), so every P value is the FP64 result rounded once. It is
-// stored twice, as the byte images of the A tiles the two GEMMs load, so one bulk
-// copy (cp.async.bulk, completing on an mbarrier) fills a stage's A tile: synthesis
-// tiles are 128 pairs x 8 degrees, analysis tiles 128 degrees x 8 pairs, both in the
-// K-major no-swizzle core-matrix order of the MMA descriptors.
+// P comes from a per-plan table of P_l^m(x_pair), l = m..lmax+1, grouped by (m, parity)
+// into segments of R rows (degrees, padded to a multiple of 16) by npp latitude pairs
+// (padded to a multiple of 128). mixed_table_kernel writes it once from the FP64
+// recurrence (extended-range seeds and FP64 recurrence coefficients), rounded once to
+// FP32, scaled and split into f16 hi/lo. It is stored twice, as the byte images of the A
+// tiles the two GEMMs load (synthesis 128 pairs x 16 degrees, analysis 128 degrees x 16
+// pairs; hi and lo tiles of 4 KB each in the K-major no-swizzle core-matrix order), so one
+// bulk copy (cp.async.bulk, completing on an mbarrier) fills a stage's A operand. The
+// synthesis B images (coefficients) arrive split the same way from mixed_pack_kernel; the
+// analysis B images (Fourier coefficients) arrive in FP32 from the FFT and are split in
+// shared memory.
 //
-// CTA organisation (576 threads, one parity class per CTA): one thread of warp 17 fills
-// a 16-stage shared-memory ring, 16 K-steps ahead, with bulk copies of the FP32 A tile
-// image and the pre-split (TF32 hi, lo) B tile images; warps 0-7, in two groups taking
-// alternate K-steps, split each A tile into TF32 hi/lo and store it into one of 16 TMEM
-// slots (8 for 16-column tiles); warp 8 allocates TMEM and one of its threads issues the
-// MMAs (A from TMEM, B from shared memory), one commit per chunk of kChunk K-steps
-// releasing that chunk's stages and slots. The tensor core accumulates the three
-// products of a chunk into one of two TMEM buffers; warps 9-16 drain each finished
-// chunk with tcgen05.ld into round-to-nearest FP32 register sums. Long accumulation
-// chains inside the tensor core round toward zero and would bias sums of many terms;
-// short chunks keep that bias below 1e-6 relative at any lmax.
+// CTA organisation (576 threads, one parity class per CTA): one thread of warp 17 fills a
+// shared-memory ring of chunk stages (8 image K-steps of A and B each) with bulk copies;
+// in the analysis, warps 0-7 split each chunk's B tiles in place; one thread of warp 8
+// (which allocates TMEM) issues the MMAs from shared memory, 12 per chunk, into one of 4
+// TMEM accumulators and commits once per chunk; warps 9-16 drain each finished chunk with
+// tcgen05.ld into round-to-nearest FP32 register sums. Long accumulation chains inside
+// the tensor core round toward zero and would bias sums of many terms; short chunks keep
+// that bias below 1e-6 relative at any lmax.
 // Every mbarrier wait is bounded (2 s of %globaltimer); a timeout sets the
 // plan's error word and the CTA drains and exits.
 #include <cuda_fp16.h>
@@ -37,28 +40,21 @@
 
 #include "kernels.cuh"
 
-#ifndef SHTB_MIXED_F16
-#define SHTB_MIXED_F16 1
-#endif
-
 namespace shtb {
 namespace mx {
 
 constexpr int kM = 128;          // UMMA M
-constexpr int kK = 8;            // TF32 K per instruction
-#ifndef SHTB_F16_CHUNK
-#define SHTB_F16_CHUNK 8
-#endif
-#ifndef SHTB_PROMO_FULLWAIT
-#define SHTB_PROMO_FULLWAIT 1
-#endif
-constexpr int kThreads = 576;       // 8 splitter warps, 1 MMA warp, 8 promotion warps, 1 loader warp
+constexpr int kK = 8;            // K-step of the FP32 tile images (8 x 4 bytes = 16 f16 values)
 constexpr int kTileBytesA = kM * kK * 4;  // 4 KB
 constexpr unsigned long long kWaitNs = 2000000000ull;
-constexpr bool kF16 = SHTB_MIXED_F16 != 0;   // fp16x3 (kind::f16, K = 16) instead of 3xTF32
-constexpr int kChunk = kF16 ? SHTB_F16_CHUNK : 4;   // FP32 K-steps accumulated in TMEM before promotion
-constexpr int kScR = 16;                      // ring of per-chunk B column scales (fp16x3)
-constexpr int kSegRows = kF16 ? 16 : 8;       // table segment padding (degrees)
+constexpr int kChunk = 8;        // image K-steps (4 f16 K-steps, 12 MMAs) accumulated before promotion
+constexpr int kScR = 16;         // ring of per-chunk B column scales
+constexpr int kSegRows = 16;     // table segment padding (degrees): one f16 K-step
+// Warp roles: splitters [0, kSW), MMA issuer kSW, promotion [kSW + 1, kSW + 9), loader kSW + 9.
+constexpr int kSW = 8;
+constexpr int kMmaWarp = kSW, kPromo0 = kSW + 1, kLoaderWarp = kSW + 9;
+constexpr int kThreads = 32 * (kSW + 10);
+constexpr int kAcc = 4;          // TMEM chunk accumulators
 
 struct Args {
   PlanDev P;
@@ -66,8 +62,10 @@ struct Args {
   const long long* seg;      // [2*nm+1] first table row of segment (im, parity); rows hold npp pairs
   int npp;
   const float2* cin;         // synthesis: coefficients (input of the B packing)
-  float* bimg;               // B tile images, FP32 (synthesis: packed coefficients, analysis:
-                             //   written by the FFT); split into TF32 hi/lo in shared memory
+  float* bimg;               // B tile images: synthesis f16 hi/lo pairs written by the packing,
+                             //   analysis FP32 written by the FFT (converted in shared memory)
+  float* bsc;                // synthesis: factor 2^-(e + s) of each (segment, B row) undoing the
+                             //   f16 scaling ([2 nm][2 nfp])
   float2* Wout;              // synthesis: Fourier buffer
   float2* cout;              // analysis: coefficients
   long long ld_k;            // coefficient field stride (complex elements)
@@ -140,54 +138,9 @@ __device__ __forceinline__ unsigned long long sdesc(const void* p) {
 }
 
 template <int N>
-__device__ __forceinline__ unsigned idesc_tf32() {
-  // F32 accumulate, A/B TF32, both K-major, N>>3 at bit 17, M>>4 at bit 24
-  return (1u << 4) | (2u << 7) | (2u << 10) | ((unsigned)(N >> 3) << 17) | ((unsigned)(kM >> 4) << 24);
-}
-
-// A from TMEM (M = 128 lanes x 8 columns of TF32), B from shared memory.
-__device__ __forceinline__ void mma_tf32_ts(unsigned tmem_d, unsigned tmem_a, unsigned long long b, unsigned idesc,
-                                            unsigned accum) {
-  const unsigned z = 0;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-      :
-      : "r"(tmem_d), "r"(tmem_a), "l"(b), "r"(idesc), "r"(accum), "r"(z), "r"(z), "r"(z), "r"(z));
-}
-
-// This thread's 8 hi values at columns taddr.. and 8 lo values at taddr + 8.. of its TMEM
-// lane; the caller waits for the stores (tcgen05.wait::st).
-__device__ __forceinline__ void tmem_st8x2(unsigned taddr, const float4& h0, const float4& h1, const float4& l0,
-                                           const float4& l1) {
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%2, %3, %4, %5, %6, %7, %8, %9};\n\t"
-      "tcgen05.st.sync.aligned.32x32b.x8.b32 [%1], {%10, %11, %12, %13, %14, %15, %16, %17};" ::"r"(taddr),
-      "r"(taddr + 8), "r"(__float_as_uint(h0.x)), "r"(__float_as_uint(h0.y)), "r"(__float_as_uint(h0.z)),
-      "r"(__float_as_uint(h0.w)), "r"(__float_as_uint(h1.x)), "r"(__float_as_uint(h1.y)), "r"(__float_as_uint(h1.z)),
-      "r"(__float_as_uint(h1.w)), "r"(__float_as_uint(l0.x)), "r"(__float_as_uint(l0.y)), "r"(__float_as_uint(l0.z)),
-      "r"(__float_as_uint(l0.w)), "r"(__float_as_uint(l1.x)), "r"(__float_as_uint(l1.y)), "r"(__float_as_uint(l1.z)),
-      "r"(__float_as_uint(l1.w))
-      : "memory");
-}
-
-template <int N>
 __device__ __forceinline__ unsigned idesc_f16() {
   // F32 accumulate, A/B F16, both K-major, N>>3 at bit 17, M>>4 at bit 24
   return (1u << 4) | ((unsigned)(N >> 3) << 17) | ((unsigned)(kM >> 4) << 24);
-}
-
-// A from TMEM (M = 128 lanes x 8 columns of f16 pairs: K = 16), B from shared memory.
-__device__ __forceinline__ void mma_f16_ts(unsigned tmem_d, unsigned tmem_a, unsigned long long b, unsigned idesc,
-                                           unsigned accum) {
-  const unsigned z = 0;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-      :
-      : "r"(tmem_d), "r"(tmem_a), "l"(b), "r"(idesc), "r"(accum), "r"(z), "r"(z), "r"(z), "r"(z));
 }
 
 // A and B from shared memory (K = 16).
@@ -200,17 +153,6 @@ __device__ __forceinline__ void mma_f16_ss(unsigned tmem_d, unsigned long long a
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
       :
       : "r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(accum), "r"(z), "r"(z), "r"(z), "r"(z));
-}
-
-// This thread's 8 hi words at columns taddr.. and 8 lo words at taddr + 8.. of its TMEM
-// lane; the caller waits for the stores (tcgen05.wait::st).
-__device__ __forceinline__ void tmem_st8x2u(unsigned taddr, const unsigned* h, const unsigned* l) {
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%2, %3, %4, %5, %6, %7, %8, %9};\n\t"
-      "tcgen05.st.sync.aligned.32x32b.x8.b32 [%1], {%10, %11, %12, %13, %14, %15, %16, %17};" ::"r"(taddr),
-      "r"(taddr + 8), "r"(h[0]), "r"(h[1]), "r"(h[2]), "r"(h[3]), "r"(h[4]), "r"(h[5]), "r"(h[6]), "r"(h[7]),
-      "r"(l[0]), "r"(l[1]), "r"(l[2]), "r"(l[3]), "r"(l[4]), "r"(l[5]), "r"(l[6]), "r"(l[7])
-      : "memory");
 }
 
 __device__ __forceinline__ unsigned h2_bits(__half2 h) {
@@ -296,12 +238,6 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
                : "memory");
 }
 
-// x = hi + lo with hi = tf32(x) and lo = tf32(x - hi) (x - hi is exact in FP32).
-__device__ __forceinline__ void split4(const float4& x, float4& h, float4& l) {
-  h.x = tf32_round(x.x); h.y = tf32_round(x.y); h.z = tf32_round(x.z); h.w = tf32_round(x.w);
-  l.x = tf32_round(x.x - h.x); l.y = tf32_round(x.y - h.y); l.z = tf32_round(x.z - h.z); l.w = tf32_round(x.w - h.w);
-}
-
 __device__ __forceinline__ float coef_factor(const Args& a, int l, int m) {
   double s = (m == 0) ? (double)a.mf0 : (double)a.mf1;
   if (a.sc_mode) {
@@ -314,35 +250,31 @@ __device__ __forceinline__ float coef_factor(const Args& a, int l, int m) {
 template <int N>
 struct Smem {
   static constexpr int kTileB = N * kK * 4;
-  // One stage holds a chunk: kChunk K-steps of A as loaded (FP32), then of B (one parity
-  // class per CTA), each operand filled by one bulk copy; the split A tiles live in TMEM.
-  // 3xTF32 splits B into the B_hi place and a B_lo area after it; fp16x3 converts each
-  // pair of FP32 B tiles in place into an f16 hi tile and an f16 lo tile of the same size.
+  // One stage holds a chunk: kChunk image K-steps of A, then of B (one parity class per
+  // CTA), each operand filled by one bulk copy. Image K-steps 2g and 2g + 1 hold the f16
+  // hi and lo tiles of f16 K-step g (the analysis converts its FP32 B tiles in place).
   static constexpr int kStageA = kChunk * kTileBytesA;
-  static constexpr int kStage = kChunk * (kTileBytesA + (kF16 ? 1 : 2) * kTileB);
+  static constexpr int kStage = kChunk * (kTileBytesA + kTileB);
   // Ring depth: up to 192 KB of stages per CTA (92 KB for each of the two 16-column CTAs
-  // of an SM), 16 per-chunk split barriers and 16 TMEM slots for the split A tiles.
+  // of an SM).
   static constexpr int kSt = ((N == 16) ? 94208 : 196608) / kStage < 14 ? ((N == 16) ? 94208 : 196608) / kStage : 14;
-  static constexpr int kFull = 16;   // per-chunk split barriers
-  static constexpr int kStA = (N == 16) ? 8 : 16;   // two 16-column CTAs share an SM's TMEM
-  static constexpr int kSlotCols = 16 * (kF16 ? kChunk / 2 : kChunk);   // TMEM columns of a chunk's A slots
-  static constexpr int kSlotCh = 16 * kStA / kSlotCols;                   // chunks whose split A tiles TMEM holds
-  static constexpr int kRel = 16;   // chunk-release barriers (>= kSt and kStA, see the tile roles below)
+  static constexpr int kFull = 16;   // per-chunk conversion barriers (analysis)
+  static constexpr int kRel = 16;    // chunk-release barriers
   static constexpr int kBar = kSt * kStage;
-  // barriers: full[kFull], ldfull[kSt], rel[kRel], acce[2]; then TMEM slot, abort flag;
-  // fp16x3 then keeps the FP32 column scales of the last kScR chunks
-  static constexpr int kScOff = (kBar + (kFull + kSt + kRel + 2) * 8 + 16 + 15) & ~15;
-  static constexpr int kBytes = kF16 ? kScOff + kScR * N * 4 : kBar + (kFull + kSt + kRel + 2) * 8 + 16;
-  // TMEM: chunk accumulators H0 [0, N) and H1 [N, 2N); A slot s: hi at 2N + 16 s, lo at
-  // 2N + 16 s + 8, one slot per K-step (3xTF32) or f16 K-step (fp16x3); the slots of
-  // chunk gc start at column 2N + kSlotCols (gc % kSlotCh)
-  static constexpr int kTmemA = 2 * N;
-  static constexpr int kTmemNeed = kF16 ? 2 * N : 2 * N + 16 * kStA;   // fp16x3 reads A from shared memory
+  // barriers: full[kFull], ldfull[kSt], rel[kRel], acce[kAcc]; then TMEM slot, abort flag;
+  // then the FP32 column scales of the last kScR chunks (analysis)
+  static constexpr int kScOff = (kBar + (kFull + kSt + kRel + kAcc) * 8 + 16 + 15) & ~15;
+  static constexpr int kBytes = kScOff + kScR * N * 4;
+  // TMEM: chunk accumulator b at columns [b N, (b + 1) N), b < kAcc
+  static constexpr int kTmemNeed = kAcc * N;
   static constexpr int kTmemCols = kTmemNeed <= 32 ? 32 : kTmemNeed <= 64 ? 64 : kTmemNeed <= 128 ? 128
                                    : kTmemNeed <= 256 ? 256 : 512;
   static_assert(kTmemNeed <= 512, "TMEM columns");
-  static_assert(kSt <= kRel && kStA <= kRel, "release barriers");
-  static_assert(kSt + 2 <= kScR && kSt + 2 <= kFull, "scale ring: a chunk's scales outlive its promotion");
+  static_assert(kSt <= kRel, "release barriers");
+  // a phase of full, rel or the scale ring is reused only after the promotion of the
+  // chunk kFull (kRel, kScR) earlier: the loader runs at most kSt chunks ahead of the
+  // MMAs, which run at most kAcc chunks ahead of the promotion
+  static_assert(kSt + kAcc <= kScR && kSt + kAcc <= kFull && kSt + kAcc <= kRel, "barrier and scale rings");
 };
 
 // Narrow tiles (N = 16: up to 8 fields) leave the tensor core mostly idle, so two CTAs
@@ -371,8 +303,8 @@ __device__ __forceinline__ Bars gemm_bars(unsigned char* sm) {
   B.full = reinterpret_cast<unsigned long long*>(sm + S::kBar);   // [kFull] chunk gc split (A in TMEM)
   B.ldfull = B.full + S::kFull;   // [kSt] bulk copies of the stage landed
   B.rel = B.ldfull + S::kSt;      // [kRel] MMAs of chunk q done (q % kRel)
-  B.acce = B.rel + S::kRel;       // [2] TMEM chunk buffer b drained by the promotion warps
-  B.tmem_slot = reinterpret_cast<unsigned*>(B.acce + 2);
+  B.acce = B.rel + S::kRel;       // [kAcc] TMEM chunk accumulator b drained by the promotion warps
+  B.tmem_slot = reinterpret_cast<unsigned*>(B.acce + kAcc);
   B.abort_flag = reinterpret_cast<volatile int*>(B.tmem_slot + 1);
   B.fsc = reinterpret_cast<float*>(sm + S::kScOff);
   return B;
@@ -391,15 +323,15 @@ template <int N>
 __device__ __forceinline__ unsigned gemm_cta_setup(const Bars& B) {
   const int tid = threadIdx.x, warp = tid >> 5;
   if (tid == 0) {
-    // two arrivals per splitter warp and chunk (8 warps x 2 = 16)
-    for (int s = 0; s < Smem<N>::kFull; ++s) mbar_init(&B.full[s], 16);
+    // two arrivals per splitter warp and chunk
+    for (int s = 0; s < Smem<N>::kFull; ++s) mbar_init(&B.full[s], 2 * kSW);
     for (int s = 0; s < Smem<N>::kSt; ++s) mbar_init(&B.ldfull[s], 1);
     for (int s = 0; s < Smem<N>::kRel; ++s) mbar_init(&B.rel[s], 1);
-    for (int b = 0; b < 2; ++b) mbar_init(&B.acce[b], 8);   // one arrival per promotion warp
+    for (int b = 0; b < kAcc; ++b) mbar_init(&B.acce[b], 8);   // one arrival per promotion warp
     *B.abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 8) {
+  if (warp == kMmaWarp) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(B.tmem_slot)),
                  "r"(Smem<N>::kTmemCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
@@ -414,7 +346,7 @@ template <int N>
 __device__ __forceinline__ void gemm_cta_teardown(unsigned tmem) {
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if ((threadIdx.x >> 5) == 8) {
+  if ((threadIdx.x >> 5) == kMmaWarp) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Smem<N>::kTmemCols));
   }
@@ -426,17 +358,18 @@ __device__ __forceinline__ void gemm_cta_teardown(unsigned tmem) {
 // each role walks that sequence on its own: the loader and splitters run ahead into the
 // next tile while the promotion warps still drain and store the previous one. c0,
 // counted identically by every role, numbers the chunks of the tiles before the current
-// one and fixes every stage index, TMEM slot and barrier phase.
+// one and fixes every stage index, accumulator and barrier phase.
 //
-// Synchronisation: chunk gc (kChunk K-steps, fewer at the end of a tile) occupies
-// shared-memory stage gc % kSt. The MMA issuer waits for all K-steps of a chunk to be
-// split (one barrier per chunk, full[gc % kFull], which every splitter warp arrives on
-// once per K-step), issues their 3 kChunk MMAs back to back and commits once, to
-// rel[gc % kRel]. Each mbarrier wait costs a few hundred cycles even when the phase has
-// completed, so the MMA issuer waits on two barriers per chunk only.
-// That one barrier releases the chunk's stage (loader), its TMEM A slots (splitters)
-// and its accumulator (promotion warps). kRel >= kSt, kSlotCh keeps a waiter from ever
-// seeing a barrier two phases ahead.
+// Synchronisation: chunk gc (kChunk image K-steps, fewer at the end of a tile) occupies
+// shared-memory stage gc % kSt and TMEM accumulator gc % kAcc. The loader's bulk copies
+// complete on ldfull[gc % kSt]; the analysis splitters convert the chunk's B tiles and
+// arrive on full[gc % kFull]; the MMA issuer waits for one of the two, issues the chunk's
+// 3 (kChunk / 2) MMAs back to back and commits once, to rel[gc % kRel]. Each mbarrier
+// wait costs a few hundred cycles even when the phase has completed, so the MMA issuer
+// waits on two barriers per chunk only. rel releases the chunk's stage (loader) and
+// hands its accumulator to the promotion warps, whose arrival on acce[gc % kAcc] frees
+// it for chunk gc + kAcc. The ring sizes keep every waiter from seeing a barrier two
+// phases ahead.
 struct TileInfo {
   int m, nks, nch;
   long long sg, ln;   // table segment start and rows of (im, par)
@@ -492,85 +425,33 @@ __device__ __forceinline__ bool loader_tile(const Args& a, const TileCoord& tc, 
     unsigned char* sa = sm + (size_t)st * S::kStage;
     unsigned char* sb = sa + S::kStageA;
     unsigned long long* bar = &B.ldfull[st];
-    const int na = kF16 ? (nk + 1) & ~1 : nk;   // fp16x3: A tiles come in hi/lo pairs
-    mbar_expect_tx(bar, (unsigned)na * abytes + (unsigned)nk * bbytes);
+    // A tiles come in hi/lo pairs, and so do the synthesis B tiles (the analysis loads its
+    // FP32 B tiles and treats a missing last odd one as zeros)
+    const int na = (nk + 1) & ~1, nb = (MODE == 0) ? na : nk;
+    mbar_expect_tx(bar, (unsigned)na * abytes + (unsigned)nb * bbytes);
     bulk_g2s(sa, a0 + (long long)k0 * T.arows * kK, na * abytes, bar);
     if (bcontig) {
-      bulk_g2s(sb, bsrc + (long long)k0 * nfp * 16, nk * bbytes, bar);
+      bulk_g2s(sb, bsrc + (long long)k0 * nfp * 16, nb * bbytes, bar);
     } else {
-      for (int s = 0; s < nk; ++s) bulk_g2s(sb + s * S::kTileB, bsrc + (long long)(k0 + s) * nfp * 16, bbytes, bar);
+      for (int s = 0; s < nb; ++s) bulk_g2s(sb + s * S::kTileB, bsrc + (long long)(k0 + s) * nfp * 16, bbytes, bar);
     }
   }
   return true;
 }
 
-// Splitter thread t of group sgp rounds row t of the A tile into TMEM lane t (its warp's
-// quadrant) for the K-steps s = sgp, sgp + 2 of each chunk, and splits those K-steps' B
-// tiles in shared memory (hi in place, lo into the B_lo area). Every splitter warp arrives
-// on the chunk's barrier once with count 2 (its two K-step places), whatever the chunk's
-// length, after waiting for the chunk's stage: that bounds how far it runs ahead.
+// Analysis splitters. The FFT writes B as FP32 tile images; image K-steps 2g and 2g + 1
+// of a chunk form f16 K-step g (K = 16), whose hi tile takes the place of FP32 tile 2g and
+// lo tile that of 2g + 1 (the table holds A in that form already). kTpr threads per row:
+// each row of the chunk is scaled by the power of two 2^e that brings its largest
+// magnitude into [2^14, 2^15), split into f16 hi + lo and written in place (the same
+// core-matrix byte order: 16-byte rows of 8 f16 values). The factor 2^-(e + s) that undoes
+// this and the table's scale 2^s goes to the chunk's entry of the scale ring. A missing odd
+// K-step at the end of a tile converts as zeros.
 template <int MODE, int N>
 __device__ __forceinline__ bool splitter_tile(const Args& a, const TileInfo& T, unsigned char* sm, const Bars& B,
-                                              unsigned tmem, unsigned c0) {
-  using S = Smem<N>;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, t = tid & 127, sgp = warp >> 2;
-  const unsigned ta_lane = tmem + ((unsigned)(32 * (warp & 3)) << 16) + S::kTmemA;
-  const int o0 = tile_off(t, 0), o1 = tile_off(t, 1);
-  const unsigned astr = (unsigned)T.arows * kK * 4;   // A tile image bytes per K-step
-  for (int c = 0; c < T.nch; ++c) {
-    const unsigned gc = c0 + c;
-    const int nk = min(kChunk, T.nks - c * kChunk);
-    bool ok = mbar_wait(&B.ldfull[gc % S::kSt], (gc / S::kSt) & 1, B.abort_flag, a.err);
-    if (ok && sgp < nk && gc >= S::kSlotCh) {
-      const unsigned q = gc - S::kSlotCh;   // the chunk that last used these TMEM slots
-      ok = mbar_wait(&B.rel[q % S::kRel], (q / S::kRel) & 1, B.abort_flag, a.err);
-    }
-    // the warp leaves together (the TMEM stores below are warp-collective)
-    if (!__all_sync(0xffffffffu, ok)) return false;
-    // the MMAs that last read these TMEM slots have completed
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    unsigned char* As = sm + (size_t)(gc % S::kSt) * S::kStage;
-    const unsigned slot0 = ta_lane + S::kSlotCols * (gc % S::kSlotCh);
-    for (int s = sgp; s < nk; s += 2) {
-      const unsigned char* Ah = As + s * astr;
-      const float4 x0 = *reinterpret_cast<const float4*>(Ah + o0);
-      const float4 x1 = *reinterpret_cast<const float4*>(Ah + o1);
-      float4 h, l, h1, l1;
-      split4(x0, h, l);
-      split4(x1, h1, l1);
-      tmem_st8x2(slot0 + 16u * s, h, h1, l, l1);
-      float4* bh = reinterpret_cast<float4*>(As + S::kStageA + s * T.bstr);
-      float4* bl = reinterpret_cast<float4*>(As + S::kStageA + kChunk * S::kTileB + s * T.bstr);
-      for (int i = t; i < (int)(T.bbytes >> 4); i += 128) {
-        float4 bx = bh[i], hb, lb;
-        split4(bx, hb, lb);
-        bh[i] = hb;
-        bl[i] = lb;
-      }
-    }
-    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-    // the B halves written here are read by the MMAs (async proxy)
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncwarp();   // one arrival per warp: 128 arrivals on one word serialize
-    if (lane == 0) mbar_arrive_cnt(&B.full[gc % S::kFull], 2);
-  }
-  return true;
-}
-
-// fp16x3 splitters. The table already holds A as f16 hi/lo tile pairs (P 2^s, below
-// 2^15): FP32 K-steps 2g and 2g+1 of a chunk form f16 K-step g (K = 16), whose hi tile
-// takes the place of FP32 tile 2g and lo tile that of 2g + 1. The 256 splitter threads
-// convert B the same way, kTpr threads per row: each row of the chunk is scaled by the
-// power of two 2^e that brings its largest magnitude into [2^14, 2^15), split into f16
-// hi + lo and written in place (the same core-matrix byte order: 16-byte rows of 8 f16
-// values). The factor 2^-(e + s) that undoes both scales goes to the chunk's entry of the
-// scale ring. A missing odd K-step at the end of a tile converts as zeros.
-template <int MODE, int N>
-__device__ __forceinline__ bool splitter_tile_f16(const Args& a, const TileInfo& T, unsigned char* sm, const Bars& B,
                                                   unsigned c0) {
   using S = Smem<N>;
-  constexpr int kTpr = (256 / N < 8) ? 256 / N : 8;   // threads per B row
+  constexpr int kTpr = (32 * kSW / N < 8) ? 32 * kSW / N : 8;   // threads per B row
   constexpr int kPieces = 2 * kChunk;                 // 16-byte pieces of a B row per chunk
   constexpr int kG = (kTpr > 4) ? kTpr / 4 : 1;       // f16 K-steps per conversion pass
   constexpr int kPp = 4 * kG / kTpr;                  // pieces per thread and pass
@@ -638,59 +519,49 @@ __device__ __forceinline__ bool splitter_tile_f16(const Args& a, const TileInfo&
   return true;
 }
 
-// One thread issues the MMAs, a chunk at a time, and commits once per chunk.
+// One thread issues the MMAs, a chunk at a time, and commits once per chunk. It waits for
+// the chunk's bulk copies (synthesis) or its B conversion (analysis, which follows them).
 template <int MODE, int N>
 __device__ __forceinline__ bool mma_tile(const Args& a, const TileInfo& T, unsigned char* sm, const Bars& B,
                                          unsigned tmem, unsigned c0) {
   using S = Smem<N>;
-  const unsigned idesc = idesc_tf32<N>(), idesc16 = idesc_f16<N>();
-  const unsigned long long bh0 = sdesc(sm + S::kStageA), bl0 = sdesc(sm + S::kStageA + kChunk * S::kTileB);
+  const unsigned idesc = idesc_f16<N>();
   constexpr unsigned long long kStageDesc = S::kStage >> 4;   // descriptor address step per stage
-  const unsigned long long kstepDesc = T.bstr >> 4;          // and per K-step within a stage
-  const unsigned long long a0 = sdesc(sm), akDesc = ((unsigned)T.arows * kK * 4) >> 4;   // A tiles (fp16x3)
+  const unsigned long long a0 = sdesc(sm), b0 = sdesc(sm + S::kStageA);
+  const unsigned long long akDesc = ((unsigned)T.arows * kK * 4) >> 4;   // per image K-step: A
+  const unsigned long long bkDesc = T.bstr >> 4;                         // and B
   for (int c = 0; c < T.nch; ++c) {
     const unsigned gc = c0 + c;
-    const int bb = gc & 1;
-    if (gc >= 2 && !mbar_wait(&B.acce[bb], ((gc >> 1) - 1) & 1, B.abort_flag, a.err)) return false;
+    const int bb = gc % kAcc;
+    if (gc >= kAcc && !mbar_wait(&B.acce[bb], ((gc / kAcc) - 1) & 1, B.abort_flag, a.err)) return false;
     const int k0 = c * kChunk, k1 = min(T.nks, k0 + kChunk);
-    if (!mbar_wait(&B.full[gc % S::kFull], (gc / S::kFull) & 1, B.abort_flag, a.err)) return false;
+    const bool ready = (MODE == 0) ? mbar_wait(&B.ldfull[gc % S::kSt], (gc / S::kSt) & 1, B.abort_flag, a.err)
+                                   : mbar_wait(&B.full[gc % S::kFull], (gc / S::kFull) & 1, B.abort_flag, a.err);
+    if (!ready) return false;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     // The accumulator rounds every addition toward zero at its current magnitude, so
     // the small cross terms (hi*lo, lo*hi) of the whole chunk go in first, while the
-    // sum is still small, and the hi*hi products last.
+    // sum is still small, and the hi*hi products last. f16 K-step g: A and B hi in image
+    // K-step 2g, lo in 2g + 1.
     const unsigned dH = tmem + bb * N;
     const unsigned long long sc = (unsigned long long)(gc % S::kSt) * kStageDesc;
-    const unsigned slot0 = tmem + S::kTmemA + S::kSlotCols * (gc % S::kSlotCh);
-    if constexpr (kF16) {
-      // f16 K-step g: A and B hi over FP32 tile 2g, lo over tile 2g + 1, both in the stage
-      const int nk2 = (k1 - k0 + 1) >> 1;
-      const unsigned long long ast = a0 + sc;
-      for (int g = 0; g < nk2; ++g) {
-        const unsigned long long ah = ast + 2 * g * akDesc, bh = bh0 + sc + 2 * g * kstepDesc;
-        mma_f16_ss(dH, ah, bh + kstepDesc, idesc16, g == 0 ? 0u : 1u);
-        mma_f16_ss(dH, ah + akDesc, bh, idesc16, 1u);
-      }
-      for (int g = 0; g < nk2; ++g)
-        mma_f16_ss(dH, ast + 2 * g * akDesc, bh0 + sc + 2 * g * kstepDesc, idesc16, 1u);
-    } else {
-      for (int ks = k0; ks < k1; ++ks) {
-        const unsigned long long so = sc + (ks - k0) * kstepDesc;
-        const unsigned ah = slot0 + 16u * (ks - k0), al = ah + 8;
-        mma_tf32_ts(dH, ah, bl0 + so, idesc, ks == k0 ? 0u : 1u);
-        mma_tf32_ts(dH, al, bh0 + so, idesc, 1u);
-      }
-      for (int ks = k0; ks < k1; ++ks) {
-        const unsigned long long so = sc + (ks - k0) * kstepDesc;
-        mma_tf32_ts(dH, slot0 + 16u * (ks - k0), bh0 + so, idesc, 1u);
-      }
+    const unsigned long long as = a0 + sc, bs = b0 + sc;
+    const int nk2 = (k1 - k0 + 1) >> 1;
+    for (int g = 0; g < nk2; ++g) {
+      const unsigned long long ah = as + 2 * g * akDesc, bh = bs + 2 * g * bkDesc;
+      mma_f16_ss(dH, ah, bh + bkDesc, idesc, g == 0 ? 0u : 1u);
+      mma_f16_ss(dH, ah + akDesc, bh, idesc, 1u);
     }
+    for (int g = 0; g < nk2; ++g) mma_f16_ss(dH, as + 2 * g * akDesc, bs + 2 * g * bkDesc, idesc, 1u);
     mma_commit(&B.rel[gc % S::kRel]);
   }
   return true;
 }
 
-// Promotion warps (9..16): drain each chunk into round-to-nearest FP32 sums, then store
-// the tile (the analysis also clears l < m and l > lcap in the first tile of an order).
+// Promotion warps: drain each chunk into round-to-nearest FP32 sums, then store the tile
+// (the analysis also clears l < m and l > lcap in the first tile of an order). The
+// analysis undoes its per-chunk B scales chunk by chunk; the synthesis sums in units of
+// its per-(segment, row) scales and multiplies once, at the store.
 template <int MODE, int N>
 __device__ __forceinline__ bool promo_tile(const Args& a, const TileCoord& tc, const TileInfo& T, const Bars& B,
                                            unsigned tmem, unsigned c0) {
@@ -698,7 +569,7 @@ __device__ __forceinline__ bool promo_tile(const Args& a, const TileCoord& tc, c
   const PlanDev& P = a.P;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int q = warp & 3;                        // TMEM lane quadrant this warp may access
-  const int h = (warp - 9) >> 2;                 // column half
+  const int h = (warp - kPromo0) >> 2;           // column half
   const int row = 32 * q + lane;
   const unsigned lane_base = (unsigned)(32 * q) << 16;
   constexpr int kLd = (N / 2 < 16) ? N / 2 : 16;   // columns per TMEM load
@@ -708,10 +579,10 @@ __device__ __forceinline__ bool promo_tile(const Args& a, const TileCoord& tc, c
   bool ok = true;
   for (int c = 0; c < T.nch; ++c) {
     const unsigned gc = c0 + c;
-    const int bb = gc & 1;
-    // fp16x3: the chunk's column scales, written by the splitters before they arrived on
-    // full (complete long before the chunk's MMAs are)
-    if (kF16 && SHTB_PROMO_FULLWAIT && ok) ok = mbar_wait(&B.full[gc % S::kFull], (gc / S::kFull) & 1, B.abort_flag, a.err);
+    const int bb = gc % kAcc;
+    // analysis: the chunk's column scales, written by the splitters before they arrived
+    // on full (complete long before the chunk's MMAs are)
+    if (MODE == 1 && ok) ok = mbar_wait(&B.full[gc % S::kFull], (gc / S::kFull) & 1, B.abort_flag, a.err);
     if (ok) ok = mbar_wait(&B.rel[gc % S::kRel], (gc / S::kRel) & 1, B.abort_flag, a.err);
     ok = __all_sync(0xffffffffu, ok);   // warp-uniform: the TMEM loads are warp-collective
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -721,7 +592,7 @@ __device__ __forceinline__ bool promo_tile(const Args& a, const TileCoord& tc, c
     for (int i = 0; i < N / 2; i += kLd) {
       float v[kLd];
       tmem_ld<kLd>(dH + i, v);
-      if constexpr (kF16) {
+      if constexpr (MODE == 1) {
 #pragma unroll
         for (int u = 0; u < kLd; u += 4) {
           const float4 f = fs[(i + u) >> 2];   // exact powers of two: fma rounds once, like the add
@@ -749,10 +620,14 @@ __device__ __forceinline__ bool promo_tile(const Args& a, const TileCoord& tc, c
     const int pr = tc.p0 + row;
     if (pr < npair) {
       const size_t fstride = (size_t)P.nm * 2 * npair;
+      const float2* fsc = reinterpret_cast<const float2*>(a.bsc + (2 * im + par) * 2 * btile_nfp(nf)) + kf0;
       float2* w = a.Wout + (((size_t)kf0 * P.nm + im) * 2 + par) * npair + pr;
 #pragma unroll
       for (int qq = 0; qq < N / 4; ++qq)
-        if (qq < nq) w[qq * fstride] = make_float2(acc[2 * qq], acc[2 * qq + 1]);
+        if (qq < nq) {
+          const float2 f = fsc[qq];
+          w[qq * fstride] = make_float2(acc[2 * qq] * f.x, acc[2 * qq + 1] * f.y);
+        }
     }
   } else {
     const int l = m + 2 * (tc.j0 + row) + par;
@@ -769,7 +644,7 @@ __device__ __forceinline__ bool promo_tile(const Args& a, const TileCoord& tc, c
     // The first tile of each order also clears that order's degrees l < m and
     // lcap < l <= lmax (dense layout; a packed output is cleared before the call); the
     // two parity tiles take half of the fields each.
-    const int pt = tid - 9 * 32;
+    const int pt = tid - kPromo0 * 32;
     const int nfl = min(N / 2, nf - kb), hf = (nfl + 1) / 2;
     const int f0 = par ? hf : 0, f1 = par ? nfl : hf;
     const int lcap = a.lcap, ntail = P.lmax - lcap, per = m + ntail;
@@ -787,8 +662,9 @@ __device__ __forceinline__ bool promo_tile(const Args& a, const TileCoord& tc, c
 template <int MODE, int N, class Src>
 __device__ __forceinline__ void gemm_tiles(const Src& src, unsigned char* sm, const Bars& B, unsigned tmem) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const bool loader = (warp == 17 && lane == 0), splitter = warp < 8, mma = (warp == 8 && lane == 0),
-             promo = (warp >= 9 && warp <= 16);
+  // the synthesis B images arrive converted: its splitter warps have no work
+  const bool loader = (warp == kLoaderWarp && lane == 0), splitter = (MODE == 1 && warp < kSW),
+             mma = (warp == kMmaWarp && lane == 0), promo = (warp >= kPromo0 && warp < kPromo0 + 8);
   if (!(loader || splitter || mma || promo)) return;
   unsigned c0 = 0;
   for (int i = blockIdx.x; i < src.n; i += gridDim.x) {
@@ -799,7 +675,7 @@ __device__ __forceinline__ void gemm_tiles(const Src& src, unsigned char* sm, co
     if (loader)
       ok = loader_tile<MODE, N>(a, tc, T, sm, B, c0);
     else if (splitter)
-      ok = kF16 ? splitter_tile_f16<MODE, N>(a, T, sm, B, c0) : splitter_tile<MODE, N>(a, T, sm, B, tmem, c0);
+      ok = splitter_tile<MODE, N>(a, T, sm, B, c0);
     else if (mma)
       ok = mma_tile<MODE, N>(a, T, sm, B, tmem, c0);
     else
@@ -810,53 +686,126 @@ __device__ __forceinline__ void gemm_tiles(const Src& src, unsigned char* sm, co
   }
 }
 
-// Synthesis B tile images: the coefficients of order im, field k, times the per-(l, m)
-// factors, in FP32 (the GEMM splits them). Rows are the degrees l = m + par + 2j of one parity
-// (region seg(im, par)/8 + j/8 of the images); every row of the segment is written,
-// zero beyond lend, so the GEMM's last K-step of each segment reads zeros there.
-__device__ __forceinline__ void pack_order(const Args& a, int im, int k) {
+// One coefficient of the synthesis B images: a_lm times the per-(l, m) factors, zero
+// beyond lend.
+__device__ __forceinline__ float2 pack_value(const Args& a, const float2* c, int l, int m, bool scaled) {
+  float2 v = make_float2(0.f, 0.f);
+  if (l <= a.lend) {
+    v = c[l];
+    if (scaled) {
+      const float sc = coef_factor(a, l, m);
+      v.x *= sc;
+      v.y *= sc;
+    }
+  }
+  return v;
+}
+
+// Synthesis B tile images of order im, field k, as f16 hi/lo pairs; one block of
+// kPackThreads threads. Rows are the degrees l = m + par + 2j of one parity; degree row j
+// lies in f16 K-step j/16 of its segment, whose hi tile is image region seg(im, par)/8 +
+// 2 (j/16) and lo tile the region after it (element k16 = j % 16 of a row at byte
+// tile_off(row, k16 / 8) + 2 (k16 % 8)). Each (parity, re|im) row is scaled by the power of
+// two 2^e that brings its largest magnitude into [2^14, 2^15), and bsc receives
+// 2^-(e + s), s the table's exponent. Thread work unit b = 16 consecutive degrees
+// l = m + 16 b + q: the 8 degrees j = 8b..8b+7 of each parity, i.e. one 16-byte run of each
+// of its 4 rows, stored hi and lo with one 16-byte store each. A thread's first unit stays
+// in registers between the maximum and the store pass; further units (degrees beyond
+// 16 kPackThreads of the order) are read again. Every row of the segment is written, zero
+// beyond lend, so the last K-steps of each segment read zeros. All threads of the block
+// call it (it synchronises them).
+constexpr int kPackThreads = 64;
+__device__ __forceinline__ void pack_field(const Args& a, int im, int k) {
+  __shared__ unsigned smx[kPackThreads / 32][4];
   const PlanDev& P = a.P;
+  const int t = threadIdx.x, lane = t & 31;
   const int m = im * P.mres;
   const int nfp = btile_nfp(a.nf), fl = k & 63;
   const float2* c = a.cin + (long long)k * a.ld_k + coef_col(a, m);
-  for (int par = 0; par < 2; ++par) {
-    const long long sg = a.seg[2 * im + par];
-    const int R = (int)(a.seg[2 * im + par + 1] - sg);
-    for (int j = threadIdx.x; j < R; j += blockDim.x) {
-      const int l = m + par + 2 * j;
-      float2 v = make_float2(0.f, 0.f);
-      if (l <= a.lend) {
-        v = c[l];
-        if (a.sc_mode || a.mf0 != 1.f || a.mf1 != 1.f) {
-          const float sc = coef_factor(a, l, m);
-          v.x *= sc;
-          v.y *= sc;
-        }
+  const bool scaled = a.sc_mode || a.mf0 != 1.f || a.mf1 != 1.f;
+  const long long sg[2] = {a.seg[2 * im], a.seg[2 * im + 1]};
+  const int R[2] = {(int)(sg[1] - sg[0]), (int)(a.seg[2 * im + 2] - sg[1])};
+  const int nb = R[0] / 8;   // R[1] <= R[0]
+  float y[4][8];             // rows (par, re|im) x j % 8 of the first unit
+  unsigned mx[4] = {0u, 0u, 0u, 0u};
+  for (int b = t; b < nb; b += kPackThreads) {
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const float2 v = pack_value(a, c, m + 16 * b + q, m, scaled);
+      mx[2 * (q & 1)] = max(mx[2 * (q & 1)], __float_as_uint(v.x) & 0x7fffffffu);
+      mx[2 * (q & 1) + 1] = max(mx[2 * (q & 1) + 1], __float_as_uint(v.y) & 0x7fffffffu);
+      if (b == t) {
+        y[2 * (q & 1)][q >> 1] = v.x;
+        y[2 * (q & 1) + 1][q >> 1] = v.y;
       }
-      const long long base = (sg / kK + j / kK) * nfp * 16 + (long long)(k >> 6) * 1024;
-      const int kk = j & 7;
-      const long long o0 = base + btile_off(2 * fl, kk), o1 = base + btile_off(2 * fl + 1, kk);
-      a.bimg[o0] = v.x;
-      a.bimg[o1] = v.y;
     }
   }
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx[r] = max(mx[r], __shfl_xor_sync(0xffffffffu, mx[r], o));
+    if (lane == 0) smx[t >> 5][r] = mx[r];
+  }
+  __syncthreads();
+  float su[4];
+  const int sa = f16_table_exp(P.lmax);
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    unsigned v = 0u;
+#pragma unroll
+    for (int w = 0; w < kPackThreads / 32; ++w) v = max(v, smx[w][r]);
+    // max 2^e in [2^14, 2^15) (e at most 100: rows below 2^-86 keep the f16 subnormal steps)
+    const int e = min(141 - (int)(v >> 23), 100);
+    su[r] = __int_as_float((e + 127) << 23);
+    if (t == 0) a.bsc[(2 * im + (r >> 1)) * 2 * nfp + 2 * k + (r & 1)] = __int_as_float((127 - e - sa) << 23);
+  }
+  const long long lo = (long long)nfp * 64;   // bytes from a hi tile to its lo tile
+  for (int b = t; b < nb; b += kPackThreads) {
+    if (b != t) {
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const float2 v = pack_value(a, c, m + 16 * b + q, m, scaled);
+        y[2 * (q & 1)][q >> 1] = v.x;
+        y[2 * (q & 1) + 1][q >> 1] = v.y;
+      }
+    }
+#pragma unroll
+    for (int par = 0; par < 2; ++par) {
+      if (8 * b >= R[par]) continue;
+      unsigned char* base = reinterpret_cast<unsigned char*>(a.bimg + (sg[par] / kK + 2 * (b / 2)) * nfp * 16 +
+                                                             (long long)(k >> 6) * 1024);
+#pragma unroll
+      for (int ri = 0; ri < 2; ++ri) {
+        const float* z = y[2 * par + ri];
+        const float f = su[2 * par + ri];
+        uint4 h, l;
+        split_h2(z[0] * f, z[1] * f, h.x, l.x);
+        split_h2(z[2] * f, z[3] * f, h.y, l.y);
+        split_h2(z[4] * f, z[5] * f, h.z, l.z);
+        split_h2(z[6] * f, z[7] * f, h.w, l.w);
+        unsigned char* d = base + tile_off(2 * fl + ri, b & 1);
+        *reinterpret_cast<uint4*>(d) = h;
+        *reinterpret_cast<uint4*>(d + lo) = l;
+      }
+    }
+  }
+  __syncthreads();   // smx is reused by the next call
 }
 
 // blockIdx.x = order, blockIdx.y = field.
-__global__ void __launch_bounds__(256) mixed_pack_kernel(const __grid_constant__ Args a) {
-  pack_order(a, blockIdx.x, blockIdx.y);
+__global__ void __launch_bounds__(kPackThreads) mixed_pack_kernel(const __grid_constant__ Args a) {
+  pack_field(a, blockIdx.x, blockIdx.y);
 }
 
 // Persistent packing for grouped transforms: item = (transform, order), all its fields.
-__global__ void __launch_bounds__(256) mixed_pack_group_kernel(const Args* __restrict__ targs,
-                                                              const int2* __restrict__ items, int nitems) {
+__global__ void __launch_bounds__(kPackThreads) mixed_pack_group_kernel(const Args* __restrict__ targs,
+                                                                       const int2* __restrict__ items, int nitems) {
   __shared__ Args sa;
   for (int i = blockIdx.x; i < nitems; i += gridDim.x) {
     const int2 it = items[i];
     if (threadIdx.x == 0) sa = targs[it.x];
     __syncthreads();
-    for (int k = 0; k < sa.nf; ++k) pack_order(sa, it.y, k);
-    __syncthreads();
+    for (int k = 0; k < sa.nf; ++k) pack_field(sa, it.y, k);
   }
 }
 
@@ -957,8 +906,8 @@ __global__ void mixed_table_kernel(PlanDev P, float* __restrict__ tabS, float* _
   const double x = P.x[pair];
   const int l0 = P.l0[(size_t)im * P.npair + pair];
   const double2 r01 = P.r01[(size_t)im * P.npair + pair];
-  const int pt = pair / kM, pr = pair % kM, pk = pair % kK, pks = pair / kK;
-  const float asc = kF16 ? (float)(1 << f16_table_exp(P.lmax)) : 1.f;   // exact scaling
+  const int pt = pair / kM, pr = pair % kM;
+  const float asc = (float)(1 << f16_table_exp(P.lmax));   // exact scaling
   double ra = 0.0, rb = 0.0;
   for (int l = m; l <= P.lrec; ++l) {
     double r;
@@ -975,28 +924,20 @@ __global__ void mixed_table_kernel(PlanDev P, float* __restrict__ tabS, float* _
     const int R = (int)(seg[2 * im + par + 1] - sg);
     const float v = (float)(P.cfac[poff + (l - m)] * r) * asc;
     const int jt = j / kM, rr = j % kM, rows = min(kM, R - jt * kM);
-    if constexpr (kF16) {
-      // f16 hi/lo of P 2^s: K-step pair (2g, 2g + 1) of the FP32 layout holds the hi and lo
-      // tiles of f16 K-step g, element k16 of a row at byte tile_off(row, k16 / 8) + 2 (k16 % 8)
-      const __half h = __float2half_rn(v), lo = __float2half_rn(v - __half2float(h));
-      const int js = j % 16, ps = pair % 16;
-      unsigned char* ds = reinterpret_cast<unsigned char*>(tabS + sg * npp) +
-                          ((long long)pt * (R / kK) + 2 * (j / 16)) * kTileBytesA + tile_off(pr, js >> 3) + 2 * (js & 7);
-      unsigned char* da = reinterpret_cast<unsigned char*>(tabA + sg * npp + (long long)jt * kM * npp) +
-                          (long long)(2 * (pair / 16)) * rows * kK * 4 + tile_off(rr, ps >> 3) + 2 * (ps & 7);
-      *reinterpret_cast<__half*>(ds) = h;
-      *reinterpret_cast<__half*>(ds + kTileBytesA) = lo;
-      *reinterpret_cast<__half*>(da) = h;
-      *reinterpret_cast<__half*>(da + rows * kK * 4) = lo;
-      continue;
-    }
-    // synthesis: tile (pt, j/8), row pr, K slot j%8
-    const int k = j % kK;
-    tabS[sg * npp + ((long long)pt * (R / kK) + j / kK) * (kM * kK) + (pr >> 3) * 64 + (k >> 2) * 32 + (pr & 7) * 4 +
-         (k & 3)] = v;
-    // analysis: tile (j/128, pair/8) of rows = min(128, R - 128 (j/128)), row j%128, K slot pair%8
-    tabA[sg * npp + (long long)jt * kM * npp + (long long)pks * rows * kK + (rr >> 3) * 64 + (pk >> 2) * 32 +
-         (rr & 7) * 4 + (pk & 3)] = v;
+    // f16 hi/lo of P 2^s: image K-step pair (2g, 2g + 1) holds the hi and lo tiles of f16
+    // K-step g, element k16 of a row at byte tile_off(row, k16 / 8) + 2 (k16 % 8).
+    // synthesis: tile (pt, degree j / 16), row pr; analysis: tile (j / 128, pair / 16) of
+    // rows = min(128, R - 128 (j / 128)), row j % 128
+    const __half h = __float2half_rn(v), lo = __float2half_rn(v - __half2float(h));
+    const int js = j % 16, ps = pair % 16;
+    unsigned char* ds = reinterpret_cast<unsigned char*>(tabS + sg * npp) +
+                        ((long long)pt * (R / kK) + 2 * (j / 16)) * kTileBytesA + tile_off(pr, js >> 3) + 2 * (js & 7);
+    unsigned char* da = reinterpret_cast<unsigned char*>(tabA + sg * npp + (long long)jt * kM * npp) +
+                        (long long)(2 * (pair / 16)) * rows * kK * 4 + tile_off(rr, ps >> 3) + 2 * (ps & 7);
+    *reinterpret_cast<__half*>(ds) = h;
+    *reinterpret_cast<__half*>(ds + kTileBytesA) = lo;
+    *reinterpret_cast<__half*>(da) = h;
+    *reinterpret_cast<__half*>(da + rows * kK * 4) = lo;
   }
 }
 
@@ -1006,7 +947,7 @@ using namespace mx;
 
 // Segment starts of the P table: rows (degrees m+par, m+par+2, .., lrec) of every
 // (order, parity), each segment padded to a multiple of kSegRows rows (one f16 K-step of
-// 16 degrees, or one TF32 K-step of 8). Returns the row count.
+// 16 degrees). Returns the row count.
 static long long table_segments(const shtb_plan* p, std::vector<long long>* seg) {
   const int nm = p->nm, LR = p->lrec;
   if (seg) seg->assign(2 * nm + 1, 0);
@@ -1028,8 +969,12 @@ static size_t align256(size_t v) { return (v + 255) / 256 * 256; }
 // Synthesis workspace: Fourier buffer [f][nm][2][npair] (float2), then the B tile
 // images (table rows x nfp x 2 floats).
 static size_t syn_w_bytes(const shtb_plan* p, int nf) { return align256((size_t)nf * p->nm * 2 * p->npair * 8); }
-static size_t syn_img_bytes(const shtb_plan* p, int nf) {
+// ... then the per-(segment, row) scales of the images ([2 nm][2 nfp] floats).
+static size_t syn_img_only(const shtb_plan* p, int nf) {
   return align256((size_t)table_segments(p, nullptr) * btile_nfp(nf) * 2 * 4);
+}
+static size_t syn_img_bytes(const shtb_plan* p, int nf) {
+  return syn_img_only(p, nf) + align256((size_t)p->nm * 2 * 2 * btile_nfp(nf) * 4);
 }
 
 static int ensure_table(const shtb_plan* cp, cudaStream_t st) {
@@ -1134,12 +1079,13 @@ int mixed_synthesis(const shtb_plan* p, const void* alm, void* f, int nf, int lt
   }
   a.Wout = (float2*)work;
   a.bimg = (float*)((char*)work + syn_w_bytes(p, nf));
+  a.bsc = (float*)((char*)a.bimg + syn_img_only(p, nf));
   a.sc_mode = p->d_scale ? 1 : 0;
   a.nf = nf;
   a.lend = ltr;
   a.lcap = ltr;
   prof_begin(st);
-  mixed_pack_kernel<<<dim3(mlim / p->mres + 1, nf), 256, 0, st>>>(a);
+  mixed_pack_kernel<<<dim3(mlim / p->mres + 1, nf), kPackThreads, 0, st>>>(a);
   SHTB_LAUNCHED("tc gemm B packing kernel");
   const int ntp = (p->npair + kM - 1) / kM;
   if ((rc = dispatch_gemm<0>(p, a, nf, 2 * ntp * (mlim / p->mres + 1), ntp, st))) return rc;
@@ -1216,6 +1162,7 @@ void mixed_fill_args(const shtb_plan* p, int mode, const void* in, void* out, in
     a.cin = (const float2*)in;
     a.Wout = (float2*)out;
     a.bimg = (float*)((char*)out + syn_w_bytes(p, nf));
+    a.bsc = (float*)((char*)a.bimg + syn_img_only(p, nf));
     a.sc_mode = p->d_scale ? 1 : 0;
   } else {
     a.tab = p->d_tab_ana;
@@ -1238,7 +1185,7 @@ int mixed_group_tile_rows() { return kM; }
 
 int launch_pack_group(const void* targs, const int2* items, int nitems, int grid, cudaStream_t st) {
   if (nitems <= 0) return SHTB_OK;
-  mixed_pack_group_kernel<<<grid, 256, 0, st>>>((const Args*)targs, items, nitems);
+  mixed_pack_group_kernel<<<grid, kPackThreads, 0, st>>>((const Args*)targs, items, nitems);
   count_launch();
   SHTB_TRY_CUDA(cudaGetLastError(), "group pack launch");
   return SHTB_OK;
