@@ -55,6 +55,10 @@ constexpr int kSW = 8;
 constexpr int kMmaWarp = kSW, kPromo0 = kSW + 1, kLoaderWarp = kSW + 9;
 constexpr int kThreads = 32 * (kSW + 10);
 constexpr int kAcc = 4;          // TMEM chunk accumulators
+#ifndef SHTB_SPLIT_GROUPS
+#define SHTB_SPLIT_GROUPS 2
+#endif
+constexpr int kSG = SHTB_SPLIT_GROUPS;   // splitter groups, taking chunks gc % kSG in turn
 
 struct Args {
   PlanDev P;
@@ -446,22 +450,26 @@ __device__ __forceinline__ bool loader_tile(const Args& a, const TileCoord& tc, 
 // magnitude into [2^14, 2^15), split into f16 hi + lo and written in place (the same
 // core-matrix byte order: 16-byte rows of 8 f16 values). The factor 2^-(e + s) that undoes
 // this and the table's scale 2^s goes to the chunk's entry of the scale ring. A missing odd
-// K-step at the end of a tile converts as zeros.
+// K-step at the end of a tile converts as zeros. The kSG groups of kSW / kSG warps take
+// the chunks in turn (group gc % kSG), so conversions of consecutive chunks overlap.
 template <int MODE, int N>
 __device__ __forceinline__ bool splitter_tile(const Args& a, const TileInfo& T, unsigned char* sm, const Bars& B,
                                                   unsigned c0) {
   using S = Smem<N>;
-  constexpr int kTpr = (32 * kSW / N < 8) ? 32 * kSW / N : 8;   // threads per B row
+  constexpr int kGT = 32 * kSW / kSG;                       // threads per group
+  constexpr int kTpr = (kGT / N < 8) ? kGT / N : 8;         // threads per B row
   constexpr int kPieces = 2 * kChunk;                 // 16-byte pieces of a B row per chunk
   constexpr int kG = (kTpr > 4) ? kTpr / 4 : 1;       // f16 K-steps per conversion pass
   constexpr int kPp = 4 * kG / kTpr;                  // pieces per thread and pass
-  const int tid = threadIdx.x, lane = tid & 31;
+  static_assert(kGT >= N, "a splitter group covers every B row");
+  const int tid = threadIdx.x % kGT, grp = threadIdx.x / kGT, lane = tid & 31;
   const int nrows = (int)(T.bbytes >> 5);             // B rows loaded (2 per field)
   const int r = tid / kTpr, v = tid % kTpr;
   const bool rowok = tid < N * kTpr && r < nrows;
   const int sa = f16_table_exp(a.P.lmax);
   for (int c = 0; c < T.nch; ++c) {
     const unsigned gc = c0 + c;
+    if ((int)(gc % kSG) != grp) continue;
     const int nk = min(kChunk, T.nks - c * kChunk), nk2 = (nk + 1) >> 1;
     const bool ok = mbar_wait(&B.ldfull[gc % S::kSt], (gc / S::kSt) & 1, B.abort_flag, a.err);
     if (!__all_sync(0xffffffffu, ok)) return false;
@@ -514,7 +522,7 @@ __device__ __forceinline__ bool splitter_tile(const Args& a, const TileInfo& T, 
     // the B tiles written here are read by the MMAs (async proxy)
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncwarp();
-    if (lane == 0) mbar_arrive_cnt(&B.full[gc % S::kFull], 2);
+    if (lane == 0) mbar_arrive_cnt(&B.full[gc % S::kFull], 2 * kSG);
   }
   return true;
 }
