@@ -55,10 +55,6 @@ constexpr int kSW = 8;
 constexpr int kMmaWarp = kSW, kPromo0 = kSW + 1, kLoaderWarp = kSW + 9;
 constexpr int kThreads = 32 * (kSW + 10);
 constexpr int kAcc = 4;          // TMEM chunk accumulators
-#ifndef SHTB_SPLIT_GROUPS
-#define SHTB_SPLIT_GROUPS 2
-#endif
-constexpr int kSG = SHTB_SPLIT_GROUPS;   // splitter groups, taking chunks gc % kSG in turn
 
 struct Args {
   PlanDev P;
@@ -259,14 +255,14 @@ struct Smem {
   // hi and lo tiles of f16 K-step g (the analysis converts its FP32 B tiles in place).
   static constexpr int kStageA = kChunk * kTileBytesA;
   static constexpr int kStage = kChunk * (kTileBytesA + kTileB);
-  // Ring depth: up to 192 KB of stages per CTA (92 KB for each of the two 16-column CTAs
+  // Ring depth: up to 192 KB of stages per CTA (110 KB for each of the two 16-column CTAs
   // of an SM).
-  static constexpr int kSt = ((N == 16) ? 94208 : 196608) / kStage < 14 ? ((N == 16) ? 94208 : 196608) / kStage : 14;
+  static constexpr int kSt = ((N == 16) ? 112640 : 196608) / kStage < 14 ? ((N == 16) ? 112640 : 196608) / kStage : 14;
   static constexpr int kFull = 16;   // per-chunk conversion barriers (analysis)
   static constexpr int kRel = 16;    // chunk-release barriers
   static constexpr int kBar = kSt * kStage;
-  // barriers: full[kFull], ldfull[kSt], rel[kRel], acce[kAcc]; then TMEM slot, abort flag;
-  // then the FP32 column scales of the last kScR chunks (analysis)
+  // barriers: full[kFull], ldfull[kSt], rel[kRel], acce[kAcc]; then TMEM slot, abort flag,
+  // then the FP32 column scales of the last kScR chunks
   static constexpr int kScOff = (kBar + (kFull + kSt + kRel + kAcc) * 8 + 16 + 15) & ~15;
   static constexpr int kBytes = kScOff + kScR * N * 4;
   // TMEM: chunk accumulator b at columns [b N, (b + 1) N), b < kAcc
@@ -450,22 +446,25 @@ __device__ __forceinline__ bool loader_tile(const Args& a, const TileCoord& tc, 
 // magnitude into [2^14, 2^15), split into f16 hi + lo and written in place (the same
 // core-matrix byte order: 16-byte rows of 8 f16 values). The factor 2^-(e + s) that undoes
 // this and the table's scale 2^s goes to the chunk's entry of the scale ring. A missing odd
-// K-step at the end of a tile converts as zeros. The kSG groups of kSW / kSG warps take
-// the chunks in turn (group gc % kSG), so conversions of consecutive chunks overlap.
+// K-step at the end of a tile converts as zeros. With an even number of stages the
+// splitter warps form two groups that take the chunks in turn (group gc % 2), so
+// conversions of consecutive chunks overlap; a group's previous chunk in a stage is then
+// its own, whose copies it saw land, so its wait on the stage's ldfull barrier cannot match
+// an older phase. With an odd number of stages one group takes every chunk.
 template <int MODE, int N>
 __device__ __forceinline__ bool splitter_tile(const Args& a, const TileInfo& T, unsigned char* sm, const Bars& B,
                                                   unsigned c0) {
   using S = Smem<N>;
-  constexpr int kGT = 32 * kSW / kSG;                       // threads per group
-  constexpr int kTpr = (kGT / N < 8) ? kGT / N : 8;         // threads per B row
+  constexpr int kSG = (S::kSt % 2 == 0) ? 2 : 1;                         // splitter groups
+  constexpr int kGT = 32 * kSW / kSG;                                    // threads per group
+  constexpr int kTpr = (kGT >= 8 * N) ? 8 : (kGT >= N) ? kGT / N : 1;     // threads per B row
+  constexpr int kRpt = (kGT >= N) ? 1 : N / kGT;                         // B rows per thread
   constexpr int kPieces = 2 * kChunk;                 // 16-byte pieces of a B row per chunk
   constexpr int kG = (kTpr > 4) ? kTpr / 4 : 1;       // f16 K-steps per conversion pass
   constexpr int kPp = 4 * kG / kTpr;                  // pieces per thread and pass
-  static_assert(kGT >= N, "a splitter group covers every B row");
   const int tid = threadIdx.x % kGT, grp = threadIdx.x / kGT, lane = tid & 31;
-  const int nrows = (int)(T.bbytes >> 5);             // B rows loaded (2 per field)
-  const int r = tid / kTpr, v = tid % kTpr;
-  const bool rowok = tid < N * kTpr && r < nrows;
+  const int nrows = min((int)(T.bbytes >> 5), N);     // B rows loaded (2 per field)
+  const int v = tid % kTpr;
   const int sa = f16_table_exp(a.P.lmax);
   for (int c = 0; c < T.nch; ++c) {
     const unsigned gc = c0 + c;
@@ -473,52 +472,56 @@ __device__ __forceinline__ bool splitter_tile(const Args& a, const TileInfo& T, 
     const int nk = min(kChunk, T.nks - c * kChunk), nk2 = (nk + 1) >> 1;
     const bool ok = mbar_wait(&B.ldfull[gc % S::kSt], (gc / S::kSt) & 1, B.abort_flag, a.err);
     if (!__all_sync(0xffffffffu, ok)) return false;
-    // B row r: piece u = 2 st + khalf of FP32 tile st holds k = 4 u .. 4 u + 3 of the chunk.
-    // Pass 1: the row's largest magnitude (a thread's pieces u = v, v + kTpr, ...).
     unsigned char* Bs = sm + (size_t)(gc % S::kSt) * S::kStage + S::kStageA;
-    unsigned mx = 0;
+    for (int ri = 0; ri < kRpt; ++ri) {
+      const int r = tid / kTpr + ri * (kGT / kTpr);
+      const bool rowok = r < nrows;
+      // B row r: piece u = 2 st + khalf of FP32 tile st holds k = 4 u .. 4 u + 3 of the chunk.
+      // Pass 1: the row's largest magnitude (a thread's pieces u = v, v + kTpr, ...).
+      unsigned mx = 0;
 #pragma unroll
-    for (int u = v; u < kPieces; u += kTpr) {
-      if (rowok && (u >> 1) < nk) {
-        const float4 x = *reinterpret_cast<const float4*>(Bs + (u >> 1) * T.bstr + tile_off(r, u & 1));
-        mx = max(mx, max(max(__float_as_uint(x.x) & 0x7fffffffu, __float_as_uint(x.y) & 0x7fffffffu),
-                         max(__float_as_uint(x.z) & 0x7fffffffu, __float_as_uint(x.w) & 0x7fffffffu)));
+      for (int u = v; u < kPieces; u += kTpr) {
+        if (rowok && (u >> 1) < nk) {
+          const float4 x = *reinterpret_cast<const float4*>(Bs + (u >> 1) * T.bstr + tile_off(r, u & 1));
+          mx = max(mx, max(max(__float_as_uint(x.x) & 0x7fffffffu, __float_as_uint(x.y) & 0x7fffffffu),
+                           max(__float_as_uint(x.z) & 0x7fffffffu, __float_as_uint(x.w) & 0x7fffffffu)));
+        }
       }
-    }
 #pragma unroll
-    for (int o = 1; o < kTpr; o <<= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    // max * 2^e in [2^14, 2^15) (e at most 100: rows below 2^-86 keep the f16 subnormal steps)
-    const int e = min(141 - (int)(mx >> 23), 100);
-    const float su = __int_as_float((e + 127) << 23);
-    // Pass 2, kG f16 K-steps at a time: their pieces are read before any of them is
-    // overwritten (a row's threads share a warp).
-    for (int g0 = 0; 2 * g0 < nk; g0 += kG) {
-      float4 xb[kPp];
-#pragma unroll
-      for (int j = 0; j < kPp; ++j) {
-        const int u = 4 * g0 + v + j * kTpr, st = u >> 1;
-        xb[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (rowok && u < 4 * (g0 + kG) && st < nk)
-          xb[j] = *reinterpret_cast<const float4*>(Bs + st * T.bstr + tile_off(r, u & 1));
-      }
-      __syncwarp();
-      if (rowok) {
+      for (int o = 1; o < kTpr; o <<= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      // max * 2^e in [2^14, 2^15) (e at most 100: rows below 2^-86 keep the f16 subnormal steps)
+      const int e = min(141 - (int)(mx >> 23), 100);
+      const float su = __int_as_float((e + 127) << 23);
+      // Pass 2, kG f16 K-steps at a time: their pieces are read before any of them is
+      // overwritten (a row's threads share a warp).
+      for (int g0 = 0; 2 * g0 < nk; g0 += kG) {
+        float4 xb[kPp];
 #pragma unroll
         for (int j = 0; j < kPp; ++j) {
           const int u = 4 * g0 + v + j * kTpr, st = u >> 1;
-          if (u < 4 * (g0 + kG) && st < 2 * nk2) {
-            unsigned h0, l0, h1, l1;
-            split_h2(xb[j].x * su, xb[j].y * su, h0, l0);
-            split_h2(xb[j].z * su, xb[j].w * su, h1, l1);
-            unsigned char* d = Bs + (st & ~1) * T.bstr + tile_off(r, st & 1) + (u & 1) * 8;
-            *reinterpret_cast<uint2*>(d) = make_uint2(h0, h1);
-            *reinterpret_cast<uint2*>(d + T.bstr) = make_uint2(l0, l1);
+          xb[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (rowok && u < 4 * (g0 + kG) && st < nk)
+            xb[j] = *reinterpret_cast<const float4*>(Bs + st * T.bstr + tile_off(r, u & 1));
+        }
+        __syncwarp();
+        if (rowok) {
+#pragma unroll
+          for (int j = 0; j < kPp; ++j) {
+            const int u = 4 * g0 + v + j * kTpr, st = u >> 1;
+            if (u < 4 * (g0 + kG) && st < 2 * nk2) {
+              unsigned h0, l0, h1, l1;
+              split_h2(xb[j].x * su, xb[j].y * su, h0, l0);
+              split_h2(xb[j].z * su, xb[j].w * su, h1, l1);
+              unsigned char* d = Bs + (st & ~1) * T.bstr + tile_off(r, st & 1) + (u & 1) * 8;
+              *reinterpret_cast<uint2*>(d) = make_uint2(h0, h1);
+              *reinterpret_cast<uint2*>(d + T.bstr) = make_uint2(l0, l1);
+            }
           }
         }
+        __syncwarp();
       }
-      __syncwarp();
+      if (rowok && v == 0) B.fsc[(gc % kScR) * N + r] = __int_as_float((127 - e - sa) << 23);
     }
-    if (rowok && v == 0) B.fsc[(gc % kScR) * N + r] = __int_as_float((127 - e - sa) << 23);
     // the B tiles written here are read by the MMAs (async proxy)
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncwarp();
