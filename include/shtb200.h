@@ -218,7 +218,7 @@ int shtb_synthesis_noalloc(const shtb_plan* plan, const void* alm, void* f, int 
                            void* stream);
 
 /*
- * Uneven batches: n independent mixed-precision (FP32 buffers, 3xTF32 tensor-core
+ * Uneven batches: n independent mixed-precision (FP32 buffers, fp16x3 tensor-core
  * Legendre stage) scalar transforms, each with its own plan (its own lmax, Gauss grid
  * and nlon) and 1..8 fields. No single counterpart in the reference, whose transforms
  * run one configuration per call (src/core_transforms.jl, src/batch_transforms.jl):

@@ -1,4 +1,4 @@
-"""GPU parity of the mixed-precision (tensor-core 3xTF32) path.
+"""GPU parity of the mixed-precision (tensor-core fp16x3) path.
 
 Inputs are rounded to FP32 (the path's I/O type); the FP64 oracle runs on the same
 rounded inputs. Bar: relative L2 <= 1e-6 against the FP64 result.
