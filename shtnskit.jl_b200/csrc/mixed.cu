@@ -720,13 +720,23 @@ __device__ __forceinline__ float2 pack_value(const Args& a, const float2* c, int
 // two 2^e that brings its largest magnitude into [2^14, 2^15), and bsc receives
 // 2^-(e + s), s the table's exponent. Thread work unit b = 16 consecutive degrees
 // l = m + 16 b + q: the 8 degrees j = 8b..8b+7 of each parity, i.e. one 16-byte run of each
-// of its 4 rows, stored hi and lo with one 16-byte store each. A thread's first unit stays
-// in registers between the maximum and the store pass; further units (degrees beyond
-// 16 kPackThreads of the order) are read again. Every row of the segment is written, zero
-// beyond lend, so the last K-steps of each segment read zeros. All threads of the block
-// call it (it synchronises them).
+// of its 4 rows, stored hi and lo with one 16-byte store each. The block stages
+// kPackThreads units at a time in shared memory (coalesced loads of the coefficient
+// column; each thread then reads its unit as 16-byte words); orders longer than one
+// staging pass are read twice (maximum pass, store pass). Every row of the segment is
+// written, zero beyond lend, so the last K-steps of each segment read zeros. All threads
+// of the block call it (it synchronises them).
 constexpr int kPackThreads = 64;
+constexpr int kPackRow = 18;   // float2 per staged unit: 16 values and 16 bytes of skew
+__device__ __forceinline__ void pack_stage(const Args& a, const float2* c, int m, int b0, int nb, bool scaled,
+                                           float2 (*buf)[kPackRow]) {
+  for (int i = threadIdx.x; i < kPackThreads * 16; i += kPackThreads) {
+    const int b = b0 + i / 16;
+    buf[i / 16][i % 16] = (b < nb) ? pack_value(a, c, m + 16 * b0 + i, m, scaled) : make_float2(0.f, 0.f);
+  }
+}
 __device__ __forceinline__ void pack_field(const Args& a, int im, int k) {
+  __shared__ __align__(16) float2 buf[kPackThreads][kPackRow];
   __shared__ unsigned smx[kPackThreads / 32][4];
   const PlanDev& P = a.P;
   const int t = threadIdx.x, lane = t & 31;
@@ -736,19 +746,21 @@ __device__ __forceinline__ void pack_field(const Args& a, int im, int k) {
   const bool scaled = a.sc_mode || a.mf0 != 1.f || a.mf1 != 1.f;
   const long long sg[2] = {a.seg[2 * im], a.seg[2 * im + 1]};
   const int R[2] = {(int)(sg[1] - sg[0]), (int)(a.seg[2 * im + 2] - sg[1])};
-  const int nb = R[0] / 8;   // R[1] <= R[0]
-  float y[4][8];             // rows (par, re|im) x j % 8 of the first unit
-  unsigned mx[4] = {0u, 0u, 0u, 0u};
-  for (int b = t; b < nb; b += kPackThreads) {
+  const int nb = R[0] / 8;   // units; R[1] <= R[0]
+  const int npass = (nb + kPackThreads - 1) / kPackThreads;
+  unsigned mx[4] = {0u, 0u, 0u, 0u};   // rows (par, re|im)
+  for (int ps = 0; ps < npass; ++ps) {
+    if (ps > 0) __syncthreads();
+    pack_stage(a, c, m, ps * kPackThreads, nb, scaled, buf);
+    __syncthreads();
+    const float4* u = reinterpret_cast<const float4*>(buf[t]);
 #pragma unroll
-    for (int q = 0; q < 16; ++q) {
-      const float2 v = pack_value(a, c, m + 16 * b + q, m, scaled);
-      mx[2 * (q & 1)] = max(mx[2 * (q & 1)], __float_as_uint(v.x) & 0x7fffffffu);
-      mx[2 * (q & 1) + 1] = max(mx[2 * (q & 1) + 1], __float_as_uint(v.y) & 0x7fffffffu);
-      if (b == t) {
-        y[2 * (q & 1)][q >> 1] = v.x;
-        y[2 * (q & 1) + 1][q >> 1] = v.y;
-      }
+    for (int q = 0; q < 8; ++q) {   // float4 q = degrees 2q (even parity) and 2q + 1
+      const float4 v = u[q];
+      mx[0] = max(mx[0], __float_as_uint(v.x) & 0x7fffffffu);
+      mx[1] = max(mx[1], __float_as_uint(v.y) & 0x7fffffffu);
+      mx[2] = max(mx[2], __float_as_uint(v.z) & 0x7fffffffu);
+      mx[3] = max(mx[3], __float_as_uint(v.w) & 0x7fffffffu);
     }
   }
 #pragma unroll
@@ -771,14 +783,23 @@ __device__ __forceinline__ void pack_field(const Args& a, int im, int k) {
     if (t == 0) a.bsc[(2 * im + (r >> 1)) * 2 * nfp + 2 * k + (r & 1)] = __int_as_float((127 - e - sa) << 23);
   }
   const long long lo = (long long)nfp * 64;   // bytes from a hi tile to its lo tile
-  for (int b = t; b < nb; b += kPackThreads) {
-    if (b != t) {
+  for (int ps = 0; ps < npass; ++ps) {
+    if (npass > 1) {   // the last staged pass is still in shared memory when npass == 1
+      __syncthreads();
+      pack_stage(a, c, m, ps * kPackThreads, nb, scaled, buf);
+      __syncthreads();
+    }
+    const int b = ps * kPackThreads + t;
+    if (b >= nb) continue;
+    const float4* u = reinterpret_cast<const float4*>(buf[t]);
+    float y[4][8];   // rows (par, re|im) x j % 8
 #pragma unroll
-      for (int q = 0; q < 16; ++q) {
-        const float2 v = pack_value(a, c, m + 16 * b + q, m, scaled);
-        y[2 * (q & 1)][q >> 1] = v.x;
-        y[2 * (q & 1) + 1][q >> 1] = v.y;
-      }
+    for (int q = 0; q < 8; ++q) {
+      const float4 v = u[q];
+      y[0][q] = v.x * su[0];
+      y[1][q] = v.y * su[1];
+      y[2][q] = v.z * su[2];
+      y[3][q] = v.w * su[3];
     }
 #pragma unroll
     for (int par = 0; par < 2; ++par) {
@@ -788,19 +809,18 @@ __device__ __forceinline__ void pack_field(const Args& a, int im, int k) {
 #pragma unroll
       for (int ri = 0; ri < 2; ++ri) {
         const float* z = y[2 * par + ri];
-        const float f = su[2 * par + ri];
         uint4 h, l;
-        split_h2(z[0] * f, z[1] * f, h.x, l.x);
-        split_h2(z[2] * f, z[3] * f, h.y, l.y);
-        split_h2(z[4] * f, z[5] * f, h.z, l.z);
-        split_h2(z[6] * f, z[7] * f, h.w, l.w);
+        split_h2(z[0], z[1], h.x, l.x);
+        split_h2(z[2], z[3], h.y, l.y);
+        split_h2(z[4], z[5], h.z, l.z);
+        split_h2(z[6], z[7], h.w, l.w);
         unsigned char* d = base + tile_off(2 * fl + ri, b & 1);
         *reinterpret_cast<uint4*>(d) = h;
         *reinterpret_cast<uint4*>(d + lo) = l;
       }
     }
   }
-  __syncthreads();   // smx is reused by the next call
+  __syncthreads();   // buf and smx are reused by the next call
 }
 
 // blockIdx.x = order, blockIdx.y = field.
