@@ -258,12 +258,13 @@ struct Smem {
   // Ring depth: up to 192 KB of stages per CTA (110 KB for each of the two 16-column CTAs
   // of an SM).
   static constexpr int kSt = ((N == 16) ? 112640 : 196608) / kStage < 14 ? ((N == 16) ? 112640 : 196608) / kStage : 14;
+  static constexpr int kLd = 2 * kSt;   // copy barriers: chunk gc's copies complete on ldfull[gc % kLd]
   static constexpr int kFull = 16;   // per-chunk conversion barriers (analysis)
   static constexpr int kRel = 16;    // chunk-release barriers
   static constexpr int kBar = kSt * kStage;
-  // barriers: full[kFull], ldfull[kSt], rel[kRel], acce[kAcc]; then TMEM slot, abort flag,
+  // barriers: full[kFull], ldfull[kLd], rel[kRel], acce[kAcc]; then TMEM slot, abort flag,
   // then the FP32 column scales of the last kScR chunks
-  static constexpr int kScOff = (kBar + (kFull + kSt + kRel + kAcc) * 8 + 16 + 15) & ~15;
+  static constexpr int kScOff = (kBar + (kFull + kLd + kRel + kAcc) * 8 + 16 + 15) & ~15;
   static constexpr int kBytes = kScOff + kScR * N * 4;
   // TMEM: chunk accumulator b at columns [b N, (b + 1) N), b < kAcc
   static constexpr int kTmemNeed = kAcc * N;
@@ -301,8 +302,8 @@ __device__ __forceinline__ Bars gemm_bars(unsigned char* sm) {
   using S = Smem<N>;  // barriers follow the stage ring
   Bars B;
   B.full = reinterpret_cast<unsigned long long*>(sm + S::kBar);   // [kFull] chunk gc split (A in TMEM)
-  B.ldfull = B.full + S::kFull;   // [kSt] bulk copies of the stage landed
-  B.rel = B.ldfull + S::kSt;      // [kRel] MMAs of chunk q done (q % kRel)
+  B.ldfull = B.full + S::kFull;   // [kLd] bulk copies of chunk q landed (q % kLd)
+  B.rel = B.ldfull + S::kLd;      // [kRel] MMAs of chunk q done (q % kRel)
   B.acce = B.rel + S::kRel;       // [kAcc] TMEM chunk accumulator b drained by the promotion warps
   B.tmem_slot = reinterpret_cast<unsigned*>(B.acce + kAcc);
   B.abort_flag = reinterpret_cast<volatile int*>(B.tmem_slot + 1);
@@ -325,7 +326,7 @@ __device__ __forceinline__ unsigned gemm_cta_setup(const Bars& B) {
   if (tid == 0) {
     // two arrivals per splitter warp and chunk
     for (int s = 0; s < Smem<N>::kFull; ++s) mbar_init(&B.full[s], 2 * kSW);
-    for (int s = 0; s < Smem<N>::kSt; ++s) mbar_init(&B.ldfull[s], 1);
+    for (int s = 0; s < Smem<N>::kLd; ++s) mbar_init(&B.ldfull[s], 1);
     for (int s = 0; s < Smem<N>::kRel; ++s) mbar_init(&B.rel[s], 1);
     for (int b = 0; b < kAcc; ++b) mbar_init(&B.acce[b], 8);   // one arrival per promotion warp
     *B.abort_flag = 0;
@@ -362,7 +363,7 @@ __device__ __forceinline__ void gemm_cta_teardown(unsigned tmem) {
 //
 // Synchronisation: chunk gc (kChunk image K-steps, fewer at the end of a tile) occupies
 // shared-memory stage gc % kSt and TMEM accumulator gc % kAcc. The loader's bulk copies
-// complete on ldfull[gc % kSt]; the analysis splitters convert the chunk's B tiles and
+// complete on ldfull[gc % kLd]; the analysis splitters convert the chunk's B tiles and
 // arrive on full[gc % kFull]; the MMA issuer waits for one of the two, issues the chunk's
 // 3 (kChunk / 2) MMAs back to back and commits once, to rel[gc % kRel]. Each mbarrier
 // wait costs a few hundred cycles even when the phase has completed, so the MMA issuer
@@ -424,7 +425,7 @@ __device__ __forceinline__ bool loader_tile(const Args& a, const TileCoord& tc, 
     const int k0 = c * kChunk, nk = min(kChunk, T.nks - k0);
     unsigned char* sa = sm + (size_t)st * S::kStage;
     unsigned char* sb = sa + S::kStageA;
-    unsigned long long* bar = &B.ldfull[st];
+    unsigned long long* bar = &B.ldfull[gc % S::kLd];
     // A tiles come in hi/lo pairs, and so do the synthesis B tiles (the analysis loads its
     // FP32 B tiles and treats a missing last odd one as zeros)
     const int na = (nk + 1) & ~1, nb = (MODE == 0) ? na : nk;
@@ -446,16 +447,18 @@ __device__ __forceinline__ bool loader_tile(const Args& a, const TileCoord& tc, 
 // magnitude into [2^14, 2^15), split into f16 hi + lo and written in place (the same
 // core-matrix byte order: 16-byte rows of 8 f16 values). The factor 2^-(e + s) that undoes
 // this and the table's scale 2^s goes to the chunk's entry of the scale ring. A missing odd
-// K-step at the end of a tile converts as zeros. With an even number of stages the
-// splitter warps form two groups that take the chunks in turn (group gc % 2), so
-// conversions of consecutive chunks overlap; a group's previous chunk in a stage is then
-// its own, whose copies it saw land, so its wait on the stage's ldfull barrier cannot match
-// an older phase. With an odd number of stages one group takes every chunk.
+// K-step at the end of a tile converts as zeros. The splitter warps form two groups that
+// take the chunks in turn (group gc % 2), so conversions of consecutive chunks overlap. A
+// group reaches chunk gc after its own chunk gc - 2, possibly before the loader has
+// refilled the stage; the copy barriers form a ring of 2 kSt (an even count), so the
+// previous phase of chunk gc's barrier belongs to chunk gc - 2 kSt, the group's own, whose
+// copies it saw land: its wait cannot match an older phase.
 template <int MODE, int N>
 __device__ __forceinline__ bool splitter_tile(const Args& a, const TileInfo& T, unsigned char* sm, const Bars& B,
                                                   unsigned c0) {
   using S = Smem<N>;
-  constexpr int kSG = (S::kSt % 2 == 0) ? 2 : 1;                         // splitter groups
+  constexpr int kSG = 2;                                                 // splitter groups
+  static_assert(S::kLd % kSG == 0, "copy-barrier ring a multiple of the groups");
   constexpr int kGT = 32 * kSW / kSG;                                    // threads per group
   constexpr int kTpr = (kGT >= 8 * N) ? 8 : (kGT >= N) ? kGT / N : 1;     // threads per B row
   constexpr int kRpt = (kGT >= N) ? 1 : N / kGT;                         // B rows per thread
@@ -470,7 +473,7 @@ __device__ __forceinline__ bool splitter_tile(const Args& a, const TileInfo& T, 
     const unsigned gc = c0 + c;
     if ((int)(gc % kSG) != grp) continue;
     const int nk = min(kChunk, T.nks - c * kChunk), nk2 = (nk + 1) >> 1;
-    const bool ok = mbar_wait(&B.ldfull[gc % S::kSt], (gc / S::kSt) & 1, B.abort_flag, a.err);
+    const bool ok = mbar_wait(&B.ldfull[gc % S::kLd], (gc / S::kLd) & 1, B.abort_flag, a.err);
     if (!__all_sync(0xffffffffu, ok)) return false;
     unsigned char* Bs = sm + (size_t)(gc % S::kSt) * S::kStage + S::kStageA;
     for (int ri = 0; ri < kRpt; ++ri) {
@@ -546,7 +549,7 @@ __device__ __forceinline__ bool mma_tile(const Args& a, const TileInfo& T, unsig
     const int bb = gc % kAcc;
     if (gc >= kAcc && !mbar_wait(&B.acce[bb], ((gc / kAcc) - 1) & 1, B.abort_flag, a.err)) return false;
     const int k0 = c * kChunk, k1 = min(T.nks, k0 + kChunk);
-    const bool ready = (MODE == 0) ? mbar_wait(&B.ldfull[gc % S::kSt], (gc / S::kSt) & 1, B.abort_flag, a.err)
+    const bool ready = (MODE == 0) ? mbar_wait(&B.ldfull[gc % S::kLd], (gc / S::kLd) & 1, B.abort_flag, a.err)
                                    : mbar_wait(&B.full[gc % S::kFull], (gc / S::kFull) & 1, B.abort_flag, a.err);
     if (!ready) return false;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
