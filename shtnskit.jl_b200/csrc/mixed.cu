@@ -463,8 +463,7 @@ __device__ __forceinline__ bool splitter_tile(const Args& a, const TileInfo& T, 
   constexpr int kTpr = (kGT >= 8 * N) ? 8 : (kGT >= N) ? kGT / N : 1;     // threads per B row
   constexpr int kRpt = (kGT >= N) ? 1 : N / kGT;                         // B rows per thread
   constexpr int kPieces = 2 * kChunk;                 // 16-byte pieces of a B row per chunk
-  constexpr int kG = (kTpr > 4) ? kTpr / 4 : 1;       // f16 K-steps per conversion pass
-  constexpr int kPp = 4 * kG / kTpr;                  // pieces per thread and pass
+  constexpr int kPt = (kPieces + kTpr - 1) / kTpr;    // pieces per thread
   const int tid = threadIdx.x % kGT, grp = threadIdx.x / kGT, lane = tid & 31;
   const int nrows = min((int)(T.bbytes >> 5), N);     // B rows loaded (2 per field)
   const int v = tid % kTpr;
@@ -480,14 +479,19 @@ __device__ __forceinline__ bool splitter_tile(const Args& a, const TileInfo& T, 
       const int r = tid / kTpr + ri * (kGT / kTpr);
       const bool rowok = r < nrows;
       // B row r: piece u = 2 st + khalf of FP32 tile st holds k = 4 u .. 4 u + 3 of the chunk.
-      // Pass 1: the row's largest magnitude (a thread's pieces u = v, v + kTpr, ...).
+      // The thread's pieces u = v, v + kTpr, ... go to registers, with the row's largest
+      // magnitude; all of the row's pieces are read before any is overwritten (a row's
+      // threads share a warp), then converted from the registers.
+      float4 xb[kPt];
       unsigned mx = 0;
 #pragma unroll
-      for (int u = v; u < kPieces; u += kTpr) {
-        if (rowok && (u >> 1) < nk) {
-          const float4 x = *reinterpret_cast<const float4*>(Bs + (u >> 1) * T.bstr + tile_off(r, u & 1));
-          mx = max(mx, max(max(__float_as_uint(x.x) & 0x7fffffffu, __float_as_uint(x.y) & 0x7fffffffu),
-                           max(__float_as_uint(x.z) & 0x7fffffffu, __float_as_uint(x.w) & 0x7fffffffu)));
+      for (int j = 0; j < kPt; ++j) {
+        const int u = v + j * kTpr;
+        xb[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (rowok && u < kPieces && (u >> 1) < nk) {
+          xb[j] = *reinterpret_cast<const float4*>(Bs + (u >> 1) * T.bstr + tile_off(r, u & 1));
+          mx = max(mx, max(max(__float_as_uint(xb[j].x) & 0x7fffffffu, __float_as_uint(xb[j].y) & 0x7fffffffu),
+                           max(__float_as_uint(xb[j].z) & 0x7fffffffu, __float_as_uint(xb[j].w) & 0x7fffffffu)));
         }
       }
 #pragma unroll
@@ -495,33 +499,20 @@ __device__ __forceinline__ bool splitter_tile(const Args& a, const TileInfo& T, 
       // max * 2^e in [2^14, 2^15) (e at most 100: rows below 2^-86 keep the f16 subnormal steps)
       const int e = min(141 - (int)(mx >> 23), 100);
       const float su = __int_as_float((e + 127) << 23);
-      // Pass 2, kG f16 K-steps at a time: their pieces are read before any of them is
-      // overwritten (a row's threads share a warp).
-      for (int g0 = 0; 2 * g0 < nk; g0 += kG) {
-        float4 xb[kPp];
+      __syncwarp();
+      if (rowok) {
 #pragma unroll
-        for (int j = 0; j < kPp; ++j) {
-          const int u = 4 * g0 + v + j * kTpr, st = u >> 1;
-          xb[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-          if (rowok && u < 4 * (g0 + kG) && st < nk)
-            xb[j] = *reinterpret_cast<const float4*>(Bs + st * T.bstr + tile_off(r, u & 1));
-        }
-        __syncwarp();
-        if (rowok) {
-#pragma unroll
-          for (int j = 0; j < kPp; ++j) {
-            const int u = 4 * g0 + v + j * kTpr, st = u >> 1;
-            if (u < 4 * (g0 + kG) && st < 2 * nk2) {
-              unsigned h0, l0, h1, l1;
-              split_h2(xb[j].x * su, xb[j].y * su, h0, l0);
-              split_h2(xb[j].z * su, xb[j].w * su, h1, l1);
-              unsigned char* d = Bs + (st & ~1) * T.bstr + tile_off(r, st & 1) + (u & 1) * 8;
-              *reinterpret_cast<uint2*>(d) = make_uint2(h0, h1);
-              *reinterpret_cast<uint2*>(d + T.bstr) = make_uint2(l0, l1);
-            }
+        for (int j = 0; j < kPt; ++j) {
+          const int u = v + j * kTpr, st = u >> 1;
+          if (u < kPieces && st < 2 * nk2) {   // a missing odd K-step is written as zeros
+            unsigned h0, l0, h1, l1;
+            split_h2(xb[j].x * su, xb[j].y * su, h0, l0);
+            split_h2(xb[j].z * su, xb[j].w * su, h1, l1);
+            unsigned char* d = Bs + (st & ~1) * T.bstr + tile_off(r, st & 1) + (u & 1) * 8;
+            *reinterpret_cast<uint2*>(d) = make_uint2(h0, h1);
+            *reinterpret_cast<uint2*>(d + T.bstr) = make_uint2(l0, l1);
           }
         }
-        __syncwarp();
       }
       if (rowok && v == 0) B.fsc[(gc % kScR) * N + r] = __int_as_float((127 - e - sa) << 23);
     }

@@ -78,3 +78,45 @@ def test_mixed_config3_size():
     assert rel_l2(host(b32), host(b64)) <= TOLMX
     assert rel_l2(host(b32), a64) <= TOLMX
     cfg.plan(0).status()
+
+
+def test_mixed_field_magnitudes():
+    """Fields 50 orders of magnitude apart, an all-zero field, a field whose low degrees
+    dominate its high ones by 1e6, and a single nonzero coefficient, in one batch. The f16
+    split scales every B row (field, re|im) by its own power of two, so each field meets
+    the bar on its own and the zero field stays exactly zero."""
+    lmax, nlat, nlon = 63, 64, 128
+    cfg = sht.create_gauss_config(lmax, nlat, nlon=nlon)
+    ocfg = so.create_gauss_config(lmax, nlat, nlon=nlon)
+    nf = 6
+    a = rand_alm(lmax, lmax, nf, seed=11)
+    a[:, :, 1] *= 1e25
+    a[:, :, 2] *= 1e-25
+    a[:, :, 3] = 0
+    a[:10, :, 4] *= 1e6
+    a[:, :, 5] = 0
+    a[7, 3, 5] = 2.5 - 1.5j
+    a = a.astype(np.complex64).astype(np.complex128)
+    f = host(sht.synthesis_batch(cfg, a.astype(np.complex64), precision="mixed"))
+    f_ref = so.synthesis_batch(ocfg, a)
+    for k in range(nf):
+        if k == 3:
+            assert not np.any(f[:, :, k]), "zero field"
+        else:
+            assert rel_l2(f[:, :, k], f_ref[:, :, k]) <= TOLMX, f"synthesis field {k}"
+    g = np.random.default_rng(12).standard_normal((nlat, nlon, nf))
+    g[:, :, 1] *= 1e25
+    g[:, :, 2] *= 1e-25
+    g[:, :, 3] = 0
+    g[:, :, 4] += 1e6 * np.cos(np.arange(nlon) * 2 * np.pi / nlon)[None, :]
+    g[:, :, 5] = 0
+    g[5, 9, 5] = 3.0
+    g = g.astype(np.float32)
+    b = host(sht.analysis_batch(cfg, g, precision="mixed"))
+    b_ref = so.analysis_batch(ocfg, g.astype(np.float64))
+    for k in range(nf):
+        if k == 3:
+            assert not np.any(b[:, :, k]), "zero field"
+        else:
+            assert rel_l2(b[:, :, k], b_ref[:, :, k]) <= TOLMX, f"analysis field {k}"
+    cfg.plan(0).status()
