@@ -706,48 +706,55 @@ __device__ __forceinline__ float2 pack_value(const Args& a, const float2* c, int
   return v;
 }
 
-// Synthesis B tile images of order im, field k, as f16 hi/lo pairs; one block of
-// kPackThreads threads. Rows are the degrees l = m + par + 2j of one parity; degree row j
-// lies in f16 K-step j/16 of its segment, whose hi tile is image region seg(im, par)/8 +
-// 2 (j/16) and lo tile the region after it (element k16 = j % 16 of a row at byte
-// tile_off(row, k16 / 8) + 2 (k16 % 8)). Each (parity, re|im) row is scaled by the power of
-// two 2^e that brings its largest magnitude into [2^14, 2^15), and bsc receives
-// 2^-(e + s), s the table's exponent. Thread work unit b = 16 consecutive degrees
-// l = m + 16 b + q: the 8 degrees j = 8b..8b+7 of each parity, i.e. one 16-byte run of each
-// of its 4 rows, stored hi and lo with one 16-byte store each. The block stages
-// kPackThreads units at a time in shared memory (coalesced loads of the coefficient
-// column; each thread then reads its unit as 16-byte words); orders longer than one
-// staging pass are read twice (maximum pass, store pass). Every row of the segment is
-// written, zero beyond lend, so the last K-steps of each segment read zeros. All threads
-// of the block call it (it synchronises them).
-constexpr int kPackThreads = 64;
-constexpr int kPackRow = 18;   // float2 per staged unit: 16 values and 16 bytes of skew
+// Synthesis B tile images of order im, fields k0..k0+3 (one 8-row core-matrix group; rows
+// of fields >= nf are written as zeros), as f16 hi/lo pairs; one block of kPackThreads
+// threads. Rows are the degrees l = m + par + 2j of one parity; degree row j lies in f16
+// K-step j/16 of its segment, whose hi tile is image region seg(im, par)/8 + 2 (j/16) and lo
+// tile the region after it (element k16 = j % 16 of a row at byte tile_off(row, k16 / 8) +
+// 2 (k16 % 8)). Each (field, parity, re|im) row is scaled by the power of two 2^e that
+// brings its largest magnitude into [2^14, 2^15), and bsc receives 2^-(e + s), s the
+// table's exponent. Unit b = 16 consecutive degrees l = m + 16 b + q, i.e. degrees
+// j = 8b..8b+7 of each parity. 64 threads per field stage 64 units of its coefficient
+// column in shared memory (coalesced loads) and find the row maxima; then each thread
+// converts one (unit, parity, row) run of 8 values, so that 8 consecutive lanes store the
+// 8 rows' 16-byte runs as one 128-byte line (hi, then lo). Orders longer than one staging
+// pass are read twice (maximum pass, store pass). Every row of the segment is written, zero
+// beyond lend, so the last K-steps of each segment read zeros. All threads of the block call
+// it (it synchronises them).
+constexpr int kPackFields = 4;
+constexpr int kPackThreads = 64 * kPackFields;
+constexpr int kPackRow = 18;                        // float2 per staged unit: 16 values + skew
+constexpr int kPackField = 64 * kPackRow + 2;       // float2 per field buffer (+16 bytes of skew)
 __device__ __forceinline__ void pack_stage(const Args& a, const float2* c, int m, int b0, int nb, bool scaled,
-                                           float2 (*buf)[kPackRow]) {
-  for (int i = threadIdx.x; i < kPackThreads * 16; i += kPackThreads) {
+                                           float2* fb) {
+  for (int i = threadIdx.x & 63; i < 64 * 16; i += 64) {
     const int b = b0 + i / 16;
-    buf[i / 16][i % 16] = (b < nb) ? pack_value(a, c, m + 16 * b0 + i, m, scaled) : make_float2(0.f, 0.f);
+    fb[(i / 16) * kPackRow + i % 16] =
+        (c != nullptr && b < nb) ? pack_value(a, c, m + 16 * b0 + i, m, scaled) : make_float2(0.f, 0.f);
   }
 }
-__device__ __forceinline__ void pack_field(const Args& a, int im, int k) {
-  __shared__ __align__(16) float2 buf[kPackThreads][kPackRow];
-  __shared__ unsigned smx[kPackThreads / 32][4];
+__device__ __forceinline__ void pack_fields(const Args& a, int im, int k0) {
+  __shared__ __align__(16) float2 buf[kPackFields * kPackField];
+  __shared__ unsigned smx[kPackFields][2][4];   // [field][warp of the field][row (par, re|im)]
+  __shared__ float ssu[kPackFields][4];         // scale 2^e of each (field, par, re|im) row
   const PlanDev& P = a.P;
-  const int t = threadIdx.x, lane = t & 31;
+  const int t = threadIdx.x, fi = t >> 6, tt = t & 63, lane = t & 31;
   const int m = im * P.mres;
-  const int nfp = btile_nfp(a.nf), fl = k & 63;
-  const float2* c = a.cin + (long long)k * a.ld_k + coef_col(a, m);
+  const int nfp = btile_nfp(a.nf);
+  const int k = k0 + fi;
+  const float2* c = (k < a.nf) ? a.cin + (long long)k * a.ld_k + coef_col(a, m) : nullptr;
   const bool scaled = a.sc_mode || a.mf0 != 1.f || a.mf1 != 1.f;
-  const long long sg[2] = {a.seg[2 * im], a.seg[2 * im + 1]};
-  const int R[2] = {(int)(sg[1] - sg[0]), (int)(a.seg[2 * im + 2] - sg[1])};
-  const int nb = R[0] / 8;   // units; R[1] <= R[0]
-  const int npass = (nb + kPackThreads - 1) / kPackThreads;
-  unsigned mx[4] = {0u, 0u, 0u, 0u};   // rows (par, re|im)
+  const long long sg0 = a.seg[2 * im], sg1 = a.seg[2 * im + 1];
+  const int R0 = (int)(sg1 - sg0), R1 = (int)(a.seg[2 * im + 2] - sg1);
+  const int nb = R0 / 8;   // units; R1 <= R0
+  const int npass = (nb + 63) / 64;
+  float2* fb = buf + fi * kPackField;
+  unsigned mx[4] = {0u, 0u, 0u, 0u};
   for (int ps = 0; ps < npass; ++ps) {
     if (ps > 0) __syncthreads();
-    pack_stage(a, c, m, ps * kPackThreads, nb, scaled, buf);
+    pack_stage(a, c, m, ps * 64, nb, scaled, fb);
     __syncthreads();
-    const float4* u = reinterpret_cast<const float4*>(buf[t]);
+    const float4* u = reinterpret_cast<const float4*>(fb + tt * kPackRow);
 #pragma unroll
     for (int q = 0; q < 8; ++q) {   // float4 q = degrees 2q (even parity) and 2q + 1
       const float4 v = u[q];
@@ -761,65 +768,54 @@ __device__ __forceinline__ void pack_field(const Args& a, int im, int k) {
   for (int r = 0; r < 4; ++r) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) mx[r] = max(mx[r], __shfl_xor_sync(0xffffffffu, mx[r], o));
-    if (lane == 0) smx[t >> 5][r] = mx[r];
+    if (lane == 0) smx[fi][tt >> 5][r] = mx[r];
   }
   __syncthreads();
-  float su[4];
-  const int sa = f16_table_exp(P.lmax);
-#pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    unsigned v = 0u;
-#pragma unroll
-    for (int w = 0; w < kPackThreads / 32; ++w) v = max(v, smx[w][r]);
+  if (tt < 4) {
+    const int r = tt;
+    const unsigned v = max(smx[fi][0][r], smx[fi][1][r]);
     // max 2^e in [2^14, 2^15) (e at most 100: rows below 2^-86 keep the f16 subnormal steps)
     const int e = min(141 - (int)(v >> 23), 100);
-    su[r] = __int_as_float((e + 127) << 23);
-    if (t == 0) a.bsc[(2 * im + (r >> 1)) * 2 * nfp + 2 * k + (r & 1)] = __int_as_float((127 - e - sa) << 23);
+    ssu[fi][r] = __int_as_float((e + 127) << 23);
+    if (k < a.nf)
+      a.bsc[(2 * im + (r >> 1)) * 2 * nfp + 2 * k + (r & 1)] =
+          __int_as_float((127 - e - f16_table_exp(P.lmax)) << 23);
   }
+  __syncthreads();
   const long long lo = (long long)nfp * 64;   // bytes from a hi tile to its lo tile
+  const int row0 = 2 * (k0 & 63);             // first image row of the group
   for (int ps = 0; ps < npass; ++ps) {
     if (npass > 1) {   // the last staged pass is still in shared memory when npass == 1
       __syncthreads();
-      pack_stage(a, c, m, ps * kPackThreads, nb, scaled, buf);
+      pack_stage(a, c, m, ps * 64, nb, scaled, fb);
       __syncthreads();
     }
-    const int b = ps * kPackThreads + t;
-    if (b >= nb) continue;
-    const float4* u = reinterpret_cast<const float4*>(buf[t]);
-    float y[4][8];   // rows (par, re|im) x j % 8
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const float4 v = u[q];
-      y[0][q] = v.x * su[0];
-      y[1][q] = v.y * su[1];
-      y[2][q] = v.z * su[2];
-      y[3][q] = v.w * su[3];
-    }
-#pragma unroll
-    for (int par = 0; par < 2; ++par) {
-      if (8 * b >= R[par]) continue;
-      unsigned char* base = reinterpret_cast<unsigned char*>(a.bimg + (sg[par] / kK + 2 * (b / 2)) * nfp * 16 +
-                                                             (long long)(k >> 6) * 1024);
-#pragma unroll
-      for (int ri = 0; ri < 2; ++ri) {
-        const float* z = y[2 * par + ri];
-        uint4 h, l;
-        split_h2(z[0], z[1], h.x, l.x);
-        split_h2(z[2], z[3], h.y, l.y);
-        split_h2(z[4], z[5], h.z, l.z);
-        split_h2(z[6], z[7], h.w, l.w);
-        unsigned char* d = base + tile_off(2 * fl + ri, b & 1);
-        *reinterpret_cast<uint4*>(d) = h;
-        *reinterpret_cast<uint4*>(d + lo) = l;
-      }
+    // item = (unit bl of the pass, parity, row rho): 8 consecutive lanes take the 8 rows
+    for (int idx = t; idx < 64 * 2 * 8; idx += kPackThreads) {
+      const int rho = idx & 7, par = (idx >> 3) & 1, bl = idx >> 4;
+      const int b = ps * 64 + bl;
+      if (b >= nb || 8 * b >= (par ? R1 : R0)) continue;
+      const int f = rho >> 1, ri = rho & 1;
+      const float* z = reinterpret_cast<const float*>(buf + f * kPackField + bl * kPackRow) + 2 * par + ri;
+      const float su = ssu[f][2 * par + ri];
+      uint4 h, l;
+      split_h2(z[0] * su, z[4] * su, h.x, l.x);
+      split_h2(z[8] * su, z[12] * su, h.y, l.y);
+      split_h2(z[16] * su, z[20] * su, h.z, l.z);
+      split_h2(z[24] * su, z[28] * su, h.w, l.w);
+      unsigned char* d = reinterpret_cast<unsigned char*>(a.bimg + ((par ? sg1 : sg0) / kK + 2 * (b / 2)) * nfp * 16 +
+                                                          (long long)(k0 >> 6) * 1024) +
+                         tile_off(row0 + rho, b & 1);
+      *reinterpret_cast<uint4*>(d) = h;
+      *reinterpret_cast<uint4*>(d + lo) = l;
     }
   }
-  __syncthreads();   // buf and smx are reused by the next call
+  __syncthreads();   // buf, smx and ssu are reused by the next call
 }
 
-// blockIdx.x = order, blockIdx.y = field.
+// blockIdx.x = order, blockIdx.y = group of kPackFields fields.
 __global__ void __launch_bounds__(kPackThreads) mixed_pack_kernel(const __grid_constant__ Args a) {
-  pack_field(a, blockIdx.x, blockIdx.y);
+  pack_fields(a, blockIdx.x, blockIdx.y * kPackFields);
 }
 
 // Persistent packing for grouped transforms: item = (transform, order), all its fields.
@@ -830,7 +826,7 @@ __global__ void __launch_bounds__(kPackThreads) mixed_pack_group_kernel(const Ar
     const int2 it = items[i];
     if (threadIdx.x == 0) sa = targs[it.x];
     __syncthreads();
-    for (int k = 0; k < sa.nf; ++k) pack_field(sa, it.y, k);
+    for (int k0 = 0; k0 < sa.nf; k0 += kPackFields) pack_fields(sa, it.y, k0);
   }
 }
 
@@ -1110,7 +1106,7 @@ int mixed_synthesis(const shtb_plan* p, const void* alm, void* f, int nf, int lt
   a.lend = ltr;
   a.lcap = ltr;
   prof_begin(st);
-  mixed_pack_kernel<<<dim3(mlim / p->mres + 1, nf), kPackThreads, 0, st>>>(a);
+  mixed_pack_kernel<<<dim3(mlim / p->mres + 1, (nf + kPackFields - 1) / kPackFields), kPackThreads, 0, st>>>(a);
   SHTB_LAUNCHED("tc gemm B packing kernel");
   const int ntp = (p->npair + kM - 1) / kM;
   if ((rc = dispatch_gemm<0>(p, a, nf, 2 * ntp * (mlim / p->mres + 1), ntp, st))) return rc;
