@@ -214,19 +214,6 @@ __device__ __forceinline__ void tmem_ld<16>(unsigned taddr, float* v) {
 #pragma unroll
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
-template <>
-__device__ __forceinline__ void tmem_ld<32>(unsigned taddr, float* v) {
-  unsigned r[32];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n\t"
-      "tcgen05.wait::ld.sync.aligned;"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-      : "r"(taddr)
-      : "memory");
-#pragma unroll
-  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
-}
-
 __device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
@@ -294,7 +281,7 @@ struct Bars {
   unsigned long long *full, *ldfull, *rel, *acce;
   unsigned* tmem_slot;
   volatile int* abort_flag;
-  float* fsc;   // fp16x3: [kScR][N] factors 2^-(row scale + table scale) of chunk gc % kScR
+  float* fsc;   // analysis: [kScR][N] factors 2^-(row scale + table scale) of chunk gc % kScR
 };
 
 template <int N>
@@ -396,8 +383,9 @@ __device__ __forceinline__ TileInfo tile_info(const Args& a, const TileCoord& tc
 }
 
 // One thread fills the shared-memory ring, kSt chunks ahead, with one bulk copy per
-// operand and chunk (the FP32 A and B tile images; B lands in the B_hi area and is split
-// in place) when the B images of the chunk are contiguous, one per K-step for B otherwise.
+// operand and chunk (the A image, f16 hi/lo tile pairs, and the B image: f16 pairs in the
+// synthesis, FP32 in the analysis, converted in place by the splitters) when the B images
+// of the chunk are contiguous, one per K-step for B otherwise.
 template <int MODE, int N>
 __device__ __forceinline__ bool loader_tile(const Args& a, const TileCoord& tc, const TileInfo& T, unsigned char* sm,
                                             const Bars& B, unsigned c0) {
