@@ -60,8 +60,10 @@ extern "C" {
 
 /* ---- arithmetic paths ---- */
 #define SHTB_PREC_FP64  0   /* plain FP64 drop-in (relative L2 <= 1e-12 vs the FP64 CPU result) */
-#define SHTB_PREC_MIXED 1   /* Legendre contraction on tensor cores, split BF16x3 products with
-                               FP32 accumulation; nodes, weights, seeds and recurrence in FP64   */
+#define SHTB_PREC_MIXED 1   /* FP32 buffers; Legendre contraction on tensor cores as fp16x3
+                               products (f16 hi/lo splits of power-of-two-scaled operands,
+                               hi*hi + hi*lo + lo*hi) with FP32 accumulation; nodes, weights,
+                               seeds and recurrence in FP64 (relative L2 <= 1e-6 vs FP64)    */
 
 /* ---- operation ids for shtb_workspace_bytes ---- */
 #define SHTB_OP_SYNTHESIS        0
