@@ -806,15 +806,126 @@ __global__ void __launch_bounds__(kPackThreads) mixed_pack_kernel(const __grid_c
   pack_fields(a, blockIdx.x, blockIdx.y * kPackFields);
 }
 
+// The same images for one field k (the grouped transforms' packing: members of 1..8
+// fields, where 4-field blocks would mostly write padding rows); one block of kPack1Threads
+// threads. Rows are the degrees l = m + par + 2j of one parity; degree row j
+// lies in f16 K-step j/16 of its segment, whose hi tile is image region seg(im, par)/8 +
+// 2 (j/16) and lo tile the region after it (element k16 = j % 16 of a row at byte
+// tile_off(row, k16 / 8) + 2 (k16 % 8)). Each (parity, re|im) row is scaled by the power of
+// two 2^e that brings its largest magnitude into [2^14, 2^15), and bsc receives
+// 2^-(e + s), s the table's exponent. Thread work unit b = 16 consecutive degrees
+// l = m + 16 b + q: the 8 degrees j = 8b..8b+7 of each parity, i.e. one 16-byte run of each
+// of its 4 rows, stored hi and lo with one 16-byte store each. The block stages
+// kPack1Threads units at a time in shared memory (coalesced loads of the coefficient
+// column; each thread then reads its unit as 16-byte words); orders longer than one
+// staging pass are read twice (maximum pass, store pass). Every row of the segment is
+// written, zero beyond lend, so the last K-steps of each segment read zeros. All threads
+// of the block call it (it synchronises them).
+constexpr int kPack1Threads = 64;
+__device__ __forceinline__ void pack_stage1(const Args& a, const float2* c, int m, int b0, int nb, bool scaled,
+                                           float2 (*buf)[kPackRow]) {
+  for (int i = threadIdx.x; i < kPack1Threads * 16; i += kPack1Threads) {
+    const int b = b0 + i / 16;
+    buf[i / 16][i % 16] = (b < nb) ? pack_value(a, c, m + 16 * b0 + i, m, scaled) : make_float2(0.f, 0.f);
+  }
+}
+__device__ __forceinline__ void pack_field1(const Args& a, int im, int k) {
+  __shared__ __align__(16) float2 buf[kPack1Threads][kPackRow];
+  __shared__ unsigned smx[kPack1Threads / 32][4];
+  const PlanDev& P = a.P;
+  const int t = threadIdx.x, lane = t & 31;
+  const int m = im * P.mres;
+  const int nfp = btile_nfp(a.nf), fl = k & 63;
+  const float2* c = a.cin + (long long)k * a.ld_k + coef_col(a, m);
+  const bool scaled = a.sc_mode || a.mf0 != 1.f || a.mf1 != 1.f;
+  const long long sg[2] = {a.seg[2 * im], a.seg[2 * im + 1]};
+  const int R[2] = {(int)(sg[1] - sg[0]), (int)(a.seg[2 * im + 2] - sg[1])};
+  const int nb = R[0] / 8;   // units; R[1] <= R[0]
+  const int npass = (nb + kPack1Threads - 1) / kPack1Threads;
+  unsigned mx[4] = {0u, 0u, 0u, 0u};   // rows (par, re|im)
+  for (int ps = 0; ps < npass; ++ps) {
+    if (ps > 0) __syncthreads();
+    pack_stage1(a, c, m, ps * kPack1Threads, nb, scaled, buf);
+    __syncthreads();
+    const float4* u = reinterpret_cast<const float4*>(buf[t]);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {   // float4 q = degrees 2q (even parity) and 2q + 1
+      const float4 v = u[q];
+      mx[0] = max(mx[0], __float_as_uint(v.x) & 0x7fffffffu);
+      mx[1] = max(mx[1], __float_as_uint(v.y) & 0x7fffffffu);
+      mx[2] = max(mx[2], __float_as_uint(v.z) & 0x7fffffffu);
+      mx[3] = max(mx[3], __float_as_uint(v.w) & 0x7fffffffu);
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx[r] = max(mx[r], __shfl_xor_sync(0xffffffffu, mx[r], o));
+    if (lane == 0) smx[t >> 5][r] = mx[r];
+  }
+  __syncthreads();
+  float su[4];
+  const int sa = f16_table_exp(P.lmax);
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    unsigned v = 0u;
+#pragma unroll
+    for (int w = 0; w < kPack1Threads / 32; ++w) v = max(v, smx[w][r]);
+    // max 2^e in [2^14, 2^15) (e at most 100: rows below 2^-86 keep the f16 subnormal steps)
+    const int e = min(141 - (int)(v >> 23), 100);
+    su[r] = __int_as_float((e + 127) << 23);
+    if (t == 0) a.bsc[(2 * im + (r >> 1)) * 2 * nfp + 2 * k + (r & 1)] = __int_as_float((127 - e - sa) << 23);
+  }
+  const long long lo = (long long)nfp * 64;   // bytes from a hi tile to its lo tile
+  for (int ps = 0; ps < npass; ++ps) {
+    if (npass > 1) {   // the last staged pass is still in shared memory when npass == 1
+      __syncthreads();
+      pack_stage1(a, c, m, ps * kPack1Threads, nb, scaled, buf);
+      __syncthreads();
+    }
+    const int b = ps * kPack1Threads + t;
+    if (b >= nb) continue;
+    const float4* u = reinterpret_cast<const float4*>(buf[t]);
+    float y[4][8];   // rows (par, re|im) x j % 8
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const float4 v = u[q];
+      y[0][q] = v.x * su[0];
+      y[1][q] = v.y * su[1];
+      y[2][q] = v.z * su[2];
+      y[3][q] = v.w * su[3];
+    }
+#pragma unroll
+    for (int par = 0; par < 2; ++par) {
+      if (8 * b >= R[par]) continue;
+      unsigned char* base = reinterpret_cast<unsigned char*>(a.bimg + (sg[par] / kK + 2 * (b / 2)) * nfp * 16 +
+                                                             (long long)(k >> 6) * 1024);
+#pragma unroll
+      for (int ri = 0; ri < 2; ++ri) {
+        const float* z = y[2 * par + ri];
+        uint4 h, l;
+        split_h2(z[0], z[1], h.x, l.x);
+        split_h2(z[2], z[3], h.y, l.y);
+        split_h2(z[4], z[5], h.z, l.z);
+        split_h2(z[6], z[7], h.w, l.w);
+        unsigned char* d = base + tile_off(2 * fl + ri, b & 1);
+        *reinterpret_cast<uint4*>(d) = h;
+        *reinterpret_cast<uint4*>(d + lo) = l;
+      }
+    }
+  }
+  __syncthreads();   // buf and smx are reused by the next call
+}
+
 // Persistent packing for grouped transforms: item = (transform, order), all its fields.
-__global__ void __launch_bounds__(kPackThreads) mixed_pack_group_kernel(const Args* __restrict__ targs,
+__global__ void __launch_bounds__(kPack1Threads) mixed_pack_group_kernel(const Args* __restrict__ targs,
                                                                        const int2* __restrict__ items, int nitems) {
   __shared__ Args sa;
   for (int i = blockIdx.x; i < nitems; i += gridDim.x) {
     const int2 it = items[i];
     if (threadIdx.x == 0) sa = targs[it.x];
     __syncthreads();
-    for (int k0 = 0; k0 < sa.nf; k0 += kPackFields) pack_fields(sa, it.y, k0);
+    for (int k = 0; k < sa.nf; ++k) pack_field1(sa, it.y, k);
   }
 }
 
@@ -1194,7 +1305,7 @@ int mixed_group_tile_rows() { return kM; }
 
 int launch_pack_group(const void* targs, const int2* items, int nitems, int grid, cudaStream_t st) {
   if (nitems <= 0) return SHTB_OK;
-  mixed_pack_group_kernel<<<grid, kPackThreads, 0, st>>>((const Args*)targs, items, nitems);
+  mixed_pack_group_kernel<<<grid, kPack1Threads, 0, st>>>((const Args*)targs, items, nitems);
   count_launch();
   SHTB_TRY_CUDA(cudaGetLastError(), "group pack launch");
   return SHTB_OK;
