@@ -64,6 +64,22 @@ def test_null_plan_rejected():
     assert lib.shtb_plan_status(None) == _lib.SHTB_ERR_BAD_ARG
 
 
+def test_newer_entry_points_reject_null_plan():
+    """Packed-LM transforms, fused div/vort transforms and the spectral operator validate
+    their plan before anything else (no GPU needed)."""
+    lib = _lib.load()
+    for fn in (lib.shtb_synthesis_packed, lib.shtb_analysis_packed):
+        assert fn(None, None, None, 1, -1, _lib.SHTB_F32, _lib.SHTB_PREC_MIXED, None, 0, None) == _lib.SHTB_ERR_BAD_ARG
+        assert "plan is NULL" in lib.shtb_last_error().decode()
+    for fn in (lib.shtb_synthesis_divvort, lib.shtb_analysis_divvort):
+        assert fn(None, None, None, None, None, 1, -1, _lib.SHTB_F64, _lib.SHTB_PREC_FP64, None, 0,
+                  None) == _lib.SHTB_ERR_BAD_ARG
+        assert "plan is NULL" in lib.shtb_last_error().decode()
+    assert lib.shtb_spectral_op(None, _lib.SHTB_SPEC_NEG_LL, None, None, 1, _lib.SHTB_F64,
+                                None) == _lib.SHTB_ERR_BAD_ARG
+    assert "plan is NULL" in lib.shtb_last_error().decode()
+
+
 def test_group_arguments_rejected_before_gpu():
     lib = _lib.load()
     h = ctypes.c_void_p()
