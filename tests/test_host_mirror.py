@@ -50,3 +50,21 @@ def test_julia_layout_helpers():
 def test_device_markers():
     assert isinstance(sht.on_device(np.zeros(3)), sht.CPU)
     assert isinstance(sht.on_device(torch.zeros(3)), sht.CPU)
+
+
+def test_transform_arguments_rejected_before_device():
+    """The mirror raises the reference's errors for bad arguments before any device work."""
+    cfg = sht.create_gauss_config(15, 16, nlon=32)
+    alm = np.zeros((16, 16), np.complex64)
+    with pytest.raises(sht.ArgumentError, match="precision must be 'fp64' or 'mixed'"):
+        sht.synthesis(cfg, alm, precision="bf16")
+    with pytest.raises(sht.ArgumentError, match="lcap"):
+        sht.synthesis(cfg, alm, lcap=16, precision="mixed")
+    with pytest.raises(sht.ArgumentError, match="use_rfft=true implies real_output"):
+        sht.synthesis(cfg, alm, real_output=False, use_rfft=True)
+    with pytest.raises(sht.BackendUnavailableError):
+        sht.synthesis(cfg, alm, real_output=False)
+    with pytest.raises(sht.DimensionMismatch):
+        sht.synthesis(cfg, np.zeros((16, 16, 2), np.complex64), precision="mixed")
+    with pytest.raises(sht.ArgumentError, match="precision"):
+        sht.analysis_batch(cfg, np.zeros((16, 32, 2), np.float32), precision="tf32")
