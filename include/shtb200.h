@@ -107,6 +107,17 @@ size_t shtb_plan_table_bytes(const shtb_plan* plan);
  */
 int shtb_plan_status(const shtb_plan* plan);
 
+/*
+ * Test hook for failure detection (no counterpart in the reference). For this plan's
+ * mixed-precision (SHTB_PREC_MIXED) calls: wait_ns replaces the 2 s limit of the tensor-core
+ * kernels' bounded device waits (0 restores it), and skip_chunk >= 0 makes the loader of the
+ * first CTA leave that chunk's copies unissued, so the wait for it runs out. The kernel then
+ * drains its own copies and MMAs in flight, frees its tensor memory and returns;
+ * shtb_plan_status reports SHTB_ERR_TIMEOUT and the plan stays usable. skip_chunk < 0 turns
+ * the skip off.
+ */
+int shtb_plan_debug_waits(shtb_plan* plan, uint64_t wait_ns, int skip_chunk);
+
 /* Workspace bytes a call needs for nfields fields (caller allocates, >= 256-byte aligned). */
 size_t shtb_workspace_bytes(const shtb_plan* plan, int op, int nfields, int dtype, int precision);
 
@@ -212,8 +223,11 @@ int shtb_analysis_sphtor_adjoint(const shtb_plan* plan, const void* Sbar, const 
  * results as shtb_synthesis with dtype SHTB_F64 and precision SHTB_PREC_FP64.
  * Scratch: a 32 MiB array owned by the library on every GPU that loads it (until process
  * exit); calls needing more (nfields * (mmax/mres+1) * 2 * ceil(nlat/2) * 16 bytes) return
- * SHTB_ERR_WORKSPACE. The first call on each device looks up the array's device address
- * (make that first call before any stream capture). All calls share the array: calls that
+ * SHTB_ERR_WORKSPACE. shtb_plan_create looks up the array's device address on the plan's
+ * device and keeps it in the plan; with CUDA's lazy module loading that lookup is when the
+ * driver reserves the 32 MiB on that device, so the reservation (and an out-of-memory
+ * failure of it, reported by this call as SHTB_ERR_CUDA) happens at plan creation, where
+ * allocation is expected, never inside a transform. All calls share the array: calls that
  * overlap on the GPU (other streams or other host threads) race and must be serialized.
  */
 int shtb_synthesis_noalloc(const shtb_plan* plan, const void* alm, void* f, int nfields, int ltr,

@@ -22,6 +22,9 @@ void count_launch(int n = 1);
 // shtb_profile_enable); prof_begin/prof_end bracket one launch.
 void prof_begin(cudaStream_t st);
 void prof_end(const char* name, cudaStream_t st);
+// Device address, on the current device, of the static scratch array that the
+// allocation-free synthesis uses (cudaGetSymbolAddress; loads the module holding it).
+cudaError_t noalloc_scratch_address(void** out);
 
 #define SHTB_TRY_CUDA(expr, what)                                   \
   do {                                                              \
@@ -126,6 +129,14 @@ struct shtb_plan {
   const double* d_dcoef = nullptr;        // packed d(l,m) = sqrt((l^2-m^2)/(4l^2-1)), l in [m, lrec]
   std::vector<int2> htiles;
   int* d_err = nullptr;                   // device status word (bounded waits that gave up)
+  // device address of the allocation-free synthesis's static scratch array on this
+  // plan's device, resolved at plan creation (null, with the reason, if that failed)
+  void* noalloc_scratch = nullptr;
+  std::string noalloc_err;
+  // test hook of the mixed GEMMs' bounded waits (shtb_plan_debug_waits): limit in ns
+  // (0: the default 2 s) and a chunk CTA 0's loader leaves unissued (-1: none)
+  unsigned long long dbg_wait_ns = 0;
+  int dbg_skip_chunk = -1;
   // mixed-precision path: FP32 table of P_l^m grouped by (m, parity), built on first use
   std::mutex tab_mu;
   float* d_tab = nullptr;                 // synthesis tile images (start of the table allocation)

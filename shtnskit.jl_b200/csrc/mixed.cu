@@ -76,6 +76,8 @@ struct Args {
   const int2* tiles;         // analysis tiles (im, j0)
   int* err;
   int cpacked;               // coefficients in the packed LM layout (field stride ld_k = nlm)
+  unsigned long long wait_ns;  // limit of every bounded mbarrier wait (kWaitNs unless a test shortens it)
+  int skip_chunk;            // test hook: CTA 0's loader leaves this chunk's copies unissued (-1: none)
 };
 
 // First coefficient of order m of one field: dense column m, or the order's packed LM block.
@@ -111,19 +113,28 @@ __device__ __forceinline__ bool mbar_test(unsigned long long* bar, unsigned pari
       : "memory");
   return ok != 0;
 }
-// Bounded wait: false after a timeout or once another thread of the CTA gave up.
+// Bounded wait: false after a timeout (limit ns) or once another thread of the CTA gave up.
 __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, volatile int* abort_flag,
-                                          int* err) {
+                                          int* err, unsigned long long limit) {
   if (mbar_test(bar, parity)) return true;
   const unsigned long long t0 = gtimer();
   while (!mbar_test(bar, parity)) {
     if (*abort_flag) return false;
-    if (gtimer() - t0 > kWaitNs) {
+    if (gtimer() - t0 > limit) {
       *abort_flag = 1;
       atomicExch(err, 1);
       return false;
     }
   }
+  return true;
+}
+// Bounded wait used after an abort, for this thread's own asynchronous work (bulk copies it
+// issued, MMAs it committed) to land before the CTA frees TMEM and exits; it ignores the
+// abort flag. false after kWaitNs.
+__device__ __forceinline__ bool mbar_wait_drain(unsigned long long* bar, unsigned parity) {
+  const unsigned long long t0 = gtimer();
+  while (!mbar_test(bar, parity))
+    if (gtimer() - t0 > kWaitNs) return false;
   return true;
 }
 
@@ -388,7 +399,7 @@ __device__ __forceinline__ TileInfo tile_info(const Args& a, const TileCoord& tc
 // of the chunk are contiguous, one per K-step for B otherwise.
 template <int MODE, int N>
 __device__ __forceinline__ bool loader_tile(const Args& a, const TileCoord& tc, const TileInfo& T, unsigned char* sm,
-                                            const Bars& B, unsigned c0) {
+                                            const Bars& B, unsigned c0, unsigned& issued) {
   using S = Smem<N>;
   const int npair = a.P.npair;
   // A tile images: synthesis [ptile][ks] blocks of 4 KB after the segment start;
@@ -408,9 +419,11 @@ __device__ __forceinline__ bool loader_tile(const Args& a, const TileCoord& tc, 
     const int st = gc % S::kSt;
     if (gc >= S::kSt) {
       const unsigned q = gc - S::kSt;   // the chunk that last used this stage
-      if (!mbar_wait(&B.rel[q % S::kRel], (q / S::kRel) & 1, B.abort_flag, err)) return false;
+      if (!mbar_wait(&B.rel[q % S::kRel], (q / S::kRel) & 1, B.abort_flag, err, a.wait_ns)) return false;
     }
     const int k0 = c * kChunk, nk = min(kChunk, T.nks - k0);
+    issued = gc + 1;
+    if (blockIdx.x == 0 && (int)gc == a.skip_chunk) continue;   // test hook: this chunk never lands
     unsigned char* sa = sm + (size_t)st * S::kStage;
     unsigned char* sb = sa + S::kStageA;
     unsigned long long* bar = &B.ldfull[gc % S::kLd];
@@ -460,7 +473,7 @@ __device__ __forceinline__ bool splitter_tile(const Args& a, const TileInfo& T, 
     const unsigned gc = c0 + c;
     if ((int)(gc % kSG) != grp) continue;
     const int nk = min(kChunk, T.nks - c * kChunk), nk2 = (nk + 1) >> 1;
-    const bool ok = mbar_wait(&B.ldfull[gc % S::kLd], (gc / S::kLd) & 1, B.abort_flag, a.err);
+    const bool ok = mbar_wait(&B.ldfull[gc % S::kLd], (gc / S::kLd) & 1, B.abort_flag, a.err, a.wait_ns);
     if (!__all_sync(0xffffffffu, ok)) return false;
     unsigned char* Bs = sm + (size_t)(gc % S::kSt) * S::kStage + S::kStageA;
     for (int ri = 0; ri < kRpt; ++ri) {
@@ -516,7 +529,7 @@ __device__ __forceinline__ bool splitter_tile(const Args& a, const TileInfo& T, 
 // the chunk's bulk copies (synthesis) or its B conversion (analysis, which follows them).
 template <int MODE, int N>
 __device__ __forceinline__ bool mma_tile(const Args& a, const TileInfo& T, unsigned char* sm, const Bars& B,
-                                         unsigned tmem, unsigned c0) {
+                                         unsigned tmem, unsigned c0, int& committed) {
   using S = Smem<N>;
   const unsigned idesc = idesc_f16<N>();
   constexpr unsigned long long kStageDesc = S::kStage >> 4;   // descriptor address step per stage
@@ -526,10 +539,10 @@ __device__ __forceinline__ bool mma_tile(const Args& a, const TileInfo& T, unsig
   for (int c = 0; c < T.nch; ++c) {
     const unsigned gc = c0 + c;
     const int bb = gc % kAcc;
-    if (gc >= kAcc && !mbar_wait(&B.acce[bb], ((gc / kAcc) - 1) & 1, B.abort_flag, a.err)) return false;
+    if (gc >= kAcc && !mbar_wait(&B.acce[bb], ((gc / kAcc) - 1) & 1, B.abort_flag, a.err, a.wait_ns)) return false;
     const int k0 = c * kChunk, k1 = min(T.nks, k0 + kChunk);
-    const bool ready = (MODE == 0) ? mbar_wait(&B.ldfull[gc % S::kLd], (gc / S::kLd) & 1, B.abort_flag, a.err)
-                                   : mbar_wait(&B.full[gc % S::kFull], (gc / S::kFull) & 1, B.abort_flag, a.err);
+    const bool ready = (MODE == 0) ? mbar_wait(&B.ldfull[gc % S::kLd], (gc / S::kLd) & 1, B.abort_flag, a.err, a.wait_ns)
+                                   : mbar_wait(&B.full[gc % S::kFull], (gc / S::kFull) & 1, B.abort_flag, a.err, a.wait_ns);
     if (!ready) return false;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     // The accumulator rounds every addition toward zero at its current magnitude, so
@@ -547,6 +560,7 @@ __device__ __forceinline__ bool mma_tile(const Args& a, const TileInfo& T, unsig
     }
     for (int g = 0; g < nk2; ++g) mma_f16_ss(dH, as + 2 * g * akDesc, bs + 2 * g * bkDesc, idesc, 1u);
     mma_commit(&B.rel[gc % S::kRel]);
+    committed = (int)gc;
   }
   return true;
 }
@@ -575,9 +589,10 @@ __device__ __forceinline__ bool promo_tile(const Args& a, const TileCoord& tc, c
     const int bb = gc % kAcc;
     // analysis: the chunk's column scales, written by the splitters before they arrived
     // on full (complete long before the chunk's MMAs are)
-    if (MODE == 1 && ok) ok = mbar_wait(&B.full[gc % S::kFull], (gc / S::kFull) & 1, B.abort_flag, a.err);
-    if (ok) ok = mbar_wait(&B.rel[gc % S::kRel], (gc / S::kRel) & 1, B.abort_flag, a.err);
+    if (MODE == 1 && ok) ok = mbar_wait(&B.full[gc % S::kFull], (gc / S::kFull) & 1, B.abort_flag, a.err, a.wait_ns);
+    if (ok) ok = mbar_wait(&B.rel[gc % S::kRel], (gc / S::kRel) & 1, B.abort_flag, a.err, a.wait_ns);
     ok = __all_sync(0xffffffffu, ok);   // warp-uniform: the TMEM loads are warp-collective
+    if (!ok) return false;              // the chunk's MMAs may not have run: leave TMEM alone
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const unsigned dH = tmem + lane_base + bb * N + h * (N / 2);
     const float4* fs = reinterpret_cast<const float4*>(B.fsc + (gc % kScR) * N + h * (N / 2));
@@ -602,7 +617,6 @@ __device__ __forceinline__ bool promo_tile(const Args& a, const TileCoord& tc, c
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncwarp();
     if (lane == 0) mbar_arrive(&B.acce[bb]);
-    if (!ok) return false;
   }
   // Every Args field and the scale factor are read before the first store: the stores
   // go through generic pointers, after which the compiler would reload them.
@@ -658,24 +672,42 @@ __device__ __forceinline__ void gemm_tiles(const Src& src, unsigned char* sm, co
   // the synthesis B images arrive converted: its splitter warps have no work
   const bool loader = (warp == kLoaderWarp && lane == 0), splitter = (MODE == 1 && warp < kSW),
              mma = (warp == kMmaWarp && lane == 0), promo = (warp >= kPromo0 && warp < kPromo0 + 8);
-  if (!(loader || splitter || mma || promo)) return;
+  const bool role = loader || splitter || mma || promo;
   unsigned c0 = 0;
-  for (int i = blockIdx.x; i < src.n; i += gridDim.x) {
+  unsigned issued = 0;   // loader: chunks 0 .. issued-1 had their copies issued (all but a skipped one)
+  int committed = -1;    // MMA issuer: last chunk committed
+  int skip = -1;
+  for (int i = blockIdx.x; role && i < src.n; i += gridDim.x) {
     const Args& a = src.args(i);
     const TileCoord tc = src.coord(i);
     const TileInfo T = tile_info<MODE>(a, tc);
+    if (blockIdx.x == 0) skip = a.skip_chunk;
     bool ok;
     if (loader)
-      ok = loader_tile<MODE, N>(a, tc, T, sm, B, c0);
+      ok = loader_tile<MODE, N>(a, tc, T, sm, B, c0, issued);
     else if (splitter)
       ok = splitter_tile<MODE, N>(a, T, sm, B, c0);
     else if (mma)
-      ok = mma_tile<MODE, N>(a, T, sm, B, tmem, c0);
+      ok = mma_tile<MODE, N>(a, T, sm, B, tmem, c0, committed);
     else
       ok = promo_tile<MODE, N>(a, tc, T, B, tmem, c0);
     if (!ok) break;
     if (promo) src.tile_done(i);
     c0 += T.nch;
+  }
+  // Every thread of the CTA: after this barrier the abort flag is final.
+  __syncthreads();
+  if (!*B.abort_flag) return;
+  // After an abort nothing of this CTA's may still run asynchronously when it frees TMEM
+  // and exits. The loader's copies in flight are among its last kSt chunks (it issues
+  // chunk gc only after chunk gc - kSt was consumed), each completing on its own copy
+  // barrier (a ring of 2 kSt); the MMA issuer's last commit completes after all its MMAs.
+  using S = Smem<N>;
+  if (loader) {
+    for (unsigned gc = issued > (unsigned)S::kSt ? issued - S::kSt : 0u; gc < issued; ++gc)
+      if ((int)gc != skip) mbar_wait_drain(&B.ldfull[gc % S::kLd], (gc / S::kLd) & 1);
+  } else if (mma && committed >= 0) {
+    mbar_wait_drain(&B.rel[committed % S::kRel], (committed / S::kRel) & 1);
   }
 }
 
@@ -1183,6 +1215,8 @@ static Args base_args(const shtb_plan* p) {
   a.sc = p->d_scale;
   a.err = p->d_err;
   a.mf0 = a.mf1 = 1.f;
+  a.wait_ns = p->dbg_wait_ns ? p->dbg_wait_ns : kWaitNs;
+  a.skip_chunk = p->dbg_skip_chunk;
   return a;
 }
 
@@ -1292,6 +1326,8 @@ void mixed_fill_args(const shtb_plan* p, int mode, const void* in, void* out, in
   }
   a.nf = nf;
   a.lend = a.lcap = p->lmax;
+  a.wait_ns = kWaitNs;   // the test hook of shtb_plan_debug_waits applies to single-plan calls only
+  a.skip_chunk = -1;
   std::memcpy(host_args, &a, sizeof(Args));
 }
 

@@ -8,8 +8,6 @@
 // pass only their input coefficients and output grid; the Fourier scratch between
 // the Legendre and FFT stages lives in `g_noalloc_scratch` below, a static device
 // array that exists on every GPU that loads this library until the process exits.
-#include <mutex>
-
 #include "kernels.cuh"
 
 namespace shtb {
@@ -20,27 +18,15 @@ constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-// Device address of g_noalloc_scratch per device, looked up once with that device current.
-// The host-side name g_noalloc_scratch is only a stand-in for the symbol; it must never be
-// passed to a kernel.
-constexpr int kMaxDevices = 64;
-static void* g_scratch_dev[kMaxDevices] = {nullptr};
-static std::mutex g_scratch_mu;
-
-static int scratch_for_current_device(void** out) {
-  int dev = -1;
-  SHTB_TRY_CUDA(cudaGetDevice(&dev), "noalloc: cudaGetDevice");
-  if (dev < 0 || dev >= kMaxDevices) return set_error(SHTB_ERR_UNSUPPORTED, "noalloc: device index out of range");
-  std::lock_guard<std::mutex> lk(g_scratch_mu);
-  if (!g_scratch_dev[dev]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || p == nullptr)
-      return set_error(SHTB_ERR_CUDA, std::string("noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
-    g_scratch_dev[dev] = p;
-  }
-  *out = g_scratch_dev[dev];
-  return SHTB_OK;
+// The host-side name g_noalloc_scratch only stands in for the symbol: passing it to a
+// kernel would hand the GPU a host address. Its device address is looked up here, with
+// the plan's device current, when a plan is created (shtb_plan_create), and kept in the
+// plan. Looking it up loads this file's module, which is when the driver reserves the
+// array on that device; doing it at plan creation keeps that reservation (and any
+// failure of it) out of the transform calls.
+cudaError_t noalloc_scratch_address(void** out) {
+  *out = nullptr;
+  return cudaGetSymbolAddress(out, g_noalloc_scratch);
 }
 
 }  // namespace shtb
@@ -65,9 +51,11 @@ extern "C" int shtb_synthesis_noalloc(const shtb_plan* p, const void* alm, void*
                                              " bytes of scratch for this plan and nfields; its static scratch holds " +
                                              std::to_string(kNoAllocScratchBytes) +
                                              " bytes (use shtb_synthesis with a caller workspace)");
-  void* W = nullptr;
-  int rc = scratch_for_current_device(&W);
-  if (rc) return rc;
+  void* W = p->noalloc_scratch;
+  if (!W)
+    return set_error(SHTB_ERR_CUDA, "shtb_synthesis_noalloc: the static scratch was not available when the plan "
+                                    "was created: " + p->noalloc_err);
+  int rc = SHTB_OK;
   // The Legendre stage writes every scratch entry the FFT stage reads, so nothing is cleared.
   cudaStream_t st = (cudaStream_t)stream;
   const int mlim = std::min(p->mmax, ltr);

@@ -429,6 +429,14 @@ extern "C" int shtb_plan_create(shtb_plan** out, int lmax, int mmax, int mres, i
     delete p;
     return set_error(SHTB_ERR_CUDA, std::string("plan setup kernel: ") + cudaGetErrorString(ce));
   }
+  // the allocation-free synthesis's scratch on this device (shtb_synthesis_noalloc); a
+  // failure here only disables that entry point
+  ce = noalloc_scratch_address(&p->noalloc_scratch);
+  if (ce != cudaSuccess || !p->noalloc_scratch) {
+    p->noalloc_scratch = nullptr;
+    p->noalloc_err = cudaGetErrorString(ce);
+    cudaGetLastError();
+  }
   *out = p;
   return SHTB_OK;
 }
@@ -459,6 +467,18 @@ extern "C" int shtb_plan_status(const shtb_plan* p) {
     cudaMemset(p->d_err, 0, sizeof(int));
     return set_error(SHTB_ERR_TIMEOUT, "a device wait exceeded its time limit; results of the affected call are invalid");
   }
+  return SHTB_OK;
+}
+
+// Test hook for the failure path of the bounded device waits: shortens the mixed GEMM
+// kernels' wait limit and makes CTA 0's loader leave one chunk's copies unissued, so the
+// wait for that chunk runs out, the CTA drains its own copies and MMAs, frees TMEM and
+// exits, and shtb_plan_status reports SHTB_ERR_TIMEOUT. Nothing faults or hangs.
+extern "C" int shtb_plan_debug_waits(shtb_plan* p, uint64_t wait_ns, int skip_chunk) {
+  if (!p) return set_error(SHTB_ERR_BAD_ARG, "plan is NULL");
+  if (wait_ns > 10000000000ull) return set_error(SHTB_ERR_BAD_ARG, "wait_ns must be <= 10 s");
+  p->dbg_wait_ns = wait_ns;
+  p->dbg_skip_chunk = skip_chunk < 0 ? -1 : skip_chunk;
   return SHTB_OK;
 }
 

@@ -68,6 +68,7 @@ SIGNATURES = {
     "shtb_plan_destroy": (_I, [_P]),
     "shtb_plan_table_bytes": (_SZ, [_P]),
     "shtb_plan_status": (_I, [_P]),
+    "shtb_plan_debug_waits": (_I, [_P, ctypes.c_uint64, _I]),
     "shtb_workspace_bytes": (_SZ, [_P, _I, _I, _I, _I]),
     "shtb_synthesis": (_I, [_P, _P, _P, _I, _I, _I, _I, _P, _SZ, _P]),
     "shtb_analysis": (_I, [_P, _P, _P, _I, _I, _I, _I, _P, _SZ, _P]),

@@ -7,9 +7,9 @@ Coefficients are in SHTns packed LM order (``src/layout.jl:143-150``) and are
 unpacked here to the dense ``(lmax+1, mmax+1[, nfields])`` layout. Fields keep
 the ``(nlat, nphi[, nfields])`` shape of the Julia arrays.
 
-Usage (needs the reference checkout, read-only)::
+Usage (needs the reference checkout, read-only; its root is a required argument)::
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <path to the SHTnsKit.jl checkout>
 
 The output is committed so that tests run without the reference present.
 """
@@ -91,4 +91,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python tests/golden/make_golden.py <path to the SHTnsKit.jl checkout>")
+    main(sys.argv[1])

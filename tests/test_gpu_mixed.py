@@ -66,17 +66,31 @@ def test_mixed_lcap():
 
 
 def test_mixed_config3_size():
-    """lmax=1023, 1024x2048, 64 fields: mixed roundtrip against the FP64 GPU path at <= 1e-6."""
+    """lmax=1023, 1024x2048, 64 fields: the mixed roundtrip against the FP64 oracle (the C
+    restatement of the reference CPU path) on two of the 64 fields, grid and coefficients,
+    and against the FP64 GPU path on all 64, each at <= 1e-6."""
+    from oracle import c_oracle as co
+
     cfg = sht.create_gauss_config(1023, 1024, nlon=2048)
+    ocfg = so.create_gauss_config(1023, 1024, nlon=2048)
     a = rand_alm(1023, 1023, 64, seed=7).astype(np.complex64)
     a64 = a.astype(np.complex128)
     f32 = sht.synthesis_batch(cfg, a, precision="mixed")
+    f32h = host(f32)
+    pick = [0, 37]
+    f_ref = co.synthesis_batch(ocfg, a64[:, :, pick])
+    for i, k in enumerate(pick):
+        assert rel_l2(f32h[:, :, k], f_ref[:, :, i]) <= TOLMX, f"synthesis field {k} vs oracle"
     f64 = sht.synthesis_batch(cfg, a64)
-    assert rel_l2(host(f32), host(f64)) <= TOLMX
+    assert rel_l2(f32h, host(f64)) <= TOLMX
     b32 = sht.analysis_batch(cfg, f32, precision="mixed")
+    b32h = host(b32)
+    b_ref = co.analysis_batch(ocfg, f32h[:, :, pick].astype(np.float64))
+    for i, k in enumerate(pick):
+        assert rel_l2(b32h[:, :, k], b_ref[:, :, i]) <= TOLMX, f"analysis field {k} vs oracle"
     b64 = sht.analysis_batch(cfg, f64)
-    assert rel_l2(host(b32), host(b64)) <= TOLMX
-    assert rel_l2(host(b32), a64) <= TOLMX
+    assert rel_l2(b32h, host(b64)) <= TOLMX
+    assert rel_l2(b32h, a64) <= TOLMX
     cfg.plan(0).status()
 
 

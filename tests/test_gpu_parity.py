@@ -143,6 +143,42 @@ def test_lcap_truncation(ltr):
         assert rel_l2(host(s), rs) <= TOL64 and rel_l2(host(t), rt2) <= TOL64
 
 
+@pytest.mark.parametrize("case", [dict(lmax=31, nlat=32, nlon=64), dict(lmax=20, nlat=23, nlon=45, mmax=15)],
+                         ids=["l31", "l20-odd"])
+def test_phi_scale_quad_vs_oracle(case, monkeypatch):
+    """SHTNSKIT_PHI_SCALE=quad (src/SHTnsKit.jl:128-177): synthesis bins scaled by nlon/(2 pi)
+    instead of nlon, analysis by 4 pi^2/nlon instead of 2 pi/nlon (the plan's two scalars);
+    scalar, sphtor and mixed paths against the oracle built with phi_scale="quad"."""
+    c = dict(case)
+    lmax, nlat = c.pop("lmax"), c.pop("nlat")
+    monkeypatch.setenv("SHTNSKIT_PHI_SCALE", "quad")
+    cfg = sht.create_gauss_config(lmax, nlat, **c)
+    ocfg = so.create_gauss_config(lmax, nlat, phi_scale="quad", **c)
+    assert abs(cfg.phi_inv_scale() - ocfg.phi_inv_scale()) == 0.0
+    assert abs(ocfg.phi_inv_scale() - cfg.nlon) > 1.0          # really a non-dft scale
+    a = rand_alm(lmax, cfg.mmax, 3, seed=61)
+    f_ref = so.synthesis_batch(ocfg, a)
+    f = host(sht.synthesis_batch(cfg, a))
+    assert rel_l2(f, f_ref) <= TOL64
+    g = np.random.default_rng(62).standard_normal((nlat, cfg.nlon, 3))
+    assert rel_l2(host(sht.analysis_batch(cfg, g)), so.analysis_batch(ocfg, g)) <= TOL64
+    # quad synthesis then quad analysis is still the identity on band-limited input
+    assert rel_l2(host(sht.analysis_batch(cfg, f)), a) <= 1e-12
+    S = rand_alm(lmax, cfg.mmax, seed=63, power=1.5, lmin=1)
+    T = rand_alm(lmax, cfg.mmax, seed=64, power=1.5, lmin=1)
+    vt, vp = sht.synthesis_sphtor(cfg, S, T)
+    rt, rp = so.synthesis_sphtor(ocfg, S, T)
+    assert rel_l2(host(vt), rt) <= TOL64 and rel_l2(host(vp), rp) <= TOL64
+    s, t = sht.analysis_sphtor(cfg, rt, rp)
+    rs, rtt = so.analysis_sphtor(ocfg, rt, rp)
+    assert rel_l2(host(s), rs) <= TOL64 and rel_l2(host(t), rtt) <= TOL64
+    a32 = a.astype(np.complex64)
+    f32 = host(sht.synthesis_batch(cfg, a32, precision="mixed"))
+    assert rel_l2(f32, so.synthesis_batch(ocfg, a32.astype(np.complex128))) <= 1e-6
+    b32 = host(sht.analysis_batch(cfg, g.astype(np.float32), precision="mixed"))
+    assert rel_l2(b32, so.analysis_batch(ocfg, g.astype(np.float32).astype(np.float64))) <= 1e-6
+
+
 def test_config2_fp64_parity():
     """lmax=511, 512x1024, 16 scalar fields + one sphtor pair, roundtrip vs the oracle at 1e-12."""
     cfg, ocfg = both(511, 512, nlon=1024)
