@@ -40,8 +40,11 @@ cudaError_t noalloc_scratch_address(void** out);
     if (_rc != SHTB_OK) return _rc;                                 \
   } while (0)
 
-// Rows of one analysis tile (degree range sharing one recurrence checkpoint).
-constexpr int kTileRows = 64;
+// Degrees of one FP64 analysis tile (64 of each parity).
+constexpr int kAnaTile = 128;
+// Largest checkpoint table the plan keeps (bytes); the spacing grows from 16 degrees
+// until the table fits.
+constexpr size_t kCkptBudget = size_t(2) << 30;
 
 // ---------------------------------------------------------------------------
 // device view of a plan (passed by value to kernels)
@@ -56,9 +59,14 @@ struct PlanDev {
   const double* cfac;      // packed: P_l = c_l r_l
   const int* l0;           // [nm*npair] first significant degree per (im, pair)
   const double2* r01;      // [nm*npair] (r_{l0}, r_{l0+1})
-  const double2* ckpt;     // [ntiles*npair] state (r_{t0-1}, r_{t0-2}) before tile row t0
-  const int2* tiles;       // [ntiles] (im, t0)
-  int ntiles;
+  // recurrence checkpoints every ckstep degrees: entry (ckbase[im] + k) * npair + pair holds
+  // the state (r_{t-1}, r_{t-2}) before degree t = m + k * ckstep
+  const double2* ckpt;
+  const int* ckbase;       // [nm]
+  int ckstep;              // 16, 32, 64 or 128 (a divisor of kAnaTile)
+  // FP64 analysis tiles of kAnaTile degrees: (im, t0, checkpoint index of t0, 0)
+  const int4* atiles;
+  int natiles;
 };
 
 // FFT description for nlon
@@ -127,7 +135,6 @@ struct shtb_plan {
   const double2* d_twp64 = nullptr;       // per-pass twiddles: pass s, factor q (1..r-1), index j < span:
   const float2* d_twp32 = nullptr;        //   entry twoff[s] + (q-1)*span + j = exp(-2 pi i j q / Ns)
   const double* d_dcoef = nullptr;        // packed d(l,m) = sqrt((l^2-m^2)/(4l^2-1)), l in [m, lrec]
-  std::vector<int2> htiles;
   int* d_err = nullptr;                   // device status word (bounded waits that gave up)
   // device address of the allocation-free synthesis's static scratch array on this
   // plan's device, resolved at plan creation (null, with the reason, if that failed)

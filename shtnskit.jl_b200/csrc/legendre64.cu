@@ -1,29 +1,38 @@
-// legendre64.cu — FP64 associated-Legendre contraction kernels.
+// legendre64.cu — FP64 associated-Legendre contraction kernels on the FP64 tensor cores.
 //
 // Both directions work per order m on latitude PAIRS (i, nlat-1-i) folded by
 // equatorial symmetry: P_l^m(-x) = (-1)^(l-m) P_l^m(x), so every contraction is
-// split into degrees of even (E) and odd (O) parity l-m.
+// split into degrees of even (E) and odd (O) parity l-m. Per order and parity each
+// direction is a dense GEMM whose P operand is regenerated on the fly:
+//   synthesis  W[pair, col] = sum_l P_l(x_pair) a[l, col]     (K = degrees)
+//   analysis   a[l, col]    = sum_pair P_l(x_pair) W[pair, col] (K = latitude pairs)
+// with col = (field, re|im).
 //
-// P_l^m is never stored: it is regenerated by the c-scaled three-term recurrence
+// P_l^m is never stored in global memory: four producer warps per CTA regenerate the
+// panels of the coming K chunks into a ring of shared-memory stages with the c-scaled
+// three-term recurrence
 //   r_l = alpha_l x r_{l-1} - r_{l-2},   P_l^m = c_l r_l
-// (one DMUL + one DFMA per value), started from per-(m, latitude) records that
-// already carry the reference's extended-range sectoral seed. The c_l factors
-// are folded into the coefficients on the way in (synthesis) or out (analysis).
+// (one DMUL + one DFMA per value), started from per-(m, pair) records that carry the
+// reference's extended-range sectoral seed (values below 2^-480 are zero until the
+// record's first degree l0) and, inside the degree range, from the plan's recurrence
+// checkpoints (every ckstep degrees), so the panel of a chunk is many short independent
+// chains rather than one long one; they fill the same stage with the chunk's coefficient
+// or Fourier panel by cp.async. Eight consumer warps multiply each stage with FP64 MMAs
+// (mma.sync m16n8k4 .f64: 512 FMAs per instruction, the DFMA units' full rate at an
+// eighth of the issue slots of DFMA code), operands from shared memory, accumulators in
+// registers. Stages are handed over on mbarriers (full: panels written and copies landed;
+// empty: every consumer warp done), so the producers run up to a ring's depth ahead and
+// their latency-bound recurrence, which shares the FP64 pipe with the MMAs, never holds
+// the consumers at a CTA-wide barrier. Every wait is bounded (pipe.cuh).
 //
-// Synthesis (leg_syn64_kernel): each thread owns TP latitude pairs and walks l
-// with the recurrence in registers; a CTA stages FB fields of coefficients per
-// 32-degree chunk in shared memory (read back as broadcasts) and accumulates
-// E and O sums for every field.
-//
-// Analysis (leg_ana64_kernel): a CTA owns a 64-degree tile of one m and a block
-// of columns (field re/im parts) and reduces over all latitude pairs in chunks
-// of 32. Warp 0 regenerates the P panel of the next chunk from the tile's
-// recurrence checkpoint while the CTA multiplies the current one: a
-// register-tiled FP64 GEMM (4 E rows + 4 O rows by TC columns per thread) fed
-// from double-buffered shared memory (cp.async for the Fourier panel).
+// Per-(l, m) multipliers (c_l, normalization, phi scales) are folded into the P panel
+// (synthesis) or applied at the store (analysis). Chunks whose P values are all zero
+// (every pair of the chunk still below its record's first degree, near the poles at
+// high m) are skipped: adding their zeros changes nothing.
 #include <climits>
 
 #include "kernels.cuh"
+#include "pipe.cuh"
 
 namespace shtb {
 
@@ -37,352 +46,452 @@ __device__ __forceinline__ double factor_at(const PlanDev& P, const Factors& F, 
   return s;
 }
 
+// D (16x8) += A (16x4, row-major) B (4x8, column-major), FP64. Fragments per lane
+// (g = lane / 4, t = lane % 4): a0 = A[g][t], a1 = A[g + 8][t]; b0 = B[t][g];
+// d0, d1 = D[g][2t], D[g][2t + 1]; d2, d3 = D[g + 8][2t], D[g + 8][2t + 1].
+__device__ __forceinline__ void dmma_16x8x4(double (&d)[4], double a0, double a1, double b0) {
+  asm("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a0), "d"(a1), "d"(b0));
+}
+
+constexpr int kConsumerWarps = 8;
+
+// Consumer warp layout shared by both directions: per parity an output tile of 64 rows
+// by NCOL columns, split over kConsumerWarps / 2 warps as RG row groups x CG column
+// groups; a warp holds MT x NT fragments of 16 x 8.
+template <int NCOL>
+struct WarpTile {
+  static constexpr int WPP = kConsumerWarps / 2;   // warps per parity
+  static constexpr int RG = NCOL >= 64 ? 2 : 4, CG = WPP / RG;
+  static constexpr int MT = 64 / RG / 16, NT = NCOL / CG / 8;
+  static constexpr int NF = NCOL / 2;   // fields per CTA
+  static_assert(MT >= 1 && NT >= 1 && RG * CG == WPP, "warp tile");
+};
+
+constexpr int kProducerWarps = 4;   // one per SM sub-partition, so the recurrence's FP64 work
+                                    // spreads over all four FP64 pipes
+constexpr int kLegThreads = 32 * (kConsumerWarps + kProducerWarps);
+
 // ---------------------------------------------------------------------------
-// synthesis
+// synthesis: CTA = (64 pairs, order m, NCOL/2 fields), K chunks of 16 degrees
 // ---------------------------------------------------------------------------
-template <int FB, int TP, int NT>
-__global__ void __launch_bounds__(NT) leg_syn64_kernel(PlanDev P, CoefSrc src, Factors F, double2* __restrict__ W,
-                                                       int nf, int row_end) {
-  constexpr int LC = 32;
-  __shared__ double2 As[LC][FB];
-  __shared__ double alph[LC];
-  __shared__ int smin;
+constexpr int kSynPairs = 64;
+constexpr int kSynDeg = 16;                    // degrees per chunk (8 per parity)
+constexpr int kSynPS = kSynPairs + 4;          // P panel row stride (doubles), = 4 mod 16
+constexpr int kSynCS = 2 * (kSynDeg / 2) + 8;  // coefficient field stride (doubles), = 8 mod 16
+constexpr int kSynStages = 4;
+
+template <int NCOL>
+struct SynSmem {
+  static constexpr int NF = WarpTile<NCOL>::NF;
+  static constexpr int PBUF = 2 * (kSynDeg / 2) * kSynPS;   // [parity][8 degrees][pairs]
+  static constexpr int CBUF = 2 * NF * kSynCS;              // [parity][field][8 degrees x re|im]
+  static constexpr int STAGE = PBUF + CBUF;                 // doubles
+  static constexpr int BAR = kSynStages * STAGE;            // then full[S], empty[S], flags
+  // stages, barriers, abort flag and two pair minima, then alpha and the folded factor of
+  // every degree m..lend
+  static size_t bytes(int ndeg) { return (size_t)BAR * 8 + 2 * kSynStages * 8 + 16 + (size_t)2 * ndeg * 8; }
+};
+
+template <int NCOL>
+__global__ void __launch_bounds__(kLegThreads, 1)
+    leg_syn64_kernel(PlanDev P, CoefSrc src, Factors F, double2* __restrict__ W, int nf, int row_end, int* err) {
+  using WT = WarpTile<NCOL>;
+  using SM = SynSmem<NCOL>;
+  constexpr int NF = WT::NF, S = kSynStages;
+  extern __shared__ __align__(16) double sm[];
+  unsigned long long* full = reinterpret_cast<unsigned long long*>(sm + SM::BAR);
+  unsigned long long* empty = full + S;
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(empty + S);
+  int* sLmin = reinterpret_cast<int*>(empty + S) + 1;
+  double* sAl = reinterpret_cast<double*>(empty + S + 2);
   const int im = blockIdx.y, m = im * P.mres;
-  const int kb = blockIdx.z * FB;
-  const int pb = blockIdx.x * (TP * NT);
+  const int p0 = blockIdx.x * kSynPairs;
+  const int kb = blockIdx.z * NF;
   const int npair = P.npair;
   const long long poff = P.off[im];
-  double xt[TP], ra[TP], rb[TP], r0[TP], r1[TP];
-  int l0[TP];
-  int lmin = INT_MAX;
-#pragma unroll
-  for (int t = 0; t < TP; ++t) {
-    const int p = pb + t * NT + threadIdx.x;
-    if (p < npair) {
-      xt[t] = P.x[p];
-      l0[t] = P.l0[(size_t)im * npair + p];
-      const double2 v = P.r01[(size_t)im * npair + p];
-      r0[t] = v.x;
-      r1[t] = v.y;
-    } else {
-      xt[t] = 0.0;
-      l0[t] = INT_MAX / 2;
-      r0[t] = r1[t] = 0.0;
-    }
-    ra[t] = rb[t] = 0.0;
-    lmin = min(lmin, l0[t]);
-  }
-  for (int o = 16; o > 0; o >>= 1) lmin = min(lmin, __shfl_xor_sync(0xffffffffu, lmin, o));
-  if (threadIdx.x == 0) smin = INT_MAX;
-  __syncthreads();
-  if ((threadIdx.x & 31) == 0) atomicMin(&smin, lmin);
-  __syncthreads();
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const bool producer = warp >= kConsumerWarps;
   const int lend = min(row_end, P.lrec);
-  int lbeg = max(smin, m);
-  lbeg -= (lbeg - m) & 1;
-  double2 accE[TP][FB], accO[TP][FB];
-#pragma unroll
-  for (int t = 0; t < TP; ++t)
-#pragma unroll
-    for (int f = 0; f < FB; ++f) {
-      accE[t][f] = make_double2(0.0, 0.0);
-      accO[t][f] = make_double2(0.0, 0.0);
+  const int ndeg = max(lend - m + 1, 0);
+  double* sFa = sAl + ndeg;
+
+  if (tid == 0) {
+    for (int q = 0; q < S; ++q) {
+      pipe_bar_init(&full[q], 64);   // one group of two producer warps fills a stage
+      pipe_bar_init(&empty[q], kConsumerWarps);
     }
+    *abort_flag = 0;
+    pipe_bar_init_fence();
+  }
+  for (int i = tid; i < ndeg; i += kLegThreads) {
+    sAl[i] = P.alpha[poff + i];
+    sFa[i] = factor_at(P, F, poff, m + i, m);
+  }
+  // producer state: the producer warps form two groups that fill alternate chunks; in
+  // each group, thread q = 32 (w % 2) + lane takes pair p0 + q
+  double px = 0.0, pr0 = 0.0, pr1 = 0.0;
+  int pl0 = INT_MAX / 2;
+  const int pw = warp - kConsumerWarps, pgroup = pw >> 1, pq = 32 * (pw & 1) + lane;
+  const int pp = p0 + pq;
+  if (producer) {
+    if (pp < npair) {
+      px = P.x[pp];
+      pl0 = P.l0[(size_t)im * npair + pp];
+      const double2 v = P.r01[(size_t)im * npair + pp];
+      pr0 = v.x;
+      pr1 = v.y;
+    }
+    int mn = pl0;
+    for (int o = 16; o > 0; o >>= 1) mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    if (lane == 0 && pw < 2) sLmin[pw] = mn;
+  }
+  __syncthreads();
+  const int lmin = max(min(sLmin[0], sLmin[1]), m);
+  // chunks start at degrees m + 16 k (even l - m first)
+  const int lbeg = m + ((lmin - m) / kSynDeg) * kSynDeg;
+  const int nchunks = (lend >= lbeg) ? (lend - lbeg) / kSynDeg + 1 : 0;
   const long long cbase = src.packed == 1 ? (poff - m)
                           : src.packed == 2 ? lm_base(P.lmax, P.mres, m) : (long long)m * src.ld_m;
-  for (int lc = lbeg; lc <= lend; lc += LC) {
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < LC * FB; idx += NT) {
-      const int j = idx % LC, f = idx / LC, l = lc + j, k = kb + f;
-      double2 v = make_double2(0.0, 0.0);
-      if (l <= lend && k < nf) {
-        v = src.ptr[(long long)k * src.ld_k + cbase + l];
-        const double s = factor_at(P, F, poff, l, m);
-        v.x *= s;
-        v.y *= s;
+
+  if (producer) {
+    for (int c = pgroup; c < nchunks; c += 2) {
+      const int st = c % S;
+      if (c >= S && !pipe_wait(&empty[st], ((c / S) - 1) & 1, abort_flag, err)) break;
+      double* Pn = sm + st * SM::STAGE;
+      double* C = Pn + SM::PBUF;
+      const int lc = lbeg + c * kSynDeg;
+      // coefficients: 8 consecutive threads fill one (parity, field) row of 8 degrees
+      for (int idx = pq; idx < NF * kSynDeg; idx += 64) {
+        const int s = 2 * (idx & 7) + ((idx >> 3) & 1), fl = idx / kSynDeg;
+        const int l = lc + s, kf = kb + fl;
+        const bool ok = (l <= lend) && (kf < nf);
+        const double2* gp = ok ? src.ptr + (long long)kf * src.ld_k + cbase + l : src.ptr;
+        pipe_cp16(C + ((s & 1) * NF + fl) * kSynCS + 2 * (s >> 1), gp, ok ? 16u : 0u);
       }
-      As[j][f] = v;
-    }
-    for (int idx = threadIdx.x; idx < LC; idx += NT) {
-      const int l = lc + idx;
-      alph[idx] = (l <= lend) ? P.alpha[poff + (l - m)] : 0.0;
-    }
-    __syncthreads();
-    const int nr = min(LC, lend - lc + 1);
-#define SYN_STEP(JJ, ACC)                                                        \
-  {                                                                              \
-    const int l = lc + (JJ);                                                     \
-    const double a = alph[(JJ)];                                                 \
-    _Pragma("unroll") for (int t = 0; t < TP; ++t) {                             \
-      double r = fma(a * xt[t], ra[t], -rb[t]);                                  \
-      r = (l == l0[t]) ? r0[t] : r;                                              \
-      r = (l == l0[t] + 1) ? r1[t] : r;                                          \
-      rb[t] = ra[t];                                                             \
-      ra[t] = r;                                                                 \
-    }                                                                            \
-    _Pragma("unroll") for (int f = 0; f < FB; ++f) {                             \
-      const double2 c = As[(JJ)][f];                                             \
-      _Pragma("unroll") for (int t = 0; t < TP; ++t) {                           \
-        ACC[t][f].x = fma(ra[t], c.x, ACC[t][f].x);                              \
-        ACC[t][f].y = fma(ra[t], c.y, ACC[t][f].y);                              \
-      }                                                                          \
-    }                                                                            \
-  }
-#pragma unroll 2
-    for (int j = 0; j < nr; j += 2) {
-      SYN_STEP(j, accE);
-      SYN_STEP(j + 1, accO);
-    }
-#undef SYN_STEP
-  }
+      pipe_arrive_cp_async(&full[st]);
+      // P panel column of pair pp, the per-degree factors folded in (zero past lend): the
+      // chain starts at the checkpoint at or below lc
+      const int ks = (lc - m) / P.ckstep, lk = m + ks * P.ckstep;
+      double ra = 0.0, rb = 0.0;
+      if (pp < npair) {
+        const double2 v = P.ckpt[(size_t)(P.ckbase[im] + ks) * npair + pp];
+        ra = v.x;
+        rb = v.y;
+      }
+      for (int l = lk; l < lc; ++l) {   // only when the checkpoints are sparser than a chunk
+        double r = fma(sAl[l - m] * px, ra, -rb);
+        r = (l == pl0) ? pr0 : r;
+        r = (l == pl0 + 1) ? pr1 : r;
+        rb = ra;
+        ra = r;
+      }
 #pragma unroll
-  for (int t = 0; t < TP; ++t) {
-    const int p = pb + t * NT + threadIdx.x;
-    if (p >= npair) continue;
-#pragma unroll
-    for (int f = 0; f < FB; ++f) {
-      const int k = kb + f;
-      if (k >= nf) continue;
-      const size_t base = ((size_t)k * P.nm + im) * 2 * npair + p;
-      W[base] = accE[t][f];
-      W[base + npair] = accO[t][f];
+      for (int s = 0; s < kSynDeg; ++s) {
+        const int l = lc + s;
+        const bool in = l <= lend;
+        const double a = in ? sAl[l - m] : 0.0, f = in ? sFa[l - m] : 0.0;
+        double r = fma(a * px, ra, -rb);
+        r = (l == pl0) ? pr0 : r;
+        r = (l == pl0 + 1) ? pr1 : r;
+        rb = ra;
+        ra = r;
+        Pn[((s & 1) * (kSynDeg / 2) + (s >> 1)) * kSynPS + pq] = r * f;
+      }
+      pipe_arrive(&full[st]);
     }
+    pipe_cp_wait_all();   // no copy of this thread is in flight when the CTA exits
+    return;
   }
+
+  // consumer warp geometry
+  const int par = warp / WT::WPP, rg = (warp % WT::WPP) / WT::CG, cg = warp % WT::CG;
+  const int rowbase = rg * (64 / WT::RG), colbase = cg * (NCOL / WT::CG);
+  const int g = lane >> 2, t = lane & 3;
+  // first degree any pair of this warp's rows needs
+  int wlmin = INT_MAX / 2;
+  {
+    const int pr = p0 + rowbase + lane;
+    if (lane < 64 / WT::RG && pr < npair) wlmin = P.l0[(size_t)im * npair + pr];
+    for (int o = 16; o > 0; o >>= 1) wlmin = min(wlmin, __shfl_xor_sync(0xffffffffu, wlmin, o));
+  }
+  double acc[WT::MT][WT::NT][4];
+#pragma unroll
+  for (int i = 0; i < WT::MT; ++i)
+#pragma unroll
+    for (int j = 0; j < WT::NT; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
+
+  for (int c = 0; c < nchunks; ++c) {
+    const int st = c % S;
+    if (!pipe_wait(&full[st], (c / S) & 1, abort_flag, err)) break;
+    const int lc = lbeg + c * kSynDeg;
+    if (lc + kSynDeg - 1 >= wlmin) {
+      const double* Pn = sm + st * SM::STAGE + par * (kSynDeg / 2) * kSynPS;
+      const double* C = sm + st * SM::STAGE + SM::PBUF + par * NF * kSynCS;
+#pragma unroll
+      for (int ks = 0; ks < kSynDeg / 8; ++ks) {
+        double a[WT::MT][2], b[WT::NT];
+#pragma unroll
+        for (int i = 0; i < WT::MT; ++i) {
+          const double* pa = Pn + (ks * 4 + t) * kSynPS + rowbase + i * 16 + g;
+          a[i][0] = pa[0];
+          a[i][1] = pa[8];
+        }
+#pragma unroll
+        for (int j = 0; j < WT::NT; ++j) {
+          const int col = colbase + j * 8 + g;
+          b[j] = C[(col >> 1) * kSynCS + 2 * (ks * 4 + t) + (col & 1)];
+        }
+#pragma unroll
+        for (int i = 0; i < WT::MT; ++i)
+#pragma unroll
+          for (int j = 0; j < WT::NT; ++j) dmma_16x8x4(acc[i][j], a[i][0], a[i][1], b[j]);
+      }
+    }
+    __syncwarp();
+    if (lane == 0) pipe_arrive(&empty[st]);
+  }
+  if (*abort_flag) return;
+#pragma unroll
+  for (int i = 0; i < WT::MT; ++i)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int pr = p0 + rowbase + i * 16 + g + 8 * h;
+      if (pr >= npair) continue;
+#pragma unroll
+      for (int j = 0; j < WT::NT; ++j) {
+        const int kf = kb + (colbase + j * 8) / 2 + t;
+        if (kf >= nf) continue;
+        W[(((size_t)kf * P.nm + im) * 2 + par) * npair + pr] = make_double2(acc[i][j][2 * h], acc[i][j][2 * h + 1]);
+      }
+    }
+}
+
+template <int NCOL>
+static int launch_syn_ncol(const shtb_plan* p, const CoefSrc& src, const Factors& F, void* W, int nf, int row_end,
+                           int mlim, cudaStream_t st) {
+  auto kern = leg_syn64_kernel<NCOL>;
+  // shared memory for the longest order (m = 0)
+  const int ndeg = std::min(row_end, p->lrec) + 1;
+  const size_t smem = SynSmem<NCOL>::bytes(ndeg);
+  if (smem > 227 * 1024) return set_error(SHTB_ERR_UNSUPPORTED, "lmax too large for the FP64 synthesis kernel");
+  SHTB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                "synthesis smem attr");
+  constexpr int NF = WarpTile<NCOL>::NF;
+  dim3 grid((p->npair + kSynPairs - 1) / kSynPairs, mlim / p->mres + 1, (nf + NF - 1) / NF);
+  prof_begin(st);
+  kern<<<grid, kLegThreads, smem, st>>>(p->dev, src, F, (double2*)W, nf, row_end, p->d_err);
+  SHTB_LAUNCHED("legendre synthesis kernel");
+  return SHTB_OK;
 }
 
 int launch_leg_syn64(const shtb_plan* p, const CoefSrc& src, const Factors& F, void* W, int nf, int row_end,
                      int mlim, cudaStream_t st) {
-  constexpr int NT = 128, TP = 2;
-  const int nmu = mlim / p->mres + 1;
-  auto go = [&](auto kern, int FB) -> int {
-    dim3 grid((p->npair + TP * NT - 1) / (TP * NT), nmu, (nf + FB - 1) / FB);
-    prof_begin(st);
-    kern<<<grid, NT, 0, st>>>(p->dev, src, F, (double2*)W, nf, row_end);
-    SHTB_LAUNCHED("legendre synthesis kernel");
-    return SHTB_OK;
-  };
-  if (nf >= 8) return go(leg_syn64_kernel<8, TP, NT>, 8);
-  if (nf >= 4) return go(leg_syn64_kernel<4, TP, NT>, 4);
-  if (nf >= 2) return go(leg_syn64_kernel<2, TP, NT>, 2);
-  return go(leg_syn64_kernel<1, TP, NT>, 1);
+  if (nf > 32) return launch_syn_ncol<128>(p, src, F, W, nf, row_end, mlim, st);
+  if (nf > 16) return launch_syn_ncol<64>(p, src, F, W, nf, row_end, mlim, st);
+  if (nf > 8) return launch_syn_ncol<32>(p, src, F, W, nf, row_end, mlim, st);
+  if (nf > 4) return launch_syn_ncol<16>(p, src, F, W, nf, row_end, mlim, st);
+  return launch_syn_ncol<8>(p, src, F, W, nf, row_end, mlim, st);
 }
 
 // ---------------------------------------------------------------------------
-// analysis
+// analysis: CTA = (128 degrees of order m, NCOL/2 fields), K chunks of kAnaPairs pairs
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+constexpr int kAnaPairs = 16;                    // latitude pairs per chunk
+constexpr int kAnaAS = kAnaPairs + 4;            // P panel row stride (doubles), = 4 mod 16
+constexpr int kAnaBS = 2 * kAnaPairs + 8;        // Fourier panel field stride (doubles), = 8 mod 16
+constexpr int kAnaMaxChunks = 512;               // npair <= 8192
+constexpr int kAnaStages = 3;
 
-constexpr int kKC = 32;       // latitude pairs per K chunk
-constexpr int kRS = 82;       // Rs row stride (doubles): 64 rows, 2 pad doubles after every 8 rows, +2
+template <int NCOL>
+struct AnaSmem {
+  static constexpr int NF = WarpTile<NCOL>::NF;
+  static constexpr int ABUF = 2 * 64 * kAnaAS;   // [parity][64 rows][pairs]
+  static constexpr int BBUF = 2 * NF * kAnaBS;   // [parity][field][pairs x re|im]
+  static constexpr int STAGE = ABUF + BBUF;
+  static constexpr int ALPH = kAnaStages * STAGE;          // alpha of the tile's 128 degrees
+  static constexpr int BAR = ALPH + kAnaTile;              // then full[S], empty[S], flags, chunk list
+  static size_t bytes() { return (size_t)BAR * 8 + 2 * kAnaStages * 8 + 16 + (kAnaMaxChunks + 8) * 4; }
+};
 
-template <int CT>
-__host__ __device__ constexpr int ana_bs() { return CT + 2; }
-
-template <int CT, int TC>
-constexpr size_t ana64_smem() {
-  constexpr int RG = 8, CG = CT / TC, KS = 256 / (RG * CG);
-  constexpr size_t main = (size_t)2 * kKC * kRS * 8 + (size_t)2 * 2 * kKC * ana_bs<CT>() * 8 + 64 * 8;
-  constexpr size_t red = (KS > 1) ? (size_t)KS * 64 * CT * 8 : 0;
-  return main > red ? main : red;
-}
-
-template <int CT, int TC>
-__global__ void __launch_bounds__(256, 1) leg_ana64_kernel(PlanDev P, const double2* __restrict__ W, int nf,
-                                                           int row_end, int mlim, CoefSink dst, Factors F,
-                                                           int zero_fill) {
-  constexpr int NT = 256, RG = 8, TRP = 4, CG = CT / TC, KS = NT / (RG * CG), KPT = kKC / KS;
-  constexpr int BS = ana_bs<CT>(), NFB = CT / 2;
-  static_assert(RG * TRP == 32, "64-row tiles");
-  static_assert(KS * RG * CG == NT, "thread layout");
-  static_assert(TC % 2 == 0, "complex column pairs");
+template <int NCOL>
+__global__ void __launch_bounds__(kLegThreads, 1)
+    leg_ana64_kernel(PlanDev P, const double2* __restrict__ W, int nf, int row_end, int mlim, CoefSink dst, Factors F,
+                     int zero_fill, int* err) {
+  using WT = WarpTile<NCOL>;
+  using SM = AnaSmem<NCOL>;
+  constexpr int NF = WT::NF, S = kAnaStages;
   extern __shared__ __align__(16) double sm[];
-  double* Rs = sm;                               // [2][kKC][kRS]
-  double* Bs = sm + 2 * kKC * kRS;               // [2][2][kKC][BS]
-  double* alph = Bs + 2 * 2 * kKC * BS;          // [64]
-  const int2 tile = P.tiles[blockIdx.x];
-  const int im = tile.x, t0 = tile.y, m = im * P.mres;
+  double* salph = sm + SM::ALPH;
+  unsigned long long* full = reinterpret_cast<unsigned long long*>(sm + SM::BAR);
+  unsigned long long* empty = full + S;
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(empty + S);
+  int* slist = reinterpret_cast<int*>(empty + S) + 4;   // nonzero chunks, then their count
+  const int4 tile = P.atiles[blockIdx.x];
+  const int im = tile.x, t0 = tile.y, ck0 = tile.z, m = im * P.mres;
   const int lend = min(row_end, P.lrec);
   if (m > mlim || t0 > lend) return;
-  const int kb = blockIdx.y * NFB;
+  const int kb = blockIdx.y * NF;
   const int npair = P.npair;
   const long long poff = P.off[im];
-  const int tid = threadIdx.x;
-  const int rg = tid % RG, cg = (tid / RG) % CG, ks = tid / (RG * CG);
-  const int lane = tid & 31;
-  const bool producer = tid < 32;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const bool producer = warp >= kConsumerWarps;
+  const int tlast = min(t0 + kAnaTile - 1, lend);
 
-  for (int i = tid; i < 64; i += NT) {
+  if (tid == 0) {
+    for (int q = 0; q < S; ++q) {
+      pipe_bar_init(&full[q], 32 * kProducerWarps);
+      pipe_bar_init(&empty[q], kConsumerWarps);
+    }
+    *abort_flag = 0;
+    pipe_bar_init_fence();
+  }
+  for (int i = tid; i < kAnaTile; i += kLegThreads) {
     const int l = t0 + i;
-    alph[i] = (l <= P.lrec) ? P.alpha[poff + (l - m)] : 0.0;
+    salph[i] = (l <= lend) ? P.alpha[poff + (l - m)] : 0.0;
+  }
+  // chunks with a nonzero P value: some pair's first significant degree is <= tlast
+  const int nch = (npair + kAnaPairs - 1) / kAnaPairs;
+  if (warp == 0) {
+    int cnt = 0;
+    for (int c0 = 0; c0 < nch; c0 += 32) {
+      const int c = c0 + lane;
+      bool nz = false;
+      if (c < nch) {
+        int mn = INT_MAX;
+        for (int q = 0; q < kAnaPairs; ++q) {
+          const int p = c * kAnaPairs + q;
+          if (p < npair) mn = min(mn, P.l0[(size_t)im * npair + p]);
+        }
+        nz = mn <= tlast;
+      }
+      const unsigned bal = __ballot_sync(0xffffffffu, nz);
+      if (nz) slist[cnt + __popc(bal & ((1u << lane) - 1u))] = c;
+      cnt += __popc(bal);
+    }
+    if (lane == 0) slist[kAnaMaxChunks] = cnt;
   }
   __syncthreads();
+  const int nz = slist[kAnaMaxChunks];
 
-  auto produce = [&](int c, int buf) {
-    const int pair = c * kKC + lane;
-    double x = 0.0, ra = 0.0, rb = 0.0, r0 = 0.0, r1 = 0.0;
-    int l0 = INT_MAX / 2;
-    if (pair < npair) {
-      x = P.x[pair];
-      const double2 stv = P.ckpt[(size_t)blockIdx.x * npair + pair];
-      ra = stv.x;
-      rb = stv.y;
-      l0 = P.l0[(size_t)im * npair + pair];
-      const double2 v = P.r01[(size_t)im * npair + pair];
-      r0 = v.x;
-      r1 = v.y;
-    }
-    double* R = Rs + (size_t)(buf * kKC + lane) * kRS;
-#pragma unroll 4
-    for (int rr = 0; rr < 64; rr += 2) {
-      double re, ro;
-      {
-        const int l = t0 + rr;
-        double r = fma(alph[rr] * x, ra, -rb);
-        r = (l == l0) ? r0 : r;
-        r = (l == l0 + 1) ? r1 : r;
-        rb = ra;
-        ra = r;
-        re = r;
+  if (producer) {
+    // every producer thread takes part in every chunk: thread q = 32 w + lane runs the chain
+    // of pair q % 16 over the tile's checkpoint segment q / 16 (ckstep degrees)
+    const int ptid = tid - 32 * kConsumerWarps, pq = ptid % kAnaPairs, seg = ptid / kAnaPairs;
+    const int cs = P.ckstep, nseg = kAnaTile / cs;
+    const bool chain = seg < nseg && t0 + seg * cs <= P.lrec;
+    for (int ci = 0; ci < nz; ++ci) {
+      const int st = ci % S;
+      if (ci >= S && !pipe_wait(&empty[st], ((ci / S) - 1) & 1, abort_flag, err)) break;
+      const int c = slist[ci];
+      double* A = sm + st * SM::STAGE;
+      double* B = A + SM::ABUF;
+      for (int idx = ptid; idx < 2 * NF * kAnaPairs; idx += 32 * kProducerWarps) {
+        const int q = idx % kAnaPairs, rest = idx / kAnaPairs, fl = rest % NF, pr = rest / NF;
+        const int pair = c * kAnaPairs + q, kf = kb + fl;
+        const bool ok = pair < npair && kf < nf;
+        const double2* gp = ok ? W + (((size_t)kf * P.nm + im) * 2 + pr) * npair + pair : W;
+        pipe_cp16(B + (pr * NF + fl) * kAnaBS + 2 * q, gp, ok ? 16u : 0u);
       }
-      {
-        const int l = t0 + rr + 1;
-        double r = fma(alph[rr + 1] * x, ra, -rb);
-        r = (l == l0) ? r0 : r;
-        r = (l == l0 + 1) ? r1 : r;
-        rb = ra;
-        ra = r;
-        ro = r;
-      }
-      // rows (rr, rr+1) = (E row rr/2, O row rr/2) side by side; 16 bytes of padding per 8 rows
-      *reinterpret_cast<double2*>(R + rr + 2 * (rr >> 3)) = make_double2(re, ro);
-    }
-  };
-  auto loadB = [&](int c, int buf) {
-    double* B = Bs + (size_t)buf * 2 * kKC * BS;
-    for (int idx = tid; idx < kKC * CT; idx += NT) {
-      const int kk = idx % kKC, rest = idx / kKC, fl = rest % NFB, par = rest / NFB;
-      const int pair = c * kKC + kk, kf = kb + fl;
-      double* d = B + ((size_t)par * kKC + kk) * BS + 2 * fl;
-      if (pair < npair && kf < nf) {
-        cp_async16(d, W + (((size_t)kf * P.nm + im) * 2 + par) * npair + pair);
-      } else {
-        d[0] = 0.0;
-        d[1] = 0.0;
-      }
-    }
-    cp_async_commit();
-  };
-
-  double accE[TRP][TC], accO[TRP][TC];
-#pragma unroll
-  for (int i = 0; i < TRP; ++i)
-#pragma unroll
-    for (int c = 0; c < TC; ++c) accE[i][c] = accO[i][c] = 0.0;
-
-  const int nchunks = (npair + kKC - 1) / kKC;
-  loadB(0, 0);
-  if (producer) produce(0, 0);
-  cp_async_wait_all();
-  __syncthreads();
-  int buf = 0;
-  for (int c = 0; c < nchunks; ++c) {
-    if (c + 1 < nchunks) {
-      loadB(c + 1, buf ^ 1);
-      if (producer) produce(c + 1, buf ^ 1);
-    }
-    const double* R = Rs + (size_t)buf * kKC * kRS;
-    const double* B = Bs + (size_t)buf * 2 * kKC * BS;
-#pragma unroll 4
-    for (int kk = 0; kk < KPT; ++kk) {
-      const int k = ks * KPT + kk;
-      double rE[TRP], rO[TRP], bE[TC], bO[TC];
-#pragma unroll
-      for (int i = 0; i < TRP; ++i) {
-        const double2 eo = *reinterpret_cast<const double2*>(R + k * kRS + 10 * rg + 2 * i);
-        rE[i] = eo.x;
-        rO[i] = eo.y;
-      }
-#pragma unroll
-      for (int q = 0; q < TC; q += 2) {
-        const double2 e = *reinterpret_cast<const double2*>(B + (size_t)k * BS + cg * TC + q);
-        const double2 o = *reinterpret_cast<const double2*>(B + ((size_t)kKC + k) * BS + cg * TC + q);
-        bE[q] = e.x; bE[q + 1] = e.y;
-        bO[q] = o.x; bO[q + 1] = o.y;
-      }
-#pragma unroll
-      for (int i = 0; i < TRP; ++i)
-#pragma unroll
-        for (int q = 0; q < TC; ++q) {
-          accE[i][q] = fma(rE[i], bE[q], accE[i][q]);
-          accO[i][q] = fma(rO[i], bO[q], accO[i][q]);
+      pipe_arrive_cp_async(&full[st]);
+      if (seg < nseg) {
+        const int p = c * kAnaPairs + pq;
+        double x = 0.0, ra = 0.0, rb = 0.0, r0 = 0.0, r1 = 0.0;
+        int l0 = INT_MAX / 2;
+        if (p < npair && chain) {
+          x = P.x[p];
+          const double2 stv = P.ckpt[(size_t)(ck0 + seg) * npair + p];
+          ra = stv.x;
+          rb = stv.y;
+          l0 = P.l0[(size_t)im * npair + p];
+          const double2 v = P.r01[(size_t)im * npair + p];
+          r0 = v.x;
+          r1 = v.y;
         }
+        const int d0 = seg * cs;
+        double* Ar = A + pq;
+#pragma unroll 4
+        for (int s = 0; s < cs; ++s) {
+          const int d = d0 + s, l = t0 + d;
+          double r = fma(salph[d] * x, ra, -rb);
+          r = (l == l0) ? r0 : r;
+          r = (l == l0 + 1) ? r1 : r;
+          rb = ra;
+          ra = r;
+          Ar[((d & 1) * 64 + (d >> 1)) * kAnaAS] = r;
+        }
+      }
+      pipe_arrive(&full[st]);
     }
-    cp_async_wait_all();
-    __syncthreads();
-    buf ^= 1;
+    pipe_cp_wait_all();   // no copy of this thread is in flight when the CTA exits
+    return;
   }
 
-  if constexpr (KS > 1) {
-    // reduce the K-split partial tiles: red[ks][row 64][CT]
-    double* red = sm;
+  const int par = warp / WT::WPP, rg = (warp % WT::WPP) / WT::CG, cg = warp % WT::CG;
+  const int rowbase = rg * (64 / WT::RG), colbase = cg * (NCOL / WT::CG);
+  const int g = lane >> 2, t = lane & 3;
+  double acc[WT::MT][WT::NT][4];
 #pragma unroll
-    for (int i = 0; i < TRP; ++i)
+  for (int i = 0; i < WT::MT; ++i)
 #pragma unroll
-      for (int q = 0; q < TC; ++q) {
-        const int rp = rg * TRP + i, col = cg * TC + q;
-        red[((size_t)ks * 64 + 2 * rp) * CT + col] = accE[i][q];
-        red[((size_t)ks * 64 + 2 * rp + 1) * CT + col] = accO[i][q];
+    for (int j = 0; j < WT::NT; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
+
+  for (int ci = 0; ci < nz; ++ci) {
+    const int st = ci % S;
+    if (!pipe_wait(&full[st], (ci / S) & 1, abort_flag, err)) break;
+    const double* A = sm + st * SM::STAGE + par * 64 * kAnaAS;
+    const double* B = sm + st * SM::STAGE + SM::ABUF + par * NF * kAnaBS;
+#pragma unroll
+    for (int ks = 0; ks < kAnaPairs / 4; ++ks) {
+      double a[WT::MT][2], b[WT::NT];
+#pragma unroll
+      for (int i = 0; i < WT::MT; ++i) {
+        const double* pa = A + (rowbase + i * 16 + g) * kAnaAS + ks * 4 + t;
+        a[i][0] = pa[0];
+        a[i][1] = pa[8 * kAnaAS];
       }
-    __syncthreads();
-    if (ks == 0) {
 #pragma unroll
-      for (int i = 0; i < TRP; ++i)
+      for (int j = 0; j < WT::NT; ++j) {
+        const int col = colbase + j * 8 + g;
+        b[j] = B[(col >> 1) * kAnaBS + 2 * (ks * 4 + t) + (col & 1)];
+      }
 #pragma unroll
-        for (int q = 0; q < TC; ++q) {
-          const int rp = rg * TRP + i, col = cg * TC + q;
-          double se = 0.0, so = 0.0;
-          for (int s = 0; s < KS; ++s) {
-            se += red[((size_t)s * 64 + 2 * rp) * CT + col];
-            so += red[((size_t)s * 64 + 2 * rp + 1) * CT + col];
-          }
-          accE[i][q] = se;
-          accO[i][q] = so;
-        }
+      for (int i = 0; i < WT::MT; ++i)
+#pragma unroll
+        for (int j = 0; j < WT::NT; ++j) dmma_16x8x4(acc[i][j], a[i][0], a[i][1], b[j]);
     }
+    __syncwarp();
+    if (lane == 0) pipe_arrive(&empty[st]);
   }
+  if (*abort_flag) return;
 
   const long long dbase = dst.packed == 1 ? (poff - m)
                           : dst.packed == 2 ? lm_base(P.lmax, P.mres, m) : (long long)m * dst.ld_m;
   const int lcap = dst.packed == 1 ? lend : min(lend, P.lmax);
-  if (ks == 0) {
 #pragma unroll
-    for (int i = 0; i < TRP; ++i) {
-      const int rp = rg * TRP + i;
+  for (int i = 0; i < WT::MT; ++i)
 #pragma unroll
-      for (int par = 0; par < 2; ++par) {
-        const int l = t0 + 2 * rp + par;
-        if (l > lcap) continue;
-        const double s = factor_at(P, F, poff, l, m);
+    for (int h = 0; h < 2; ++h) {
+      const int row = rowbase + i * 16 + g + 8 * h;
+      const int l = t0 + 2 * row + par;
+      if (l > lcap) continue;
+      const double s = factor_at(P, F, poff, l, m);
 #pragma unroll
-        for (int q = 0; q < TC; q += 2) {
-          const int kf = kb + (cg * TC + q) / 2;
-          if (kf >= nf) continue;
-          const double re = par ? accO[i][q] : accE[i][q];
-          const double imv = par ? accO[i][q + 1] : accE[i][q + 1];
-          dst.ptr[(long long)kf * dst.ld_k + dbase + l] = make_double2(re * s, imv * s);
-        }
+      for (int j = 0; j < WT::NT; ++j) {
+        const int kf = kb + (colbase + j * 8) / 2 + t;
+        if (kf >= nf) continue;
+        dst.ptr[(long long)kf * dst.ld_k + dbase + l] = make_double2(acc[i][j][2 * h] * s, acc[i][j][2 * h + 1] * s);
       }
     }
-  }
   if (zero_fill && !dst.packed && t0 == m) {
     const int nz_lo = m, nz_hi = P.lmax - lcap;  // rows [0, m) and (lcap, lmax]
     const int nrow = nz_lo + max(nz_hi, 0);
-    for (int idx = tid; idx < nrow * NFB; idx += NT) {
+    for (int idx = tid; idx < nrow * NF; idx += 32 * kConsumerWarps) {
       const int r = idx % nrow, fl = idx / nrow, kf = kb + fl;
       if (kf >= nf) continue;
       const int l = (r < nz_lo) ? r : lcap + 1 + (r - nz_lo);
@@ -391,24 +500,30 @@ __global__ void __launch_bounds__(256, 1) leg_ana64_kernel(PlanDev P, const doub
   }
 }
 
+template <int NCOL>
+static int launch_ana_ncol(const shtb_plan* p, const void* W, int nf, int row_end, int mlim, const CoefSink& dst,
+                           const Factors& F, int zero_fill, cudaStream_t st) {
+  if ((p->npair + kAnaPairs - 1) / kAnaPairs > kAnaMaxChunks)
+    return set_error(SHTB_ERR_UNSUPPORTED, "nlat too large for the FP64 analysis kernel");
+  auto kern = leg_ana64_kernel<NCOL>;
+  const size_t smem = AnaSmem<NCOL>::bytes();
+  SHTB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                "analysis smem attr");
+  constexpr int NF = WarpTile<NCOL>::NF;
+  dim3 grid(p->dev.natiles, (nf + NF - 1) / NF);
+  prof_begin(st);
+  kern<<<grid, kLegThreads, smem, st>>>(p->dev, (const double2*)W, nf, row_end, mlim, dst, F, zero_fill, p->d_err);
+  SHTB_LAUNCHED("legendre analysis kernel");
+  return SHTB_OK;
+}
+
 int launch_leg_ana64(const shtb_plan* p, const void* W, int nf, int row_end, int mlim, const CoefSink& dst,
                      const Factors& F, int zero_fill, cudaStream_t st) {
-  auto go = [&](auto kern, size_t smem, int nfb) -> int {
-    SHTB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-                  "analysis smem attr");
-    dim3 grid(p->dev.ntiles, (nf + nfb - 1) / nfb);
-    prof_begin(st);
-    kern<<<grid, 256, smem, st>>>(p->dev, (const double2*)W, nf, row_end, mlim, dst, F, zero_fill);
-    SHTB_LAUNCHED("legendre analysis kernel");
-    return SHTB_OK;
-  };
-  if (nf > 32) return go(leg_ana64_kernel<128, 4>, ana64_smem<128, 4>(), 64);
-  if (nf > 16) return go(leg_ana64_kernel<64, 4>, ana64_smem<64, 4>(), 32);
-  if (nf > 8) return go(leg_ana64_kernel<32, 4>, ana64_smem<32, 4>(), 16);
-  if (nf > 4) return go(leg_ana64_kernel<16, 4>, ana64_smem<16, 4>(), 8);
-  if (nf > 2) return go(leg_ana64_kernel<8, 4>, ana64_smem<8, 4>(), 4);
-  if (nf > 1) return go(leg_ana64_kernel<4, 4>, ana64_smem<4, 4>(), 2);
-  return go(leg_ana64_kernel<2, 2>, ana64_smem<2, 2>(), 1);
+  if (nf > 32) return launch_ana_ncol<128>(p, W, nf, row_end, mlim, dst, F, zero_fill, st);
+  if (nf > 16) return launch_ana_ncol<64>(p, W, nf, row_end, mlim, dst, F, zero_fill, st);
+  if (nf > 8) return launch_ana_ncol<32>(p, W, nf, row_end, mlim, dst, F, zero_fill, st);
+  if (nf > 4) return launch_ana_ncol<16>(p, W, nf, row_end, mlim, dst, F, zero_fill, st);
+  return launch_ana_ncol<8>(p, W, nf, row_end, mlim, dst, F, zero_fill, st);
 }
 
 }  // namespace shtb

@@ -43,10 +43,9 @@ __device__ inline double plm_b(int l, int m) {
 // exponent (legendre.jl:252-271), the scaled recurrence until the exponent
 // returns to zero (legendre.jl:287-322), then the c-scaled recurrence
 //   r_l = alpha_l x r_{l-1} - r_{l-2}
-// through lrec, recording the state in front of every analysis tile.
+// through lrec, recording the state in front of every ckstep-th degree.
 // Values whose exponent is still negative are below 2^-480 and are dropped.
-__global__ void plan_setup_kernel(PlanDev P, const double* __restrict__ seedfac,
-                                  const int* __restrict__ tile_base, int* __restrict__ l0_out,
+__global__ void plan_setup_kernel(PlanDev P, const double* __restrict__ seedfac, int* __restrict__ l0_out,
                                   double2* __restrict__ r01_out, double2* __restrict__ ckpt_out) {
   const int pair = blockIdx.x * blockDim.x + threadIdx.x;
   const int im = blockIdx.y;
@@ -107,12 +106,12 @@ __global__ void plan_setup_kernel(PlanDev P, const double* __restrict__ seedfac,
   }
   l0_out[(size_t)im * P.npair + pair] = l0;
   r01_out[(size_t)im * P.npair + pair] = make_double2(r0, r1);
-  // checkpoints: state before rows t0 = m + kTileRows * t
-  const int tb = tile_base[im];
+  // checkpoints: state before degrees m + ckstep * k
+  const int tb = P.ckbase[im];
   double ra = 0.0, rb = 0.0;
   for (int l = m; l <= LR; ++l) {
-    if (((l - m) % kTileRows) == 0)
-      ckpt_out[(size_t)(tb + (l - m) / kTileRows) * P.npair + pair] = make_double2(ra, rb);
+    if (((l - m) % P.ckstep) == 0)
+      ckpt_out[(size_t)(tb + (l - m) / P.ckstep) * P.npair + pair] = make_double2(ra, rb);
     double r;
     if (l == l0)
       r = r0;
@@ -289,19 +288,32 @@ extern "C" int shtb_plan_create(shtb_plan** out, int lmax, int mmax, int mres, i
   const int nm = p->nm, npair = p->npair, LR = p->lrec;
   p->hoff.resize(nm + 1);
   long long acc = 0;
-  std::vector<int> tile_base(nm);
-  int ntiles = 0;
   for (int im = 0; im < nm; ++im) {
-    const int m = im * mres;
     p->hoff[im] = acc;
-    acc += LR - m + 1;
-    tile_base[im] = ntiles;
-    const int nt = (LR - m + 1 + kTileRows - 1) / kTileRows;
-    for (int t = 0; t < nt; ++t) p->htiles.push_back(make_int2(im, m + t * kTileRows));
-    ntiles += nt;
+    acc += LR - im * mres + 1;
   }
   p->hoff[nm] = acc;
   const long long npk = acc;
+  // checkpoint spacing: the finest of 16, 32, 64, 128 degrees whose table fits the budget
+  int ckstep = 16;
+  auto nseg_total = [&](int cs) {
+    long long n = 0;
+    for (int im = 0; im < nm; ++im) n += (LR - im * mres + cs) / cs;
+    return n;
+  };
+  while (ckstep < kAnaTile && (size_t)nseg_total(ckstep) * npair * 16 > kCkptBudget) ckstep *= 2;
+  std::vector<int> ckbase(nm);
+  int nseg = 0;
+  for (int im = 0; im < nm; ++im) {
+    ckbase[im] = nseg;
+    nseg += (LR - im * mres + ckstep) / ckstep;
+  }
+  std::vector<int4> atiles;
+  for (int im = 0; im < nm; ++im) {
+    const int m = im * mres;
+    for (int t0 = m; t0 <= LR; t0 += kAnaTile) atiles.push_back(make_int4(im, t0, ckbase[im] + (t0 - m) / ckstep, 0));
+  }
+  const int natiles = (int)atiles.size();
   std::vector<double> alpha(npk, 0.0), cfac(npk, 1.0), dco(npk, 0.0);
   for (int im = 0; im < nm; ++im) {
     const int m = im * mres;
@@ -354,10 +366,11 @@ extern "C" int shtb_plan_create(shtb_plan** out, int lmax, int mmax, int mres, i
   const size_t o_x = take(nlat * 8), o_w = take(nlat * 8), o_s = take(nlat * 8);
   const size_t o_off = take((nm + 1) * 8), o_alpha = take(npk * 8), o_c = take(npk * 8), o_d = take(npk * 8);
   const size_t o_l0 = take((size_t)nm * npair * 4), o_r01 = take((size_t)nm * npair * 16);
-  const size_t o_ck = take((size_t)ntiles * npair * 16), o_tiles = take((size_t)ntiles * 8);
+  const size_t o_ck = take((size_t)nseg * npair * 16), o_ckbase = take((size_t)nm * 4);
+  const size_t o_atiles = take((size_t)natiles * 16);
   const size_t o_scale = coeff_scale ? take((size_t)(lmax + 1) * (mmax + 1) * 8) : 0;
   const size_t o_tw = take((size_t)nlon * 16), o_tw32 = take((size_t)nlon * 8);
-  const size_t o_seed = take((mmax + 2) * 8), o_tb = take(nm * 4), o_rev = take((size_t)nlon * 4), o_rinv = take((size_t)nlon * 4);
+  const size_t o_seed = take((mmax + 2) * 8), o_rev = take((size_t)nlon * 4), o_rinv = take((size_t)nlon * 4);
   const size_t o_twp = take((size_t)ntwp * 16), o_twp32 = take((size_t)ntwp * 8);
   const size_t o_err = take(16);
   p->dbytes = o;
@@ -378,12 +391,12 @@ extern "C" int shtb_plan_create(shtb_plan** out, int lmax, int mmax, int mres, i
   if (ce == cudaSuccess) ce = up(o_alpha, alpha.data(), npk * 8);
   if (ce == cudaSuccess) ce = up(o_c, cfac.data(), npk * 8);
   if (ce == cudaSuccess) ce = up(o_d, dco.data(), npk * 8);
-  if (ce == cudaSuccess) ce = up(o_tiles, p->htiles.data(), (size_t)ntiles * 8);
+  if (ce == cudaSuccess) ce = up(o_ckbase, ckbase.data(), (size_t)nm * 4);
+  if (ce == cudaSuccess) ce = up(o_atiles, atiles.data(), (size_t)natiles * 16);
   if (ce == cudaSuccess && coeff_scale) ce = up(o_scale, coeff_scale, (size_t)(lmax + 1) * (mmax + 1) * 8);
   if (ce == cudaSuccess) ce = up(o_tw, tw.data(), (size_t)nlon * 16);
   if (ce == cudaSuccess) ce = up(o_tw32, tw32.data(), (size_t)nlon * 8);
   if (ce == cudaSuccess) ce = up(o_seed, seedfac.data(), (mmax + 2) * 8);
-  if (ce == cudaSuccess) ce = up(o_tb, tile_base.data(), nm * 4);
   if (ce == cudaSuccess) ce = up(o_rev, rev.data(), (size_t)nlon * 4);
   if (ce == cudaSuccess) ce = up(o_rinv, rinv.data(), (size_t)nlon * 4);
   if (ce == cudaSuccess) ce = up(o_twp, twp.data(), (size_t)ntwp * 16);
@@ -405,8 +418,10 @@ extern "C" int shtb_plan_create(shtb_plan** out, int lmax, int mmax, int mres, i
   dv.l0 = (const int*)(D + o_l0);
   dv.r01 = (const double2*)(D + o_r01);
   dv.ckpt = (const double2*)(D + o_ck);
-  dv.tiles = (const int2*)(D + o_tiles);
-  dv.ntiles = ntiles;
+  dv.ckbase = (const int*)(D + o_ckbase);
+  dv.ckstep = ckstep;
+  dv.atiles = (const int4*)(D + o_atiles);
+  dv.natiles = natiles;
   p->d_scale = coeff_scale ? (const double*)(D + o_scale) : nullptr;
   p->d_tw64 = (const double2*)(D + o_tw);
   p->d_tw32 = (const float2*)(D + o_tw32);
@@ -419,8 +434,8 @@ extern "C" int shtb_plan_create(shtb_plan** out, int lmax, int mmax, int mres, i
   if (ce == cudaSuccess) ce = cudaMemset(D + o_err, 0, 16);
 
   dim3 grid((npair + 127) / 128, nm);
-  plan_setup_kernel<<<grid, 128>>>(dv, (const double*)(D + o_seed), (const int*)(D + o_tb), (int*)(D + o_l0),
-                                   (double2*)(D + o_r01), (double2*)(D + o_ck));
+  plan_setup_kernel<<<grid, 128>>>(dv, (const double*)(D + o_seed), (int*)(D + o_l0), (double2*)(D + o_r01),
+                                   (double2*)(D + o_ck));
   count_launch();
   ce = cudaGetLastError();
   if (ce == cudaSuccess) ce = cudaDeviceSynchronize();
