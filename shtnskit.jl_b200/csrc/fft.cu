@@ -568,6 +568,10 @@ template <typename T, typename GT>
 int launch_fft_syn(const shtb_plan* p, const void* W, GT* out0, GT* out1, int ncomp, int nfw, int mlim,
                    double gscale, int use_w, int spow, cudaStream_t st) {
   static_assert(std::is_same<T, GT>::value, "grid and compute types match");
+  if constexpr (std::is_same<T, float>::value) {
+    if (ncomp == 1 && !use_w && !spow && fft2_applicable(p))
+      return launch_fft2_syn(p, W, (float*)out0, nfw, mlim, gscale, st);
+  }
   switch (fft_pick_h(p->fft, sizeof(typename V2<T>::type), p->npair)) {
     case 16: return launch_syn_h<T, 16>(p, W, out0, out1, ncomp, nfw, mlim, gscale, use_w, spow, st);
     case 8: return launch_syn_h<T, 8>(p, W, out0, out1, ncomp, nfw, mlim, gscale, use_w, spow, st);
@@ -581,6 +585,10 @@ template <typename T, typename GT>
 int launch_fft_ana(const shtb_plan* p, const GT* in0, const GT* in1, int ncomp, void* W, int nfw, int mlim,
                    double wscale, int use_w, int spow, cudaStream_t st, int wtile) {
   static_assert(std::is_same<T, GT>::value, "grid and compute types match");
+  if constexpr (std::is_same<T, float>::value) {
+    if (ncomp == 1 && use_w && !spow && wtile && fft2_applicable(p))
+      return launch_fft2_ana(p, (const float*)in0, W, nfw, mlim, wscale, st);
+  }
   switch (fft_pick_h(p->fft, sizeof(typename V2<T>::type), p->npair)) {
     case 16: return launch_ana_h<T, 16>(p, in0, in1, ncomp, W, nfw, mlim, wscale, use_w, spow, wtile, st);
     case 8: return launch_ana_h<T, 8>(p, in0, in1, ncomp, W, nfw, mlim, wscale, use_w, spow, wtile, st);

@@ -52,6 +52,12 @@ int launch_sphtor_post64(const shtb_plan* p, const double2* V, double2* S, doubl
                          const Factors& F, int div_ll, cudaStream_t st);
 int launch_zero_columns64(const shtb_plan* p, double2* a, int nf, int mlim, cudaStream_t st);
 
+// FP32 FFTs on packed pairs of latitude pairs (fft2.cu) for power-of-two nlon <= 2048 and
+// nlat a multiple of 4: the mixed path's analysis into B tile images, and its synthesis.
+bool fft2_applicable(const shtb_plan* p);
+int launch_fft2_ana(const shtb_plan* p, const float* grid, void* W, int nf, int mlim, double wscale, cudaStream_t st);
+int launch_fft2_syn(const shtb_plan* p, const void* W, float* grid, int nf, int mlim, double gscale, cudaStream_t st);
+
 // Floats of one analysis B tile image of the mixed path (hi and lo images back to back).
 size_t fft_btile_floats(const shtb_plan* p, int nf);
 // Bytes of the mixed path's workspace for op (SHTB_OP_SYNTHESIS or SHTB_OP_ANALYSIS).

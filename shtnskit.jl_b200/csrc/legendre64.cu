@@ -441,13 +441,19 @@ __global__ void __launch_bounds__(kLegThreads, 1)
 #pragma unroll
       for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
 
+  // 16-row fragments whose first degree lies past lend hold no output: no MMAs for them
+  // (m-tiles are in increasing degree order, so live[0] false means none is live)
+  bool live[WT::MT];
+#pragma unroll
+  for (int i = 0; i < WT::MT; ++i) live[i] = t0 + 2 * (rowbase + i * 16) + par <= lend;
+
   for (int ci = 0; ci < nz; ++ci) {
     const int st = ci % S;
     if (!pipe_wait(&full[st], (ci / S) & 1, abort_flag, err)) break;
     const double* A = sm + st * SM::STAGE + par * 64 * kAnaAS;
     const double* B = sm + st * SM::STAGE + SM::ABUF + par * NF * kAnaBS;
 #pragma unroll
-    for (int ks = 0; ks < kAnaPairs / 4; ++ks) {
+    for (int ks = 0; ks < kAnaPairs / 4 && live[0]; ++ks) {
       double a[WT::MT][2], b[WT::NT];
 #pragma unroll
       for (int i = 0; i < WT::MT; ++i) {
@@ -462,8 +468,10 @@ __global__ void __launch_bounds__(kLegThreads, 1)
       }
 #pragma unroll
       for (int i = 0; i < WT::MT; ++i)
+        if (live[i]) {
 #pragma unroll
-        for (int j = 0; j < WT::NT; ++j) dmma_16x8x4(acc[i][j], a[i][0], a[i][1], b[j]);
+          for (int j = 0; j < WT::NT; ++j) dmma_16x8x4(acc[i][j], a[i][0], a[i][1], b[j]);
+        }
     }
     __syncwarp();
     if (lane == 0) pipe_arrive(&empty[st]);
