@@ -132,6 +132,22 @@ int shtb_synthesis(const shtb_plan* plan, const void* alm, void* f, int nfields,
 int shtb_analysis(const shtb_plan* plan, const void* f, void* alm, int nfields, int ltr,
                   int dtype, int precision, void* work, size_t work_bytes, void* stream);
 
+/*
+ * Complex grids, FP64 (complex double grids f[i, j, k], coefficients as shtb_synthesis):
+ *   shtb_synthesis_cplx  synthesis with real_output = false: f = ifft of the bins m >= 0
+ *                        without the Hermitian fill (`synthesis(cfg, alm; real_output=false)`,
+ *                        `synthesis_cplx`, src/core_transforms.jl:271-344; CUDA adapter
+ *                        ext/SHTnsKitGPUExt.jl:788-826 with real_output=false)
+ *   shtb_analysis_cplx   analysis of a complex-valued field from its bins m >= 0
+ *                        (src/core_transforms.jl:169-207; ext/SHTnsKitGPUExt.jl:750-786 on a
+ *                        complex CuArray)
+ * Workspace: SHTB_OP_SYNTHESIS / SHTB_OP_ANALYSIS with SHTB_F64, SHTB_PREC_FP64.
+ */
+int shtb_synthesis_cplx(const shtb_plan* plan, const void* alm, void* f, int nfields, int ltr,
+                        void* work, size_t work_bytes, void* stream);
+int shtb_analysis_cplx(const shtb_plan* plan, const void* f, void* alm, int nfields, int ltr,
+                       void* work, size_t work_bytes, void* stream);
+
 /* Spheroidal/toroidal synthesis to (Vt, Vp), real output. */
 int shtb_synthesis_sphtor(const shtb_plan* plan, const void* S, const void* T, void* Vt, void* Vp,
                           int nfields, int ltr, int dtype, int precision,

@@ -603,6 +603,131 @@ template int launch_fft_ana<double, double>(const shtb_plan*, const double*, con
 template int launch_fft_syn<float, float>(const shtb_plan*, const void*, float*, float*, int, int, int, double, int, int, cudaStream_t);
 template int launch_fft_ana<float, float>(const shtb_plan*, const float*, const float*, int, void*, int, int, double, int, int, cudaStream_t, int);
 
+// ---------------------------------------------------------------- complex grids (FP64)
+// Complex-valued grids have no Hermitian symmetry, so each latitude row is its own complex
+// sequence: a CTA holds the north and south rows of H latitude pairs (2H sequences).
+// Synthesis with complex output (real_output = false, src/core_transforms.jl:293-344):
+// bins m >= 0 of the north row are E + O, of the south row E - O, every other bin zero
+// (no Hermitian fill), inverse FFT, times gscale. Analysis of a complex field: forward
+// FFT of both rows, E = w (X_N + X_S), O = w (X_N - X_S) from their bins m >= 0.
+template <int H, bool GENERIC>
+__global__ void __launch_bounds__(512) fft_syn_cplx_kernel(PlanDev P, FFTDesc fd, const int* __restrict__ rinv,
+                                                           const double2* __restrict__ tw,
+                                                           const double2* __restrict__ twp,
+                                                           const double2* __restrict__ W, double2* __restrict__ out,
+                                                           int mlim, double gscale) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int sh = fft_padsh(fd, sizeof(double2)), N = fd.n, S = fft_row_stride(N, sh);
+  double2* Z = reinterpret_cast<double2*>(smem_raw);
+  double2* scratch = Z + 2 * H * S;
+  const int p0 = blockIdx.x * H, k = blockIdx.y;
+  const int npair = P.npair, nlat = P.nlat;
+  const int hv = min(H, npair - p0);
+  for (int idx = threadIdx.x; idx < 2 * H * N; idx += blockDim.x) Z[(idx / N) * S + fft_pad(idx % N, sh)] = make_double2(0.0, 0.0);
+  __syncthreads();
+  const int nmu = mlim / P.mres + 1;
+  for (int idx = threadIdx.x; idx < nmu * H; idx += blockDim.x) {
+    const int im = idx / H, h = idx - im * H, m = im * P.mres;
+    if (h >= hv) continue;
+    const size_t base = ((size_t)k * P.nm + im) * 2 * npair + p0 + h;
+    const double2 E = W[base], O = W[base + npair];
+    Z[(2 * h) * S + fft_pad(m, sh)] = cadd(E, O);
+    Z[(2 * h + 1) * S + fft_pad(m, sh)] = csub(E, O);
+  }
+  __syncthreads();
+  fft_rows<double, double2, GENERIC>(Z, scratch, 2 * H, S, fd, tw, twp, +1);
+  // storage position q holds longitude rinv[q]; threads take the 2H rows of one position
+  for (int idx = threadIdx.x; idx < 2 * H * N; idx += blockDim.x) {
+    const int r = idx % (2 * H), q = idx / (2 * H), h = r >> 1;
+    if (h >= hv) continue;
+    const int pair = p0 + h, row = (r & 1) ? nlat - 1 - pair : pair;
+    if ((r & 1) && row == pair) continue;   // the equator row of odd nlat is its north row
+    out[((size_t)k * N + rinv[q]) * nlat + row] = cscale(Z[r * S + fft_pad(q, sh)], gscale);
+  }
+}
+
+template <int H, bool GENERIC>
+__global__ void __launch_bounds__(512) fft_ana_cplx_kernel(PlanDev P, FFTDesc fd, const int* __restrict__ rev,
+                                                           const double2* __restrict__ tw,
+                                                           const double2* __restrict__ twp,
+                                                           const double2* __restrict__ in, double2* __restrict__ W,
+                                                           int mlim, double wscale) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int sh = fft_padsh(fd, sizeof(double2)), N = fd.n, S = fft_row_stride(N, sh);
+  double2* Z = reinterpret_cast<double2*>(smem_raw);
+  double2* scratch = Z + 2 * H * S;
+  const int p0 = blockIdx.x * H, k = blockIdx.y;
+  const int npair = P.npair, nlat = P.nlat;
+  const int hv = min(H, npair - p0);
+  // threads take the 2H rows of one longitude (contiguous runs of the grid)
+  for (int idx = threadIdx.x; idx < 2 * H * N; idx += blockDim.x) {
+    const int r = idx % (2 * H), j = idx / (2 * H), h = r >> 1;
+    double2 v = make_double2(0.0, 0.0);
+    if (h < hv) {
+      const int pair = p0 + h, row = (r & 1) ? nlat - 1 - pair : pair;
+      if (!((r & 1) && row == pair)) v = in[((size_t)k * N + j) * nlat + row];
+    }
+    Z[r * S + fft_pad(j, sh)] = v;
+  }
+  __syncthreads();
+  fft_rows<double, double2, GENERIC>(Z, scratch, 2 * H, S, fd, tw, twp, -1);
+  const int nmu = mlim / P.mres + 1;
+  for (int idx = threadIdx.x; idx < nmu * H; idx += blockDim.x) {
+    const int im = idx / H, h = idx - im * H, m = im * P.mres;
+    if (h >= hv) continue;
+    const double wt = wscale * P.w[p0 + h];
+    const double2 XN = Z[(2 * h) * S + fft_pad(rev[m], sh)], XS = Z[(2 * h + 1) * S + fft_pad(rev[m], sh)];
+    const size_t base = ((size_t)k * P.nm + im) * 2 * npair + p0 + h;
+    W[base] = cscale(cadd(XN, XS), wt);
+    W[base + npair] = cscale(csub(XN, XS), wt);
+  }
+}
+
+// Latitude pairs per CTA for complex rows: the largest H <= 8 whose 2H padded rows fit
+// ~200 KB of shared memory.
+static int fft_pick_h_cplx(const FFTDesc& fd, int npair) {
+  const size_t S = (size_t)fft_row_stride(fd.n, fft_padsh(fd, sizeof(double2)));
+  int h = 8;
+  while (h > 1 && (size_t)2 * h * S * sizeof(double2) * (fd.direct ? 2 : 1) > 200 * 1024) h >>= 1;
+  while (h > 1 && h / 2 >= npair) h >>= 1;
+  return h;
+}
+
+template <int H>
+static int launch_cplx_h(const shtb_plan* p, int syn, const void* src, void* dst, int nf, int mlim, double scale,
+                         cudaStream_t st) {
+  const size_t smem = (size_t)2 * H * fft_row_stride(p->fft.n, fft_padsh(p->fft, sizeof(double2))) * sizeof(double2) *
+                      (p->fft.direct ? 2 : 1);
+  if (smem > 227 * 1024) return set_error(SHTB_ERR_UNSUPPORTED, "nlon too large for the complex-row FFT");
+  const bool gen = fft_generic(p);
+  dim3 grid((p->npair + H - 1) / H, nf);
+  prof_begin(st);
+  if (syn) {
+    auto kern = gen ? fft_syn_cplx_kernel<H, true> : fft_syn_cplx_kernel<H, false>;
+    SHTB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "fft smem attr");
+    kern<<<grid, 512, smem, st>>>(p->dev, p->fft, p->d_rinv, p->d_tw64, p->d_twp64, (const double2*)src,
+                                  (double2*)dst, mlim, scale);
+    SHTB_LAUNCHED("fft synthesis kernel");
+  } else {
+    auto kern = gen ? fft_ana_cplx_kernel<H, true> : fft_ana_cplx_kernel<H, false>;
+    SHTB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "fft smem attr");
+    kern<<<grid, 512, smem, st>>>(p->dev, p->fft, p->d_rev, p->d_tw64, p->d_twp64, (const double2*)src,
+                                  (double2*)dst, mlim, scale);
+    SHTB_LAUNCHED("fft analysis kernel");
+  }
+  return SHTB_OK;
+}
+
+int launch_fft_cplx64(const shtb_plan* p, int syn, const void* src, void* dst, int nf, int mlim, double scale,
+                      cudaStream_t st) {
+  switch (fft_pick_h_cplx(p->fft, p->npair)) {
+    case 8: return launch_cplx_h<8>(p, syn, src, dst, nf, mlim, scale, st);
+    case 4: return launch_cplx_h<4>(p, syn, src, dst, nf, mlim, scale, st);
+    case 2: return launch_cplx_h<2>(p, syn, src, dst, nf, mlim, scale, st);
+    default: return launch_cplx_h<1>(p, syn, src, dst, nf, mlim, scale, st);
+  }
+}
+
 // ---------------------------------------------------------------- grouped transforms
 // Host-side pieces of the persistent grouped FP32 FFTs.
 

@@ -40,6 +40,12 @@ template <typename T, typename GT>
 int launch_fft_ana(const shtb_plan* p, const GT* in0, const GT* in1, int ncomp, void* W, int nfw, int mlim,
                    double wscale, int use_w, int spow, cudaStream_t st, int wtile = 0);
 
+// FP64 FFTs of complex grids (each latitude row its own sequence): syn = 1 takes the
+// Fourier buffer to a complex grid (bins m >= 0 only, times scale), syn = 0 a complex grid
+// to the Fourier buffer (weights w times scale).
+int launch_fft_cplx64(const shtb_plan* p, int syn, const void* src, void* dst, int nf, int mlim, double scale,
+                      cudaStream_t st);
+
 int launch_leg_syn64(const shtb_plan* p, const CoefSrc& src, const Factors& F, void* W, int nf, int row_end,
                      int mlim, cudaStream_t st);
 int launch_leg_ana64(const shtb_plan* p, const void* W, int nf, int row_end, int mlim, const CoefSink& dst,

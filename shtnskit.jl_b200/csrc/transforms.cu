@@ -256,6 +256,35 @@ static int scalar_analysis(const shtb_plan* p, const void* f, void* alm, int nf,
   return SHTB_OK;
 }
 
+// Complex grids (FP64): synthesis with real_output = false, analysis of complex fields.
+extern "C" int shtb_synthesis_cplx(const shtb_plan* p, const void* alm, void* f, int nf, int ltr, void* work,
+                                   size_t wb, void* stream) {
+  int rc = check_common(p, nf, &ltr, SHTB_F64, SHTB_PREC_FP64, work, wb, SHTB_OP_SYNTHESIS);
+  if (rc) return rc;
+  if ((rc = check_ptrs({alm, f}))) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int mlim = std::min(p->mmax, ltr);
+  CoefSrc src{(const double2*)alm, (long long)(p->lmax + 1) * (p->mmax + 1), (long long)(p->lmax + 1), 0};
+  Factors F{p->dev.cfac, p->d_scale, p->d_scale ? 1 : 0, 1.0, 1.0};
+  if ((rc = launch_leg_syn64(p, src, F, work, nf, ltr, mlim, st))) return rc;
+  return launch_fft_cplx64(p, 1, work, f, nf, mlim, p->phi_inv_scale / p->nlon, st);
+}
+
+extern "C" int shtb_analysis_cplx(const shtb_plan* p, const void* f, void* alm, int nf, int ltr, void* work,
+                                  size_t wb, void* stream) {
+  int rc = check_common(p, nf, &ltr, SHTB_F64, SHTB_PREC_FP64, work, wb, SHTB_OP_ANALYSIS);
+  if (rc) return rc;
+  if ((rc = check_ptrs({alm, f}))) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int mlim = std::min(p->mmax, ltr);
+  if ((rc = launch_fft_cplx64(p, 0, f, work, nf, mlim, p->ana_scale, st))) return rc;
+  Factors F{p->dev.cfac, p->d_scale, p->d_scale ? 2 : 0, 1.0, 1.0};
+  CoefSink dst{(double2*)alm, (long long)(p->lmax + 1) * (p->mmax + 1), (long long)(p->lmax + 1), 0};
+  if ((rc = launch_leg_ana64(p, work, nf, ltr, mlim, dst, F, 1, st))) return rc;
+  if (p->mres > 1 || mlim < p->mmax) return launch_zero_columns64(p, (double2*)alm, nf, mlim, st);
+  return SHTB_OK;
+}
+
 extern "C" int shtb_synthesis(const shtb_plan* p, const void* alm, void* f, int nf, int ltr, int dtype,
                               int precision, void* work, size_t wb, void* stream) {
   return scalar_synthesis(p, alm, f, nf, ltr, dtype, precision, work, wb, stream, 0);

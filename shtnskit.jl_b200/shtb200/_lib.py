@@ -72,6 +72,8 @@ SIGNATURES = {
     "shtb_workspace_bytes": (_SZ, [_P, _I, _I, _I, _I]),
     "shtb_synthesis": (_I, [_P, _P, _P, _I, _I, _I, _I, _P, _SZ, _P]),
     "shtb_analysis": (_I, [_P, _P, _P, _I, _I, _I, _I, _P, _SZ, _P]),
+    "shtb_synthesis_cplx": (_I, [_P, _P, _P, _I, _I, _P, _SZ, _P]),
+    "shtb_analysis_cplx": (_I, [_P, _P, _P, _I, _I, _P, _SZ, _P]),
     "shtb_synthesis_sphtor": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _P, _SZ, _P]),
     "shtb_analysis_sphtor": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _P, _SZ, _P]),
     "shtb_synthesis_packed": (_I, [_P, _P, _P, _I, _I, _I, _I, _P, _SZ, _P]),

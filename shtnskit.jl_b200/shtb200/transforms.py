@@ -348,6 +348,36 @@ def _check_scratch(fft_scratch):
         raise ArgumentError("CUDA scalar transforms do not accept a host fft_scratch")
 
 
+def _cplx_call(name, op, cfg, src, dst, ltr):
+    dev = src.device.index
+    plan = cfg.plan(dev)
+    nf = src.shape[2]
+    ws, nb = _workspace(plan, op, nf, _lib.SHTB_F64, _lib.SHTB_PREC_FP64, dev)
+    with torch.cuda.device(dev):
+        rc = getattr(_lib.load(), name)(plan.handle, _ptr(src), _ptr(dst), nf, ltr, _ptr(ws), nb, _stream(dev))
+    _lib.check(rc, name)
+    return dst
+
+
+def _synthesis_cplx(cfg, alm, batched, lcap, precision, out):
+    # real_output = false: complex grid from the bins m >= 0 without the Hermitian fill
+    # (src/core_transforms.jl:293-344), FP64 path
+    if _prec_code(precision) != _lib.SHTB_PREC_FP64:
+        raise BackendUnavailableError("synthesis", "complex output runs on the FP64 path only")
+    a = _as_tensor(alm)
+    _check_coeff_shape(cfg, a, batched)
+    ltr = _lcap(cfg, lcap)
+    dev = _device_index(alm, out)
+    a3 = to_device(a if a.is_complex() else a.to(torch.complex128), torch.complex128, dev)
+    a3 = a3 if batched else a3.unsqueeze(2)
+    f = julia_empty((cfg.nlat, cfg.nlon, a3.shape[2]), torch.complex128, a3.device)
+    _cplx_call("shtb_synthesis_cplx", _lib.SHTB_OP_SYNTHESIS, cfg, a3.detach(), f, ltr)
+    if out is not None:
+        out.copy_(f.reshape(out.shape))
+        return out
+    return f if batched else f[:, :, 0]
+
+
 def _synthesis_impl(cfg, alm, batched, real_output, use_rfft, fft_scratch, lcap, precision, out=None):
     _check_scratch(fft_scratch)
     if use_rfft and not real_output:
@@ -355,7 +385,7 @@ def _synthesis_impl(cfg, alm, batched, real_output, use_rfft, fft_scratch, lcap,
     if use_rfft and cfg.mmax > cfg.nlon // 2:
         raise ArgumentError(f"use_rfft=true requires mmax ≤ nlon÷2, got mmax={cfg.mmax}, nlon={cfg.nlon}")
     if not real_output:
-        raise BackendUnavailableError("synthesis", "complex output (real_output=false) is not implemented by this backend")
+        return _synthesis_cplx(cfg, alm, batched, lcap, precision, out)
     a = _as_tensor(alm)
     _check_coeff_shape(cfg, a, batched)
     ltr = _lcap(cfg, lcap)
@@ -387,7 +417,19 @@ def _analysis_impl(cfg, f, batched, use_rfft, fft_scratch, lcap, precision, out=
     if t.is_complex():
         if use_rfft:
             raise ArgumentError("use_rfft=true requires a real-valued input")
-        raise BackendUnavailableError("analysis", "complex-valued fields are not implemented by this backend")
+        # complex field: coefficients from its bins m >= 0 (src/core_transforms.jl:169-207), FP64 path
+        if _prec_code(precision) != _lib.SHTB_PREC_FP64:
+            raise BackendUnavailableError("analysis", "complex fields run on the FP64 path only")
+        _check_grid_shape(cfg, t, batched)
+        ltr = _lcap(cfg, lcap)
+        t3 = to_device(t, torch.complex128, _device_index(f, out))
+        t3 = t3 if batched else t3.unsqueeze(2)
+        a = julia_empty((cfg.lmax + 1, cfg.mmax + 1, t3.shape[2]), torch.complex128, t3.device)
+        _cplx_call("shtb_analysis_cplx", _lib.SHTB_OP_ANALYSIS, cfg, t3.detach(), a, ltr)
+        if out is not None:
+            out.copy_(a.reshape(out.shape))
+            return out
+        return a if batched else a[:, :, 0]
     _check_grid_shape(cfg, t, batched)
     ltr = _lcap(cfg, lcap)
     prec = _prec_code(precision)
