@@ -91,59 +91,127 @@ workspace(p::Plan, op, nf, dtype, prec) =
 stream() = CUDA.stream().handle
 dtype_of(::Type{<:Union{Float64,ComplexF64}}) = SHTB_F64
 dtype_of(::Type{<:Union{Float32,ComplexF32}}) = SHTB_F32
-prec_of(T) = dtype_of(T) == SHTB_F64 ? SHTB_PREC_FP64 : SHTB_PREC_MIXED
+
+# Arithmetic path of a call. The rule is explicit: Float64/ComplexF64 arrays run the plain
+# FP64 path (relative L2 <= 1e-12 against the reference CPU result); Float32/ComplexF32
+# arrays run the mixed path (`precision = :mixed`: Legendre contraction as fp16x3 tensor-core
+# products with FP32 accumulation, relative L2 <= 1e-6, measured 2e-7..4e-7 at lmax 1023),
+# which is at least as accurate as a plain Float32 recurrence. `precision = :fp64` on Float32
+# arrays promotes them to Float64 for the call and rounds the result back.
+function precision_of(::Type{T}, precision::Symbol) where {T}
+    precision === :auto && return dtype_of(T) == SHTB_F64 ? SHTB_PREC_FP64 : SHTB_PREC_MIXED
+    precision === :fp64 && return SHTB_PREC_FP64
+    precision === :mixed && return SHTB_PREC_MIXED
+    throw(ArgumentError("precision must be :auto, :fp64 or :mixed, got :$precision"))
+end
 
 # ---------------------------------------------------------------- transforms (3-D = batch)
-function _synthesis(cfg, alm::CuArray{Complex{T}}; lcap::Int=cfg.lmax) where {T<:Union{Float32,Float64}}
+# Writes into `f` (nlat, nlon, nf), real of the precision's element type.
+function _synthesis!(f::CuArray{T,3}, cfg, alm::CuArray{Complex{T},3}, lcap::Int, prec::Cint) where {T}
     nf = size(alm, 3)
-    f = CuArray{T}(undef, cfg.nlat, cfg.nlon, nf)
     p = plan(cfg)
-    ws = workspace(p, OP_SYN, nf, dtype_of(T), prec_of(T))
+    ws = workspace(p, OP_SYN, nf, dtype_of(T), prec)
     check(ccall((:shtb_synthesis, LIB), Cint,
                 (Ptr{Cvoid}, CuPtr{Cvoid}, CuPtr{Cvoid}, Cint, Cint, Cint, Cint, CuPtr{Cvoid}, Csize_t, Ptr{Cvoid}),
-                p.ptr, alm, f, nf, lcap, dtype_of(T), prec_of(T), ws, sizeof(ws), stream()), :synthesis)
+                p.ptr, alm, f, nf, lcap, dtype_of(T), prec, ws, sizeof(ws), stream()), :synthesis)
     return f
 end
 
-function _analysis(cfg, f::CuArray{T}; lcap::Int=cfg.lmax) where {T<:Union{Float32,Float64}}
+function _analysis!(alm::CuArray{Complex{T},3}, cfg, f::CuArray{T,3}, lcap::Int, prec::Cint) where {T}
     nf = size(f, 3)
-    alm = CuArray{Complex{T}}(undef, cfg.lmax + 1, cfg.mmax + 1, nf)
     p = plan(cfg)
-    ws = workspace(p, OP_ANA, nf, dtype_of(T), prec_of(T))
+    ws = workspace(p, OP_ANA, nf, dtype_of(T), prec)
     check(ccall((:shtb_analysis, LIB), Cint,
                 (Ptr{Cvoid}, CuPtr{Cvoid}, CuPtr{Cvoid}, Cint, Cint, Cint, Cint, CuPtr{Cvoid}, Csize_t, Ptr{Cvoid}),
-                p.ptr, f, alm, nf, lcap, dtype_of(T), prec_of(T), ws, sizeof(ws), stream()), :analysis)
+                p.ptr, f, alm, nf, lcap, dtype_of(T), prec, ws, sizeof(ws), stream()), :analysis)
+    return alm
+end
+
+# complex grids (FP64): synthesis with real_output = false, analysis of complex fields
+function _synthesis_cplx!(g::CuArray{ComplexF64,3}, cfg, alm::CuArray{ComplexF64,3}, lcap::Int)
+    nf = size(alm, 3)
+    p = plan(cfg)
+    ws = workspace(p, OP_SYN, nf, SHTB_F64, SHTB_PREC_FP64)
+    check(ccall((:shtb_synthesis_cplx, LIB), Cint,
+                (Ptr{Cvoid}, CuPtr{Cvoid}, CuPtr{Cvoid}, Cint, Cint, CuPtr{Cvoid}, Csize_t, Ptr{Cvoid}),
+                p.ptr, alm, g, nf, lcap, ws, sizeof(ws), stream()), :synthesis)
+    return g
+end
+
+function _analysis_cplx!(alm::CuArray{ComplexF64,3}, cfg, g::CuArray{ComplexF64,3}, lcap::Int)
+    nf = size(g, 3)
+    p = plan(cfg)
+    ws = workspace(p, OP_ANA, nf, SHTB_F64, SHTB_PREC_FP64)
+    check(ccall((:shtb_analysis_cplx, LIB), Cint,
+                (Ptr{Cvoid}, CuPtr{Cvoid}, CuPtr{Cvoid}, Cint, Cint, CuPtr{Cvoid}, Csize_t, Ptr{Cvoid}),
+                p.ptr, g, alm, nf, lcap, ws, sizeof(ws), stream()), :analysis)
     return alm
 end
 
 as3(x::CuArray) = ndims(x) == 3 ? x : reshape(x, size(x, 1), size(x, 2), 1)
 drop3(x, like) = ndims(like) == 3 ? x : reshape(x, size(x, 1), size(x, 2))
+dense3(x, ::Type{T}) where {T} = as3(x isa CuArray{T} ? x : CuArray{T}(x))
+
+check_spectral(cfg, alm) = size(alm, 1) == cfg.lmax + 1 && size(alm, 2) == cfg.mmax + 1 || throw(DimensionMismatch(
+    "coefficients must have size ($(cfg.lmax + 1), $(cfg.mmax + 1)), got $(size(alm))"))
+check_grid(cfg, f) = size(f, 1) == cfg.nlat && size(f, 2) == cfg.nlon || throw(DimensionMismatch(
+    "field must have size ($(cfg.nlat), $(cfg.nlon)), got $(size(f))"))
+check_lcap(cfg, lcap) = 0 <= lcap <= cfg.lmax || throw(ArgumentError("lcap must satisfy 0 ≤ lcap ≤ lmax=$(cfg.lmax)"))
+
+# synthesis of any 2-D/3-D coefficient array: real grid of the precision's type, or a
+# complex grid (real_output = false, FP64)
+function synthesis_any(cfg, alm; real_output::Bool=true, use_rfft::Bool=false, lcap::Int=cfg.lmax,
+                       precision::Symbol=:auto)
+    use_rfft && !real_output && throw(ArgumentError("use_rfft=true implies real_output"))
+    check_spectral(cfg, alm)
+    check_lcap(cfg, lcap)
+    if !real_output
+        a = dense3(alm, ComplexF64)
+        return drop3(_synthesis_cplx!(CuArray{ComplexF64}(undef, cfg.nlat, cfg.nlon, size(a, 3)), cfg, a, lcap), alm)
+    end
+    Tin = real(eltype(alm)) <: Float32 ? Float32 : Float64
+    prec = precision_of(Tin, precision)
+    T = prec == SHTB_PREC_FP64 ? Float64 : Float32
+    a = dense3(alm, Complex{T})
+    f = _synthesis!(CuArray{T}(undef, cfg.nlat, cfg.nlon, size(a, 3)), cfg, a, lcap, prec)
+    return drop3(T === Tin ? f : CuArray{Tin}(f), alm)
+end
+
+# analysis of any 2-D/3-D grid: real fields on the precision's path, complex fields on FP64
+function analysis_any(cfg, f; use_rfft::Bool=false, lcap::Int=cfg.lmax, precision::Symbol=:auto)
+    check_grid(cfg, f)
+    check_lcap(cfg, lcap)
+    if eltype(f) <: Complex
+        use_rfft && throw(ArgumentError("use_rfft=true requires a real-valued input"))
+        g = dense3(f, ComplexF64)
+        return drop3(_analysis_cplx!(CuArray{ComplexF64}(undef, cfg.lmax + 1, cfg.mmax + 1, size(g, 3)), cfg, g, lcap), f)
+    end
+    Tin = eltype(f) <: Float32 ? Float32 : Float64
+    prec = precision_of(Tin, precision)
+    T = prec == SHTB_PREC_FP64 ? Float64 : Float32
+    x = dense3(f, T)
+    alm = _analysis!(CuArray{Complex{T}}(undef, cfg.lmax + 1, cfg.mmax + 1, size(x, 3)), cfg, x, lcap, prec)
+    return drop3(T === Tin ? alm : CuArray{Complex{Tin}}(alm), f)
+end
 
 function SHTnsKit._gpu_adapter_synthesis(::B200Adapter, cfg::SHTnsKit.SHTConfig, alm;
                                          real_output::Bool=true, use_rfft::Bool=false,
-                                         fft_scratch=nothing, lcap::Int=cfg.lmax)
+                                         fft_scratch=nothing, lcap::Int=cfg.lmax, precision::Symbol=:auto)
     fft_scratch === nothing || throw(ArgumentError("CUDA scalar transforms do not accept a host fft_scratch"))
-    use_rfft && !real_output && throw(ArgumentError("use_rfft=true implies real_output"))
-    real_output || throw(SHTnsKit.BackendUnavailableError(:synthesis, "real_output=false is not implemented by this backend"))
-    size(alm, 1) == cfg.lmax + 1 && size(alm, 2) == cfg.mmax + 1 || throw(DimensionMismatch(
-        "coefficients must have size ($(cfg.lmax + 1), $(cfg.mmax + 1)), got $(size(alm))"))
-    a = alm isa CuArray{<:Complex} ? alm : CuArray{ComplexF64}(alm)
-    return drop3(_synthesis(cfg, as3(a); lcap), alm)
+    return synthesis_any(cfg, alm; real_output, use_rfft, lcap, precision)
 end
 
 function SHTnsKit._gpu_adapter_analysis(::B200Adapter, cfg::SHTnsKit.SHTConfig, f;
-                                        use_rfft::Bool=false, fft_scratch=nothing, lcap::Int=cfg.lmax)
+                                        use_rfft::Bool=false, fft_scratch=nothing, lcap::Int=cfg.lmax,
+                                        precision::Symbol=:auto)
     fft_scratch === nothing || throw(ArgumentError("CUDA scalar transforms do not accept a host fft_scratch"))
-    eltype(f) <: Real || throw(SHTnsKit.BackendUnavailableError(:analysis, "complex fields are not implemented by this backend"))
-    size(f, 1) == cfg.nlat && size(f, 2) == cfg.nlon || throw(DimensionMismatch(
-        "field must have size ($(cfg.nlat), $(cfg.nlon)), got $(size(f))"))
-    return drop3(_analysis(cfg, as3(f); lcap), f)
+    return analysis_any(cfg, f; use_rfft, lcap, precision)
 end
 
-function SHTnsKit._gpu_adapter_synthesis_sphtor(::B200Adapter, cfg::SHTnsKit.SHTConfig, S, T;
-                                                real_output::Bool=true, use_rfft::Bool=false, lcap::Int=cfg.lmax)
+function _synthesis_sphtor(cfg, S, T; real_output::Bool=true, lcap::Int=cfg.lmax)
     real_output || throw(SHTnsKit.BackendUnavailableError(:synthesis_sphtor, "real_output=false is not implemented"))
-    S3, T3 = as3(CuArray{ComplexF64}(S)), as3(CuArray{ComplexF64}(T))
+    check_spectral(cfg, S); check_spectral(cfg, T); check_lcap(cfg, lcap)
+    S3, T3 = dense3(S, ComplexF64), dense3(T, ComplexF64)
     nf = size(S3, 3)
     Vt = CuArray{Float64}(undef, cfg.nlat, cfg.nlon, nf); Vp = similar(Vt)
     p = plan(cfg)
@@ -155,9 +223,9 @@ function SHTnsKit._gpu_adapter_synthesis_sphtor(::B200Adapter, cfg::SHTnsKit.SHT
     return drop3(Vt, S), drop3(Vp, S)
 end
 
-function SHTnsKit._gpu_adapter_analysis_sphtor(::B200Adapter, cfg::SHTnsKit.SHTConfig, Vt, Vp;
-                                               use_rfft::Bool=false, lcap::Int=cfg.lmax)
-    A, B = as3(CuArray{Float64}(Vt)), as3(CuArray{Float64}(Vp))
+function _analysis_sphtor(cfg, Vt, Vp; lcap::Int=cfg.lmax)
+    check_grid(cfg, Vt); check_grid(cfg, Vp); check_lcap(cfg, lcap)
+    A, B = dense3(Vt, Float64), dense3(Vp, Float64)
     nf = size(A, 3)
     S = CuArray{ComplexF64}(undef, cfg.lmax + 1, cfg.mmax + 1, nf); T = similar(S)
     p = plan(cfg)
@@ -169,21 +237,128 @@ function SHTnsKit._gpu_adapter_analysis_sphtor(::B200Adapter, cfg::SHTnsKit.SHTC
     return drop3(S, Vt), drop3(T, Vt)
 end
 
-# batched entry points of the reference's CUDA extension (ext/SHTnsKitGPUExt.jl:1845-1975)
-SHTnsKit.synthesis_batch(cfg::SHTnsKit.SHTConfig, alm::CuArray{<:Complex,3}; lcap::Int=cfg.lmax, kwargs...) =
-    _synthesis(cfg, alm; lcap)
-SHTnsKit.analysis_batch(cfg::SHTnsKit.SHTConfig, f::CuArray{<:Real,3}; lcap::Int=cfg.lmax, kwargs...) =
-    _analysis(cfg, f; lcap)
+SHTnsKit._gpu_adapter_synthesis_sphtor(::B200Adapter, cfg::SHTnsKit.SHTConfig, S, T;
+                                       real_output::Bool=true, use_rfft::Bool=false, lcap::Int=cfg.lmax) =
+    _synthesis_sphtor(cfg, S, T; real_output, lcap)
+SHTnsKit._gpu_adapter_analysis_sphtor(::B200Adapter, cfg::SHTnsKit.SHTConfig, Vt, Vp;
+                                      use_rfft::Bool=false, lcap::Int=cfg.lmax) =
+    _analysis_sphtor(cfg, Vt, Vp; lcap)
+
+# ---------------------------------------------------------------- direct methods of the reference's CUDA extension
+# batched scalar transforms (ext/SHTnsKitGPUExt.jl:1845-1975)
+SHTnsKit.synthesis_batch(::SHTnsKit.GPU, cfg::SHTnsKit.SHTConfig, alm::CuArray{<:Complex,3};
+                         real_output::Bool=true, use_rfft::Bool=false, lcap::Int=cfg.lmax, precision::Symbol=:auto) =
+    synthesis_any(cfg, alm; real_output, use_rfft, lcap, precision)
+SHTnsKit.synthesis_batch(cfg::SHTnsKit.SHTConfig, alm::CuArray{<:Complex,3}; kwargs...) =
+    SHTnsKit.synthesis_batch(SHTnsKit.GPU(), cfg, alm; kwargs...)
+SHTnsKit.synthesis_batch_cplx(::SHTnsKit.GPU, cfg::SHTnsKit.SHTConfig, alm::CuArray{<:Complex,3}) =
+    synthesis_any(cfg, alm; real_output=false)
+SHTnsKit.synthesis_batch_cplx(cfg::SHTnsKit.SHTConfig, alm::CuArray{<:Complex,3}) =
+    synthesis_any(cfg, alm; real_output=false)
+SHTnsKit.analysis_batch(::SHTnsKit.GPU, cfg::SHTnsKit.SHTConfig, f::CuArray{<:Real,3};
+                        use_rfft::Bool=false, lcap::Int=cfg.lmax, precision::Symbol=:auto) =
+    analysis_any(cfg, f; use_rfft, lcap, precision)
+SHTnsKit.analysis_batch(cfg::SHTnsKit.SHTConfig, f::CuArray{<:Real,3}; kwargs...) =
+    SHTnsKit.analysis_batch(SHTnsKit.GPU(), cfg, f; kwargs...)
+
+# into caller-owned device outputs: the library writes `output` directly when it is a dense
+# CuArray of the path's element type, else through a temporary
+function _into!(output, result)
+    result === output || copyto!(output, result)
+    return output
+end
+function SHTnsKit.synthesis_batch!(::SHTnsKit.GPU, cfg::SHTnsKit.SHTConfig, output::CuArray{T,3},
+                                   alm::CuArray{<:Complex,3}; real_output::Bool=true, use_rfft::Bool=false,
+                                   lcap::Int=cfg.lmax, precision::Symbol=:auto) where {T}
+    check_grid(cfg, output); check_spectral(cfg, alm); check_lcap(cfg, lcap)
+    size(output, 3) == size(alm, 3) || throw(DimensionMismatch("output and coefficient batches differ"))
+    if real_output && T <: Real
+        prec = precision_of(T, precision)
+        if (prec == SHTB_PREC_FP64 && T === Float64) || (prec == SHTB_PREC_MIXED && T === Float32)
+            return _synthesis!(output, cfg, dense3(alm, Complex{T}), lcap, prec)
+        end
+    elseif !real_output && T === ComplexF64
+        return _synthesis_cplx!(output, cfg, dense3(alm, ComplexF64), lcap)
+    end
+    !real_output && T <: Real && throw(ArgumentError("real plan output storage requires real_output=true"))
+    return _into!(output, synthesis_any(cfg, alm; real_output, use_rfft, lcap, precision))
+end
+SHTnsKit.synthesis_batch!(cfg::SHTnsKit.SHTConfig, output::CuArray{<:Number,3}, alm::CuArray{<:Complex,3};
+                          kwargs...) = SHTnsKit.synthesis_batch!(SHTnsKit.GPU(), cfg, output, alm; kwargs...)
+function SHTnsKit.analysis_batch!(::SHTnsKit.GPU, cfg::SHTnsKit.SHTConfig, output::CuArray{Complex{T},3},
+                                  f::CuArray{<:Number,3}; use_rfft::Bool=false, lcap::Int=cfg.lmax,
+                                  precision::Symbol=:auto) where {T}
+    check_grid(cfg, f); check_spectral(cfg, output); check_lcap(cfg, lcap)
+    size(output, 3) == size(f, 3) || throw(DimensionMismatch("output and field batches differ"))
+    if eltype(f) === T
+        prec = precision_of(T, precision)
+        if (prec == SHTB_PREC_FP64 && T === Float64) || (prec == SHTB_PREC_MIXED && T === Float32)
+            return _analysis!(output, cfg, f, lcap, prec)
+        end
+    elseif eltype(f) === ComplexF64 && T === Float64
+        return _analysis_cplx!(output, cfg, f, lcap)
+    end
+    return _into!(output, analysis_any(cfg, f; use_rfft, lcap, precision))
+end
+SHTnsKit.analysis_batch!(cfg::SHTnsKit.SHTConfig, output::CuArray{<:Complex,3}, f::CuArray{<:Number,3};
+                         kwargs...) = SHTnsKit.analysis_batch!(SHTnsKit.GPU(), cfg, output, f; kwargs...)
+
+# in-place single-field transforms, with a plan or a configuration (ext/SHTnsKitGPUExt.jl:1978-2020)
+SHTnsKit.synthesis!(::SHTnsKit.GPU, plan::SHTnsKit.SHTPlan, output::CuArray{<:Number,2}, alm::CuArray{<:Complex,2};
+                    real_output::Bool=true) =
+    (SHTnsKit.synthesis_batch!(SHTnsKit.GPU(), plan.cfg, as3(output), as3(alm); real_output); output)
+SHTnsKit.synthesis!(plan::SHTnsKit.SHTPlan, output::CuArray{<:Number,2}, alm::CuArray{<:Complex,2};
+                    real_output::Bool=true) = SHTnsKit.synthesis!(SHTnsKit.GPU(), plan, output, alm; real_output)
+SHTnsKit.analysis!(::SHTnsKit.GPU, plan::SHTnsKit.SHTPlan, output::CuArray{<:Complex,2}, f::CuArray{<:Number,2}) =
+    (SHTnsKit.analysis_batch!(SHTnsKit.GPU(), plan.cfg, as3(output), as3(f)); output)
+SHTnsKit.analysis!(plan::SHTnsKit.SHTPlan, output::CuArray{<:Complex,2}, f::CuArray{<:Number,2}) =
+    SHTnsKit.analysis!(SHTnsKit.GPU(), plan, output, f)
+function SHTnsKit.synthesis!(cfg::SHTnsKit.SHTConfig, output::CuArray{<:Number,2}, alm::CuArray{<:Complex,2};
+                             real_output::Bool=true, fft_scratch=nothing, use_rfft::Bool=false)
+    fft_scratch === nothing || throw(ArgumentError("CUDA scalar transforms do not accept fft_scratch"))
+    SHTnsKit.synthesis_batch!(SHTnsKit.GPU(), cfg, as3(output), as3(alm); real_output, use_rfft)
+    return output
+end
+function SHTnsKit.analysis!(cfg::SHTnsKit.SHTConfig, output::CuArray{<:Complex,2}, f::CuArray{<:Number,2};
+                            fft_scratch=nothing, use_rfft::Bool=false)
+    fft_scratch === nothing || throw(ArgumentError("CUDA scalar transforms do not accept fft_scratch"))
+    SHTnsKit.analysis_batch!(SHTnsKit.GPU(), cfg, as3(output), as3(f); use_rfft)
+    return output
+end
+
+# batched vector transforms (ext/SHTnsKitGPUExt.jl:1294-1315)
+SHTnsKit.synthesis_sphtor_batch(::SHTnsKit.GPU, cfg::SHTnsKit.SHTConfig, S::CuArray{<:Complex,3},
+                                T::CuArray{<:Complex,3}; real_output::Bool=true) =
+    _synthesis_sphtor(cfg, S, T; real_output)
+SHTnsKit.synthesis_sphtor_batch(cfg::SHTnsKit.SHTConfig, S::CuArray{<:Complex,3}, T::CuArray{<:Complex,3}; kwargs...) =
+    SHTnsKit.synthesis_sphtor_batch(SHTnsKit.GPU(), cfg, S, T; kwargs...)
+SHTnsKit.analysis_sphtor_batch(::SHTnsKit.GPU, cfg::SHTnsKit.SHTConfig, Vt::CuArray{<:Real,3}, Vp::CuArray{<:Real,3}) =
+    _analysis_sphtor(cfg, Vt, Vp)
+SHTnsKit.analysis_sphtor_batch(cfg::SHTnsKit.SHTConfig, Vt::CuArray{<:Real,3}, Vp::CuArray{<:Real,3}) =
+    SHTnsKit.analysis_sphtor_batch(SHTnsKit.GPU(), cfg, Vt, Vp)
+
+# in-place vector transforms with a plan (ext/SHTnsKitGPUExt.jl:1349-1364)
+function SHTnsKit.analysis_sphtor!(plan::SHTnsKit.SHTPlan, Sout::CuArray, Tout::CuArray, Vt::CuArray, Vp::CuArray)
+    S, T = _analysis_sphtor(plan.cfg, Vt, Vp)
+    copyto!(Sout, S); copyto!(Tout, T)
+    return Sout, Tout
+end
+function SHTnsKit.synthesis_sphtor!(plan::SHTnsKit.SHTPlan, Vt::CuArray, Vp::CuArray, S::CuArray, T::CuArray;
+                                    real_output::Bool=true)
+    A, B = _synthesis_sphtor(plan.cfg, S, T; real_output)
+    copyto!(Vt, A); copyto!(Vp, B)
+    return Vt, Vp
+end
 
 # ---------------------------------------------------------------- packed LM layout (src/transforms.jl:125-227)
 function _synthesis_packed(cfg, Q::CuVector{Complex{T}}, lcap::Int) where {T<:Union{Float32,Float64}}
     length(Q) == cfg.nlm || throw(DimensionMismatch("Qlm must have length $(cfg.nlm)"))
     f = CuArray{T}(undef, cfg.nlat, cfg.nlon)
     p = plan(cfg)
-    ws = workspace(p, OP_SYN, 1, dtype_of(T), prec_of(T))
+    ws = workspace(p, OP_SYN, 1, dtype_of(T), precision_of(T, :auto))
     check(ccall((:shtb_synthesis_packed, LIB), Cint,
                 (Ptr{Cvoid}, CuPtr{Cvoid}, CuPtr{Cvoid}, Cint, Cint, Cint, Cint, CuPtr{Cvoid}, Csize_t, Ptr{Cvoid}),
-                p.ptr, Q, f, 1, lcap, dtype_of(T), prec_of(T), ws, sizeof(ws), stream()), :synthesis_packed)
+                p.ptr, Q, f, 1, lcap, dtype_of(T), precision_of(T, :auto), ws, sizeof(ws), stream()), :synthesis_packed)
     return vec(f)
 end
 
@@ -191,10 +366,10 @@ function _analysis_packed(cfg, Vr::CuVector{T}, lcap::Int) where {T<:Union{Float
     length(Vr) == cfg.nlat * cfg.nlon || throw(DimensionMismatch("Vr must have length $(cfg.nlat * cfg.nlon)"))
     Q = CuArray{Complex{T}}(undef, cfg.nlm)
     p = plan(cfg)
-    ws = workspace(p, OP_ANA, 1, dtype_of(T), prec_of(T))
+    ws = workspace(p, OP_ANA, 1, dtype_of(T), precision_of(T, :auto))
     check(ccall((:shtb_analysis_packed, LIB), Cint,
                 (Ptr{Cvoid}, CuPtr{Cvoid}, CuPtr{Cvoid}, Cint, Cint, Cint, Cint, CuPtr{Cvoid}, Csize_t, Ptr{Cvoid}),
-                p.ptr, Vr, Q, 1, lcap, dtype_of(T), prec_of(T), ws, sizeof(ws), stream()), :analysis_packed)
+                p.ptr, Vr, Q, 1, lcap, dtype_of(T), precision_of(T, :auto), ws, sizeof(ws), stream()), :analysis_packed)
     return Q
 end
 
@@ -262,6 +437,39 @@ function ChainRulesCore.rrule(::typeof(SHTnsKit.analysis), cfg::SHTnsKit.SHTConf
         fbar = CuArray{Float64}(undef, cfg.nlat, cfg.nlon, 1)
         _adjoint(:shtb_analysis_adjoint, OP_SYN, cfg, (a,), (fbar,), 1)
         return ChainRulesCore.NoTangent(), ChainRulesCore.NoTangent(), reshape(fbar, size(f))
+    end
+    return alm, pullback
+end
+
+# batch rrules (ext/SHTnsKitAdvancedADExt.jl:95-135): one adjoint launch over all nfields
+# slices instead of a loop of per-slice adjoints
+function ChainRulesCore.rrule(::typeof(SHTnsKit.synthesis_batch), cfg::SHTnsKit.SHTConfig,
+                              alm::CuArray{ComplexF64,3}; real_output::Bool=true, use_rfft::Bool=false)
+    real_output || throw(SHTnsKit.BackendUnavailableError(:synthesis_batch, "adjoint of real_output=false is not implemented"))
+    f = SHTnsKit.synthesis_batch(cfg, alm; real_output, use_rfft)
+    function pullback(fbar)
+        fb = ChainRulesCore.unthunk(fbar)
+        fb isa ChainRulesCore.AbstractZero && return ChainRulesCore.NoTangent(), ChainRulesCore.NoTangent(), ChainRulesCore.ZeroTangent()
+        ybar = CuArray{Float64}(fb)
+        nf = size(ybar, 3)
+        abar = CuArray{ComplexF64}(undef, cfg.lmax + 1, cfg.mmax + 1, nf)
+        _adjoint(:shtb_synthesis_adjoint, OP_ANA, cfg, (ybar,), (abar,), nf)
+        return ChainRulesCore.NoTangent(), ChainRulesCore.NoTangent(), abar
+    end
+    return f, pullback
+end
+
+function ChainRulesCore.rrule(::typeof(SHTnsKit.analysis_batch), cfg::SHTnsKit.SHTConfig,
+                              f::CuArray{Float64,3}; use_rfft::Bool=false)
+    alm = SHTnsKit.analysis_batch(cfg, f; use_rfft)
+    function pullback(abar)
+        ab = ChainRulesCore.unthunk(abar)
+        ab isa ChainRulesCore.AbstractZero && return ChainRulesCore.NoTangent(), ChainRulesCore.NoTangent(), ChainRulesCore.ZeroTangent()
+        a = CuArray{ComplexF64}(ab)
+        nf = size(a, 3)
+        fbar = CuArray{Float64}(undef, cfg.nlat, cfg.nlon, nf)
+        _adjoint(:shtb_analysis_adjoint, OP_SYN, cfg, (a,), (fbar,), nf)
+        return ChainRulesCore.NoTangent(), ChainRulesCore.NoTangent(), fbar
     end
     return alm, pullback
 end
