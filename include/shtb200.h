@@ -256,7 +256,8 @@ int shtb_synthesis_noalloc(const shtb_plan* plan, const void* alm, void* f, int 
  * run one configuration per call (src/core_transforms.jl, src/batch_transforms.jl):
  * a group runs every member's tiles in one persistent launch per stage (B packing,
  * order-GEMM synthesis, FFT synthesis, FFT analysis, order-GEMM analysis), work items
- * sorted by cost, the stage launches captured once in a CUDA graph and replayed.
+ * sorted by cost and claimed by the CTAs from a device work counter, the stage launches
+ * captured once in a CUDA graph and replayed.
  * Members must use lcap = lmax and mres = 1. Buffers (device pointers, per member):
  * alm_in and alm_out are (lmax+1, mmax+1, nfields) complex FP32 (Julia column-major),
  * grid is (nlat, nlon, nfields) FP32. Results equal those of shtb_synthesis /
@@ -271,9 +272,10 @@ int shtb_group_bind(shtb_group* group, void* const* alm_in, void* const* grid, v
 int shtb_group_roundtrip(shtb_group* group, void* stream);
 /* The same stages launched directly (no graph); op = SHTB_OP_SYNTHESIS, SHTB_OP_ANALYSIS or -1 (both). */
 int shtb_group_launch(shtb_group* group, int op, void* stream);
-/* Time the candidate launch shapes on the bound buffers and keep the fastest (blocking). */
+/* Time the candidate launch shapes on the bound buffers and keep the fastest (blocking):
+ * FFT latitude pairs per CTA x FFT CTAs per SM, then GEMM CTAs per SM of each GEMM stage. */
 int shtb_group_autotune(shtb_group* group, void* stream);
-/* Launch shape in use: FFT latitude pairs per CTA, FFT CTAs, GEMM CTAs. */
+/* Launch shape in use: FFT latitude pairs per CTA, FFT CTAs, CTAs of the synthesis GEMM. */
 int shtb_group_config(const shtb_group* group, int* fft_pairs, int* fft_ctas, int* gemm_ctas);
 /* After the last roundtrip completed: per-member completion time in ns after its start (n values). */
 int shtb_group_latency_ns(const shtb_group* group, uint64_t* ns);

@@ -455,23 +455,31 @@ __global__ void __launch_bounds__(512) fft_ana_kernel(const __grid_constant__ FF
     fft_ana_body<T, H, GENERIC>(J, blockIdx.x * H, blockIdx.y, smem_raw);
 }
 
-// Persistent FFTs over many independent transforms: CTA i runs items i, i + gridDim.x,
-// ...; item = (transform, first latitude pair, field). Shared memory is sized for the
-// longest row of the group.
+// Persistent FFTs over many independent transforms; item = (transform, first latitude
+// pair, field), list sorted by decreasing row length. Each CTA claims the next item from
+// the device counter *queue (zero at launch) when it finishes one. Shared memory is sized
+// for the longest row of the group.
 template <typename T, int H, bool GENERIC, bool SYN>
 __global__ void __launch_bounds__(512) fft_group_kernel(const FFTJob<T>* __restrict__ jobs,
-                                                        const int4* __restrict__ items, int nitems) {
+                                                        const int4* __restrict__ items, int nitems,
+                                                        int* __restrict__ queue) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ FFTJob<T> sj;
-  for (int i = blockIdx.x; i < nitems; i += gridDim.x) {
-    const int4 it = items[i];
-    if (threadIdx.x == 0) sj = jobs[it.x];
+  __shared__ int4 s_it;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const int i = atomicAdd(queue, 1);
+      s_it = (i < nitems) ? items[i] : make_int4(-1, 0, 0, 0);
+      if (i < nitems) sj = jobs[s_it.x];
+    }
     __syncthreads();
+    const int4 it = s_it;
+    if (it.x < 0) break;
     if (SYN)
       fft_syn_body<T, H, GENERIC>(sj, it.y, it.z, smem_raw);
     else
       fft_ana_body<T, H, GENERIC>(sj, it.y, it.z, smem_raw);
-    __syncthreads();
+    __syncthreads();   // sj, s_it and the shared rows are rewritten for the next item
   }
 }
 
@@ -748,22 +756,22 @@ bool fft_plan_generic(const shtb_plan* p) { return fft_generic(p); }
 
 template <int H, bool GENERIC>
 static int launch_fft_group_h(int syn, const void* jobs, const int4* items, int nitems, int grid, size_t smem,
-                              cudaStream_t st) {
+                              int* queue, cudaStream_t st) {
   auto kern = syn ? fft_group_kernel<float, H, GENERIC, true> : fft_group_kernel<float, H, GENERIC, false>;
   SHTB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "group fft smem attr");
-  kern<<<grid, 512, smem, st>>>((const FFTJob<float>*)jobs, items, nitems);
+  kern<<<grid, 512, smem, st>>>((const FFTJob<float>*)jobs, items, nitems, queue);
   count_launch();
   SHTB_TRY_CUDA(cudaGetLastError(), "group fft launch");
   return SHTB_OK;
 }
 
 int launch_fft_group_f32(int syn, int h, bool generic, const void* jobs, const int4* items, int nitems, int grid,
-                         size_t smem, cudaStream_t st) {
+                         size_t smem, int* queue, cudaStream_t st) {
   if (nitems <= 0) return SHTB_OK;
   if (smem > 227 * 1024) return set_error(SHTB_ERR_UNSUPPORTED, "group FFT tile does not fit in shared memory");
-#define SHTB_GFFT(H_)                                                                   \
-  if (h == H_) return generic ? launch_fft_group_h<H_, true>(syn, jobs, items, nitems, grid, smem, st) \
-                              : launch_fft_group_h<H_, false>(syn, jobs, items, nitems, grid, smem, st);
+#define SHTB_GFFT(H_)                                                                                 \
+  if (h == H_) return generic ? launch_fft_group_h<H_, true>(syn, jobs, items, nitems, grid, smem, queue, st) \
+                              : launch_fft_group_h<H_, false>(syn, jobs, items, nitems, grid, smem, queue, st);
   SHTB_GFFT(16) SHTB_GFFT(8) SHTB_GFFT(4) SHTB_GFFT(2)
 #undef SHTB_GFFT
   return set_error(SHTB_ERR_BAD_ARG, "group FFT: unsupported pairs per CTA");

@@ -16,6 +16,7 @@
 // its mirror, the south rows of two pairs are adjacent, and pair-pairs start on 16-byte
 // boundaries of the Fourier buffer); other sizes use the general kernels.
 // One CTA transforms 2 HP latitude pairs (HP pair-pairs) of one field with 128 HP threads.
+#include <algorithm>
 #include <cstring>
 
 #include "fft.cuh"
@@ -247,11 +248,9 @@ __device__ __forceinline__ size_t f2_btile_base(int im, int par, int p, int k, i
   return (((size_t)im * 2 + par) * nks8 + (p >> 3)) * (size_t)btile_nfp(nf) * 16 + (size_t)(k >> 6) * 1024;
 }
 
+// Pairs p0 .. p0 + 2 HP - 1 of field k.
 template <int HP>
-__global__ void __launch_bounds__(128 * HP, 4 / HP) ana_kernel(const __grid_constant__ Job J) {
-  extern __shared__ __align__(16) float4 X[];
-  __shared__ float wfac[2 * HP];
-  const int k = blockIdx.x, p0 = blockIdx.y * (2 * HP);
+__device__ __forceinline__ void ana_body(const Job& J, int k, int p0, float4* X, float* wfac) {
   const PlanDev& P = J.P;
   const int N = J.fd.n, npair = P.npair;
   for (int h = threadIdx.x; h < 2 * HP; h += blockDim.x) {
@@ -311,6 +310,13 @@ __global__ void __launch_bounds__(128 * HP, 4 / HP) ana_kernel(const __grid_cons
   }
 }
 
+template <int HP>
+__global__ void __launch_bounds__(128 * HP, 4 / HP) ana_kernel(const __grid_constant__ Job J) {
+  extern __shared__ __align__(16) float4 X[];
+  __shared__ float wfac[2 * HP];
+  ana_body<HP>(J, blockIdx.x, blockIdx.y * (2 * HP), X, wfac);
+}
+
 // ----------------------------------------------------------------------------- synthesis
 template <int HP, int RL>
 __device__ __forceinline__ void last_to_grid(const float4* X, const Job& J, float* __restrict__ out, int p0,
@@ -342,11 +348,9 @@ __device__ __forceinline__ void last_to_grid(const float4* X, const Job& J, floa
   }
 }
 
+// Pairs p0 .. p0 + 2 HP - 1 of field k.
 template <int HP>
-__global__ void __launch_bounds__(128 * HP, 4 / HP) syn_kernel(const __grid_constant__ Job J) {
-  extern __shared__ __align__(16) float4 X[];
-  __shared__ float gfac[2 * HP];
-  const int p0 = blockIdx.x * (2 * HP), k = blockIdx.y;
+__device__ __forceinline__ void syn_body(const Job& J, int k, int p0, float4* X, float* gfac) {
   const PlanDev& P = J.P;
   const int N = J.fd.n, npair = P.npair;
   const int mlim = J.mlim;
@@ -420,6 +424,42 @@ __global__ void __launch_bounds__(128 * HP, 4 / HP) syn_kernel(const __grid_cons
   }
 }
 
+template <int HP>
+__global__ void __launch_bounds__(128 * HP, 4 / HP) syn_kernel(const __grid_constant__ Job J) {
+  extern __shared__ __align__(16) float4 X[];
+  __shared__ float gfac[2 * HP];
+  syn_body<HP>(J, blockIdx.y, blockIdx.x * (2 * HP), X, gfac);
+}
+
+// Persistent FFTs of many transforms (uneven batches): item = (transform, first pair of a
+// block of 2 HP pairs, field), list sorted by decreasing row length; each CTA claims the
+// next item from the device counter *queue (zero at launch) when it finishes one. Shared
+// memory is sized for the longest row of the group.
+template <int HP, bool SYN>
+__global__ void __launch_bounds__(128 * HP, 4 / HP) group_kernel(const Job* __restrict__ jobs,
+                                                                const int4* __restrict__ items, int nitems,
+                                                                int* __restrict__ queue) {
+  extern __shared__ __align__(16) float4 X[];
+  __shared__ float fac[2 * HP];
+  __shared__ Job sj;
+  __shared__ int4 s_it;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const int i = atomicAdd(queue, 1);
+      s_it = (i < nitems) ? items[i] : make_int4(-1, 0, 0, 0);
+      if (i < nitems) sj = jobs[s_it.x];
+    }
+    __syncthreads();
+    const int4 it = s_it;
+    if (it.x < 0) break;
+    if (SYN)
+      syn_body<HP>(sj, it.z, it.y, X, fac);
+    else
+      ana_body<HP>(sj, it.z, it.y, X, fac);
+    __syncthreads();   // sj, s_it, fac and X are rewritten for the next item
+  }
+}
+
 }  // namespace f2
 
 // Whether the packed-pair kernels take this plan's FP32 FFTs.
@@ -466,6 +506,39 @@ int launch_fft2_ana(const shtb_plan* p, const float* grid, void* W, int nf, int 
   prof_begin(st);
   f2::ana_kernel<HP><<<grd, 128 * HP, smem, st>>>(J);
   SHTB_LAUNCHED("fft analysis kernel");
+  return SHTB_OK;
+}
+
+// ---------------------------------------------------------------- grouped transforms
+size_t fft2_job_bytes() { return sizeof(f2::Job); }
+
+int fft2_group_pairs() { return 2 * kFft2HP; }
+
+size_t fft2_group_smem(const shtb_plan* p) { return (size_t)f2::smem_elems<kFft2HP>(p->fft.n) * 16; }
+
+void fft2_fill_job(const shtb_plan* p, int syn, const void* W, void* grid, int nf, void* host_job) {
+  const int mlim = std::min(p->mmax, p->lmax);
+  f2::Job J = syn ? fft2_job(p, p->d_rinv, p->phi_inv_scale / p->nlon, nf, mlim)
+                  : fft2_job(p, p->d_rev, p->ana_scale, nf, mlim);
+  J.grid = (float*)grid;
+  if (syn)
+    J.Win = (const float2*)W;
+  else
+    J.Wout = (float*)const_cast<void*>(W);
+  std::memcpy(host_job, &J, sizeof(J));
+}
+
+int launch_fft2_group(int syn, const void* jobs, const int4* items, int nitems, int grid, size_t smem, int* queue,
+                      cudaStream_t st) {
+  if (nitems <= 0) return SHTB_OK;
+  constexpr int HP = kFft2HP;
+  if (smem > 227 * 1024) return set_error(SHTB_ERR_UNSUPPORTED, "group FFT tile does not fit in shared memory");
+  auto kern = syn ? f2::group_kernel<HP, true> : f2::group_kernel<HP, false>;
+  SHTB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                "group fft2 smem attr");
+  kern<<<grid, 128 * HP, smem, st>>>((const f2::Job*)jobs, items, nitems, queue);
+  count_launch();
+  SHTB_TRY_CUDA(cudaGetLastError(), "group fft2 launch");
   return SHTB_OK;
 }
 

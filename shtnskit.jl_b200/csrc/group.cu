@@ -5,18 +5,25 @@
 //
 // Every stage owns a list of work items over all members — GEMM tiles (member, order,
 // first latitude pair or degree, parity) and FFT tiles (member, first latitude pair,
-// field) — sorted by decreasing cost. A stage launches min(items, SMs x CTAs per SM)
-// CTAs and CTA i runs items i, i + gridDim.x, ...: the longest tiles start first and
-// the short ones fill in behind them, so a batch of mixed sizes keeps every SM busy
-// without one launch per member. The six launches of a roundtrip (a start marker plus
-// the five stages) are captured once into a CUDA graph and replayed.
+// field) — sorted by decreasing cost, and a device work counter (zeroed by a memset at
+// the start of every roundtrip). A stage launches min(items, SMs x CTAs per SM)
+// persistent CTAs; each claims the next item with an atomicAdd on the counter whenever
+// it has room for one, so the longest tiles start first and the short ones fill in
+// behind whichever CTA frees up first, and a batch of mixed sizes keeps every SM busy
+// without one launch per member. Members whose FFTs the packed-pair kernels take
+// (fft2_applicable) run them in a second persistent FFT kernel per direction, forked
+// beside the general one, so every member's results equal its single-plan calls bit for
+// bit. The memset and the six launches of a roundtrip (a start marker plus the five
+// stages; eight when both FFT kinds are present) are captured once into a CUDA graph and
+// replayed.
 //
 // Per-member latency: the start marker records %globaltimer; the analysis GEMM stores,
 // per member, the time its last tile finished.
 //
-// Launch-shape autotuning times every FFT shape (latitude pairs per CTA; 1, 2 or 4 CTAs
-// per SM, the extra CTAs queueing behind the resident ones) on the bound buffers and
-// keeps the fastest; the shape changes no result.
+// Launch-shape autotuning times, on the bound buffers, every FFT shape (latitude pairs per
+// CTA; 1, 2 or 4 CTAs per SM, the extra CTAs queueing behind the resident ones), then one
+// or two GEMM CTAs per SM for the synthesis and for the analysis GEMM, and keeps the
+// fastest; the shape changes no result.
 #include <algorithm>
 #include <numeric>
 #include <vector>
@@ -36,6 +43,8 @@ __global__ void group_start_kernel(unsigned long long* done, int n, unsigned lon
 
 static size_t align256(size_t v) { return (v + 255) / 256 * 256; }
 
+constexpr int kGroupQueues = 7;   // pack, GEMM syn, FFT syn, FFT ana, GEMM ana, fft2 syn, fft2 ana
+
 }  // namespace shtb
 
 using namespace shtb;
@@ -45,11 +54,17 @@ struct shtb_group {
   std::vector<const shtb_plan*> plans;
   std::vector<int> nf;
   std::vector<size_t> woff;             // byte offset of member t's Fourier buffer
-  size_t argsz = 0, jobsz = 0;
+  std::vector<char> f2;                 // member runs the packed-pair FFTs (fft2_applicable)
+  size_t argsz = 0, jobsz = 0, job2sz = 0;
   // device memory: [args syn | args ana | jobs syn | jobs ana | done | t0 | gemm items | W]
   unsigned char* dmem = nullptr;
   unsigned char *d_args_syn = nullptr, *d_args_ana = nullptr, *d_jobs_syn = nullptr, *d_jobs_ana = nullptr;
+  unsigned char *d_jobs2_syn = nullptr, *d_jobs2_ana = nullptr;
+  int4* d_items_fft2 = nullptr;         // packed-pair FFT items (members with f2 set)
+  int n_fft2 = 0, fft2_ctas = 148;
+  size_t fft2_smem = 0;
   unsigned long long *d_done = nullptr, *d_t0 = nullptr;
+  int* d_queue = nullptr;               // work counters (kGroupQueues)
   int4 *d_items_syn = nullptr, *d_items_ana = nullptr;
   int2* d_items_pack = nullptr;
   int n_syn = 0, n_ana = 0, n_pack = 0;
@@ -62,8 +77,9 @@ struct shtb_group {
   size_t fft_smem = 0;
   bool bound = false;
   // graph
-  cudaStream_t priv = nullptr;
-  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  cudaStream_t priv = nullptr, aux = nullptr;   // aux: the packed-pair FFTs, forked beside the others
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr, ev_fork = nullptr, ev_join = nullptr;
+  int graph_kernels = 0;
   cudaGraphExec_t exec = nullptr;
 };
 
@@ -72,7 +88,10 @@ static void group_free(shtb_group* g) {
   if (g->exec) cudaGraphExecDestroy(g->exec);
   if (g->ev_in) cudaEventDestroy(g->ev_in);
   if (g->ev_out) cudaEventDestroy(g->ev_out);
+  if (g->ev_fork) cudaEventDestroy(g->ev_fork);
+  if (g->ev_join) cudaEventDestroy(g->ev_join);
   if (g->priv) cudaStreamDestroy(g->priv);
+  if (g->aux) cudaStreamDestroy(g->aux);
   if (g->d_items_fft) cudaFree(g->d_items_fft);
   if (g->dmem) cudaFree(g->dmem);
   delete g;
@@ -89,6 +108,7 @@ static int build_fft_items(shtb_group* g, int h) {
   std::vector<int> cost;
   for (int t = 0; t < g->n; ++t) {
     const shtb_plan* p = g->plans[t];
+    if (g->f2[t]) continue;
     for (int p0 = 0; p0 < p->npair; p0 += h)
       for (int k = 0; k < g->nf[t]; ++k) {
         it.push_back(make_int4(t, p0, k, 0));
@@ -111,7 +131,8 @@ static int build_fft_items(shtb_group* g, int h) {
 
 static size_t group_fft_smem(const shtb_group* g, int h) {
   size_t s = 0;
-  for (const shtb_plan* p : g->plans) s = std::max(s, fft_group_smem_f32(p, h));
+  for (int t = 0; t < g->n; ++t)
+    if (!g->f2[t]) s = std::max(s, fft_group_smem_f32(g->plans[t], h));
   return s;
 }
 
@@ -125,24 +146,46 @@ static int set_fft_shape(shtb_group* g, int h, int ctas) {
   return SHTB_OK;
 }
 
+// One FFT stage: the packed-pair kernel of the fft2 members on the aux stream, forked from
+// and joined back into st, beside the general kernel of the others on st.
+static int group_fft_stage(shtb_group* g, int syn, int* q_gen, int* q_f2, cudaStream_t st) {
+  int rc;
+  const bool fork = g->n_fft2 > 0 && g->n_fft > 0;
+  if (fork) {
+    SHTB_TRY_CUDA(cudaEventRecord(g->ev_fork, st), "group fork");
+    SHTB_TRY_CUDA(cudaStreamWaitEvent(g->aux, g->ev_fork, 0), "group fork");
+  }
+  if ((rc = launch_fft2_group(syn, syn ? g->d_jobs2_syn : g->d_jobs2_ana, g->d_items_fft2, g->n_fft2, g->fft2_ctas,
+                              g->fft2_smem, q_f2, fork ? g->aux : st)))
+    return rc;
+  if ((rc = launch_fft_group_f32(syn, g->fft_h, g->generic, syn ? g->d_jobs_syn : g->d_jobs_ana, g->d_items_fft,
+                                 g->n_fft, g->fft_ctas, g->fft_smem, q_gen, st)))
+    return rc;
+  if (fork) {
+    SHTB_TRY_CUDA(cudaEventRecord(g->ev_join, g->aux), "group join");
+    SHTB_TRY_CUDA(cudaStreamWaitEvent(st, g->ev_join, 0), "group join");
+  }
+  return SHTB_OK;
+}
+
 static int group_launch_stages(shtb_group* g, int op, cudaStream_t st) {
   int rc;
+  int* q = g->d_queue;
+  SHTB_TRY_CUDA(cudaMemsetAsync(q, 0, kGroupQueues * sizeof(int), st), "group work counters");
   if (op != SHTB_OP_ANALYSIS) {
     group_start_kernel<<<1, 256, 0, st>>>(g->d_done, g->n, g->d_t0);
     count_launch();
     SHTB_TRY_CUDA(cudaGetLastError(), "group start marker");
-    if ((rc = launch_pack_group(g->d_args_syn, g->d_items_pack, g->n_pack, std::min(g->n_pack, 24 * g->nsm), st)))
+    if ((rc = launch_pack_group(g->d_args_syn, g->d_items_pack, g->n_pack, std::min(g->n_pack, 24 * g->nsm), q, st)))
       return rc;
-    if ((rc = launch_gemm_group(0, g->d_args_syn, g->d_items_syn, g->n_syn, g->gemm_ctas_syn, nullptr, st))) return rc;
-    if ((rc = launch_fft_group_f32(1, g->fft_h, g->generic, g->d_jobs_syn, g->d_items_fft, g->n_fft, g->fft_ctas,
-                                   g->fft_smem, st)))
+    if ((rc = launch_gemm_group(0, g->d_args_syn, g->d_items_syn, g->n_syn, g->gemm_ctas_syn, nullptr, q + 1, st)))
       return rc;
+    if ((rc = group_fft_stage(g, 1, q + 2, q + 5, st))) return rc;
   }
   if (op != SHTB_OP_SYNTHESIS) {
-    if ((rc = launch_fft_group_f32(0, g->fft_h, g->generic, g->d_jobs_ana, g->d_items_fft, g->n_fft, g->fft_ctas,
-                                   g->fft_smem, st)))
+    if ((rc = group_fft_stage(g, 0, q + 3, q + 6, st))) return rc;
+    if ((rc = launch_gemm_group(1, g->d_args_ana, g->d_items_ana, g->n_ana, g->gemm_ctas_ana, g->d_done, q + 4, st)))
       return rc;
-    if ((rc = launch_gemm_group(1, g->d_args_ana, g->d_items_ana, g->n_ana, g->gemm_ctas_ana, g->d_done, st))) return rc;
   }
   return SHTB_OK;
 }
@@ -179,11 +222,36 @@ extern "C" int shtb_group_create(shtb_group** out, const shtb_plan* const* plans
     group_free(g);
     return rc;
   };
+  g->f2.resize(n);
   for (int t = 0; t < n; ++t) {
     int rc = mixed_prepare(plans[t], 0);
     if (rc) return fail(rc);
-    g->generic = g->generic || fft_plan_generic(plans[t]);
+    g->f2[t] = fft2_applicable(plans[t]) ? 1 : 0;
+    if (!g->f2[t]) g->generic = g->generic || fft_plan_generic(plans[t]);
   }
+  // packed-pair FFT items: blocks of fft2_group_pairs() pairs, longest rows first
+  std::vector<int4> f2items;
+  {
+    std::vector<int> cost;
+    const int hp = fft2_group_pairs();
+    for (int t = 0; t < n; ++t) {
+      if (!g->f2[t]) continue;
+      g->fft2_smem = std::max(g->fft2_smem, fft2_group_smem(plans[t]));
+      for (int p0 = 0; p0 < plans[t]->npair; p0 += hp)
+        for (int k = 0; k < nfields[t]; ++k) {
+          f2items.push_back(make_int4(t, p0, k, 0));
+          cost.push_back(plans[t]->nlon);
+        }
+    }
+    std::vector<int> ord(f2items.size());
+    std::iota(ord.begin(), ord.end(), 0);
+    std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    std::vector<int4> sorted(f2items.size());
+    for (size_t i = 0; i < ord.size(); ++i) sorted[i] = f2items[ord[i]];
+    f2items.swap(sorted);
+  }
+  g->n_fft2 = (int)f2items.size();
+  g->fft2_ctas = std::max(1, std::min(g->nsm, g->n_fft2));
   // GEMM tiles, most K-steps first
   const int TM = mixed_group_tile_rows();
   std::vector<int4> syn, ana;
@@ -236,10 +304,14 @@ extern "C" int shtb_group_create(shtb_group** out, const shtb_plan* const* plans
   // one device allocation
   g->argsz = mixed_args_bytes();
   g->jobsz = fft_job_bytes_f32();
+  g->job2sz = fft2_job_bytes();
   size_t o = 0;
   auto take = [&](size_t b) { size_t r = o; o = align256(o + b); return r; };
   const size_t o_as = take(n * g->argsz), o_aa = take(n * g->argsz), o_js = take(n * g->jobsz), o_ja = take(n * g->jobsz);
-  const size_t o_done = take(n * 8), o_t0 = take(8), o_is = take(syn.size() * sizeof(int4)),
+  const size_t o_j2s = take(n * g->job2sz), o_j2a = take(n * g->job2sz),
+               o_i2 = take(std::max<size_t>(1, f2items.size()) * sizeof(int4));
+  const size_t o_done = take(n * 8), o_t0 = take(8), o_q = take(kGroupQueues * sizeof(int)),
+               o_is = take(syn.size() * sizeof(int4)),
                o_ia = take(ana.size() * sizeof(int4)), o_ip = take(pack.size() * sizeof(int2));
   g->woff.resize(n);
   size_t wbytes = 0;
@@ -255,8 +327,12 @@ extern "C" int shtb_group_create(shtb_group** out, const shtb_plan* const* plans
   g->d_args_ana = g->dmem + o_aa;
   g->d_jobs_syn = g->dmem + o_js;
   g->d_jobs_ana = g->dmem + o_ja;
+  g->d_jobs2_syn = g->dmem + o_j2s;
+  g->d_jobs2_ana = g->dmem + o_j2a;
+  g->d_items_fft2 = (int4*)(g->dmem + o_i2);
   g->d_done = (unsigned long long*)(g->dmem + o_done);
   g->d_t0 = (unsigned long long*)(g->dmem + o_t0);
+  g->d_queue = (int*)(g->dmem + o_q);
   g->d_items_syn = (int4*)(g->dmem + o_is);
   g->d_items_ana = (int4*)(g->dmem + o_ia);
   g->d_items_pack = (int2*)(g->dmem + o_ip);
@@ -264,10 +340,15 @@ extern "C" int shtb_group_create(shtb_group** out, const shtb_plan* const* plans
   e = cudaMemcpy(g->d_items_syn, syn.data(), syn.size() * sizeof(int4), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(g->d_items_ana, ana.data(), ana.size() * sizeof(int4), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(g->d_items_pack, pack.data(), pack.size() * sizeof(int2), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && !f2items.empty())
+    e = cudaMemcpy(g->d_items_fft2, f2items.data(), f2items.size() * sizeof(int4), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemset(g->d_done, 0, n * 8);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&g->priv, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&g->aux, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->ev_in, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->ev_out, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->ev_fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->ev_join, cudaEventDisableTiming);
   if (e != cudaSuccess) return fail(set_error(SHTB_ERR_CUDA, std::string("group setup: ") + cudaGetErrorString(e)));
   // default FFT shape: the most latitude pairs per CTA that fit in ~200 KB
   int h = 16;
@@ -289,7 +370,8 @@ extern "C" int shtb_group_bind(shtb_group* g, void* const* alm_in, void* const* 
   if (!alm_in || !grid || !alm_out) return set_error(SHTB_ERR_BAD_ARG, "NULL buffer array");
   int rc = check_device(g);
   if (rc) return rc;
-  std::vector<unsigned char> as(g->n * g->argsz), aa(g->n * g->argsz), js(g->n * g->jobsz), ja(g->n * g->jobsz);
+  std::vector<unsigned char> as(g->n * g->argsz), aa(g->n * g->argsz), js(g->n * g->jobsz), ja(g->n * g->jobsz),
+      j2s(g->n * g->job2sz), j2a(g->n * g->job2sz);
   for (int t = 0; t < g->n; ++t) {
     if (!alm_in[t] || !grid[t] || !alm_out[t])
       return set_error(SHTB_ERR_BAD_ARG, "NULL buffer for member " + std::to_string(t));
@@ -301,11 +383,17 @@ extern "C" int shtb_group_bind(shtb_group* g, void* const* alm_in, void* const* 
     mixed_fill_args(p, 1, W, alm_out[t], g->nf[t], aa.data() + t * g->argsz);
     fft_fill_job_f32(p, 1, W, grid[t], g->nf[t], js.data() + t * g->jobsz);
     fft_fill_job_f32(p, 0, W, grid[t], g->nf[t], ja.data() + t * g->jobsz);
+    if (g->f2[t]) {
+      fft2_fill_job(p, 1, W, grid[t], g->nf[t], j2s.data() + t * g->job2sz);
+      fft2_fill_job(p, 0, W, grid[t], g->nf[t], j2a.data() + t * g->job2sz);
+    }
   }
   SHTB_TRY_CUDA(cudaMemcpy(g->d_args_syn, as.data(), as.size(), cudaMemcpyHostToDevice), "group bind");
   SHTB_TRY_CUDA(cudaMemcpy(g->d_args_ana, aa.data(), aa.size(), cudaMemcpyHostToDevice), "group bind");
   SHTB_TRY_CUDA(cudaMemcpy(g->d_jobs_syn, js.data(), js.size(), cudaMemcpyHostToDevice), "group bind");
   SHTB_TRY_CUDA(cudaMemcpy(g->d_jobs_ana, ja.data(), ja.size(), cudaMemcpyHostToDevice), "group bind");
+  SHTB_TRY_CUDA(cudaMemcpy(g->d_jobs2_syn, j2s.data(), j2s.size(), cudaMemcpyHostToDevice), "group bind");
+  SHTB_TRY_CUDA(cudaMemcpy(g->d_jobs2_ana, j2a.data(), j2a.size(), cudaMemcpyHostToDevice), "group bind");
   g->bound = true;
   drop_graph(g);
   return SHTB_OK;
@@ -331,7 +419,8 @@ extern "C" int shtb_group_roundtrip(shtb_group* g, void* stream) {
     rc = group_launch_stages(g, -1, g->priv);
     cudaGraph_t graph = nullptr;
     const cudaError_t e = cudaStreamEndCapture(g->priv, &graph);
-    count_launch(-(int)(shtb_launch_count(0) - before));   // capturing runs no kernel
+    g->graph_kernels = (int)(shtb_launch_count(0) - before);
+    count_launch(-g->graph_kernels);   // capturing runs no kernel
     if (rc) {
       if (graph) cudaGraphDestroy(graph);
       return rc;
@@ -348,7 +437,7 @@ extern "C" int shtb_group_roundtrip(shtb_group* g, void* stream) {
   SHTB_TRY_CUDA(cudaEventRecord(g->ev_in, st), "group event");
   SHTB_TRY_CUDA(cudaStreamWaitEvent(g->priv, g->ev_in, 0), "group wait");
   SHTB_TRY_CUDA(cudaGraphLaunch(g->exec, g->priv), "group graph launch");
-  count_launch(6);   // start marker, B packing and four stage kernels
+  count_launch(g->graph_kernels);   // start marker, B packing, GEMMs and the FFT kernels
   SHTB_TRY_CUDA(cudaEventRecord(g->ev_out, g->priv), "group event");
   SHTB_TRY_CUDA(cudaStreamWaitEvent(st, g->ev_out, 0), "group wait");
   return SHTB_OK;
@@ -364,37 +453,69 @@ extern "C" int shtb_group_autotune(shtb_group* g, void* stream) {
   cudaEvent_t e0, e1;
   SHTB_TRY_CUDA(cudaEventCreate(&e0), "event");
   SHTB_TRY_CUDA(cudaEventCreate(&e1), "event");
+  // best of three roundtrips with the current shape
+  auto time_shape = [&](float& ms_min) {
+    ms_min = 1e30f;
+    for (int rep = 0; rep < 3; ++rep) {
+      cudaEventRecord(e0, g->priv);
+      const int r = group_launch_stages(g, -1, g->priv);
+      cudaEventRecord(e1, g->priv);
+      if (r) return r;
+      if (cudaEventSynchronize(e1) == cudaSuccess) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms_min = std::min(ms_min, ms);
+      }
+    }
+    return SHTB_OK;
+  };
   float best = 1e30f;
   int bh = g->fft_h, bc = g->fft_ctas;
   for (int h : {16, 8, 4}) {
+    if (g->n_fft == 0) {   // only packed-pair FFTs: their shape is fixed
+      if ((rc = time_shape(best))) break;
+      break;
+    }
     if (group_fft_smem(g, h) > 200 * 1024) continue;
     for (int mult : {1, 2, 4}) {
-      if ((rc = set_fft_shape(g, h, g->nsm * mult))) break;
-      float ms_min = 1e30f;
-      for (int rep = 0; rep < 3 && !rc; ++rep) {
-        cudaEventRecord(e0, g->priv);
-        rc = group_launch_stages(g, -1, g->priv);
-        cudaEventRecord(e1, g->priv);
-        if (!rc && cudaEventSynchronize(e1) == cudaSuccess) {
-          float ms = 0.f;
-          cudaEventElapsedTime(&ms, e0, e1);
-          ms_min = std::min(ms_min, ms);
-        }
-      }
-      if (rc) break;
-      if (ms_min < best) {
-        best = ms_min;
+      float ms;
+      if ((rc = set_fft_shape(g, h, g->nsm * mult)) || (rc = time_shape(ms))) break;
+      if (ms < best) {
+        best = ms;
         bh = h;
         bc = g->fft_ctas;
       }
     }
     if (rc) break;
   }
+  if (!rc && g->n_fft > 0) rc = set_fft_shape(g, bh, bc);
+  // GEMM CTAs per SM (the kernel's resources allow two), synthesis then analysis
+  for (int which = 0; which < 2 && !rc; ++which) {
+    int& ctas = which == 0 ? g->gemm_ctas_syn : g->gemm_ctas_ana;
+    const int nitems = which == 0 ? g->n_syn : g->n_ana;
+    int keep = ctas;
+    for (int mult : {1, 2}) {
+      const int c = std::max(1, std::min(mult * g->nsm, nitems));
+      if (c == keep) continue;
+      const int prev = ctas;
+      ctas = c;
+      float ms;
+      if ((rc = time_shape(ms))) break;
+      if (ms < best) {
+        best = ms;
+        keep = c;
+      } else {
+        ctas = prev;
+      }
+    }
+    ctas = keep;
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc) return rc;
   SHTB_TRY_CUDA(cudaStreamSynchronize(g->priv), "group autotune");
-  return set_fft_shape(g, bh, bc);
+  drop_graph(g);
+  return SHTB_OK;
 }
 
 extern "C" int shtb_group_config(const shtb_group* g, int* fft_pairs, int* fft_ctas, int* gemm_ctas) {

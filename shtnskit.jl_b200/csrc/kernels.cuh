@@ -76,13 +76,20 @@ void mixed_fill_args(const shtb_plan* p, int mode, const void* in, void* out, in
 int mixed_group_ksteps(const shtb_plan* p, int mode, int im, int par);
 int mixed_group_tile_rows();
 int launch_gemm_group(int mode, const void* targs, const int4* items, int nitems, int grid, unsigned long long* done,
-                      cudaStream_t st);
-int launch_pack_group(const void* targs, const int2* items, int nitems, int grid, cudaStream_t st);
+                      int* queue, cudaStream_t st);
+int launch_pack_group(const void* targs, const int2* items, int nitems, int grid, int* queue, cudaStream_t st);
 size_t fft_job_bytes_f32();
 void fft_fill_job_f32(const shtb_plan* p, int syn, const void* W, void* grid, int nf, void* host_job);
 size_t fft_group_smem_f32(const shtb_plan* p, int h);
 bool fft_plan_generic(const shtb_plan* p);
 int launch_fft_group_f32(int syn, int h, bool generic, const void* jobs, const int4* items, int nitems, int grid,
-                         size_t smem, cudaStream_t st);
+                         size_t smem, int* queue, cudaStream_t st);
+// the packed-pair FP32 FFTs of fft2_applicable members (2 HP latitude pairs per item)
+size_t fft2_job_bytes();
+int fft2_group_pairs();
+size_t fft2_group_smem(const shtb_plan* p);
+void fft2_fill_job(const shtb_plan* p, int syn, const void* W, void* grid, int nf, void* host_job);
+int launch_fft2_group(int syn, const void* jobs, const int4* items, int nitems, int grid, size_t smem, int* queue,
+                      cudaStream_t st);
 
 }  // namespace shtb

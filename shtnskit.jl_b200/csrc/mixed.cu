@@ -264,6 +264,10 @@ struct Smem {
   // then the FP32 column scales of the last kScR chunks
   static constexpr int kScOff = (kBar + (kFull + kLd + kRel + kAcc) * 8 + 16 + 15) & ~15;
   static constexpr int kBytes = kScOff + kScR * N * 4;
+  // grouped kernels only: a ring of kQ claimed tile indices with its full/empty barriers
+  static constexpr int kQ = 8;
+  static constexpr int kQOff = (kBytes + 15) & ~15;
+  static constexpr int kBytesQ = kQOff + kQ * (8 + 8 + 4);
   // TMEM: chunk accumulator b at columns [b N, (b + 1) N), b < kAcc
   static constexpr int kTmemNeed = kAcc * N;
   static constexpr int kTmemCols = kTmemNeed <= 32 ? 32 : kTmemNeed <= 64 ? 64 : kTmemNeed <= 128 ? 128
@@ -665,7 +669,31 @@ __device__ __forceinline__ bool promo_tile(const Args& a, const TileCoord& tc, c
   return true;
 }
 
-// Runs the tiles blockIdx.x, blockIdx.x + gridDim.x, ... of src (args(i), coord(i), n).
+// Tile-index ring of the grouped kernels. The loader thread claims tile indices from the
+// launch's device counter (atomicAdd: the list is sorted by decreasing cost, so the CTAs
+// take the longest remaining tile whenever they have room) and publishes each in slot
+// t % kQ of the ring, -1 once the list is exhausted; the other roles read the slots in the
+// same order. full[s]: one arrival (the loader's, after writing the index); empty[s]: one
+// arrival per consumer (each splitter and promotion warp and the MMA thread) after reading.
+struct TileQueue {
+  unsigned long long *full, *empty;
+  volatile int* ids;
+};
+template <int N>
+__device__ __forceinline__ TileQueue tile_queue(unsigned char* sm) {
+  using S = Smem<N>;
+  TileQueue Q;
+  Q.full = reinterpret_cast<unsigned long long*>(sm + S::kQOff);
+  Q.empty = Q.full + S::kQ;
+  Q.ids = reinterpret_cast<volatile int*>(Q.empty + S::kQ);
+  return Q;
+}
+template <int MODE>
+constexpr unsigned kQueueConsumers = (MODE == 1 ? kSW : 0) + 1 + 8;
+
+// Runs the tiles of src (args(i), coord(i), n): i = blockIdx.x, blockIdx.x + gridDim.x, ...
+// for a static source; for a dynamic one (Src::kDynamic, the grouped kernels) the tiles
+// the loader claims from src.queue, in claim order.
 template <int MODE, int N, class Src>
 __device__ __forceinline__ void gemm_tiles(const Src& src, unsigned char* sm, const Bars& B, unsigned tmem) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -677,7 +705,32 @@ __device__ __forceinline__ void gemm_tiles(const Src& src, unsigned char* sm, co
   unsigned issued = 0;   // loader: chunks 0 .. issued-1 had their copies issued (all but a skipped one)
   int committed = -1;    // MMA issuer: last chunk committed
   int skip = -1;
-  for (int i = blockIdx.x; role && i < src.n; i += gridDim.x) {
+  int i = blockIdx.x;
+  for (unsigned t = 0; role; ++t) {
+    if constexpr (Src::kDynamic) {
+      using S = Smem<N>;
+      const TileQueue Q = tile_queue<N>(sm);
+      const unsigned s = t % S::kQ;
+      if (loader) {
+        if (t >= (unsigned)S::kQ &&
+            !mbar_wait(&Q.empty[s], ((t / S::kQ) - 1) & 1, B.abort_flag, src.err(), kWaitNs))
+          break;
+        const int c = atomicAdd(src.queue, 1);
+        i = (c < src.n) ? c : -1;
+        Q.ids[s] = i;
+        mbar_arrive(&Q.full[s]);
+      } else {
+        bool ok = mbar_wait(&Q.full[s], (t / S::kQ) & 1, B.abort_flag, src.err(), kWaitNs);
+        if (!mma) ok = __all_sync(0xffffffffu, ok);   // splitter and promotion warps: warp-uniform
+        if (!ok) break;
+        i = Q.ids[s];
+        if (!mma) __syncwarp();
+        if (mma || lane == 0) mbar_arrive(&Q.empty[s]);
+      }
+      if (i < 0) break;
+    } else {
+      if (i >= src.n) break;
+    }
     const Args& a = src.args(i);
     const TileCoord tc = src.coord(i);
     const TileInfo T = tile_info<MODE>(a, tc);
@@ -694,6 +747,7 @@ __device__ __forceinline__ void gemm_tiles(const Src& src, unsigned char* sm, co
     if (!ok) break;
     if (promo) src.tile_done(i);
     c0 += T.nch;
+    if constexpr (!Src::kDynamic) i += gridDim.x;
   }
   // Every thread of the CTA: after this barrier the abort flag is final.
   __syncthreads();
@@ -949,15 +1003,28 @@ __device__ __forceinline__ void pack_field1(const Args& a, int im, int k) {
   __syncthreads();   // buf and smx are reused by the next call
 }
 
-// Persistent packing for grouped transforms: item = (transform, order), all its fields.
+// Persistent packing for grouped transforms: item = (transform, order), all its fields,
+// claimed in list order from the device counter *queue (zero at launch).
 __global__ void __launch_bounds__(kPack1Threads) mixed_pack_group_kernel(const Args* __restrict__ targs,
-                                                                       const int2* __restrict__ items, int nitems) {
+                                                                       const int2* __restrict__ items, int nitems,
+                                                                       int* __restrict__ queue) {
   __shared__ Args sa;
-  for (int i = blockIdx.x; i < nitems; i += gridDim.x) {
-    const int2 it = items[i];
-    if (threadIdx.x == 0) sa = targs[it.x];
+  __shared__ int s_item, s_order;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const int i = atomicAdd(queue, 1);
+      s_item = i;
+      if (i < nitems) {
+        const int2 it = items[i];
+        s_order = it.y;
+        sa = targs[it.x];
+      }
+    }
     __syncthreads();
-    for (int k = 0; k < sa.nf; ++k) pack_field1(sa, it.y, k);
+    const int item = s_item, order = s_order, nf = sa.nf;
+    __syncthreads();   // everyone holds the item before thread 0 may claim the next one
+    if (item >= nitems) break;
+    for (int k = 0; k < nf; ++k) pack_field1(sa, order, k);   // ends with __syncthreads
   }
 }
 
@@ -966,6 +1033,7 @@ __global__ void __launch_bounds__(kPack1Threads) mixed_pack_group_kernel(const A
 // index * nz + z) * 2 + par over the (im, j0) list. z = block of N/2 fields.
 template <int MODE, int N>
 struct SingleSrc {
+  static constexpr bool kDynamic = false;
   const Args& a;
   int n, nz, ntp;
   __device__ const Args& args(int) const { return a; }
@@ -1005,14 +1073,18 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm<N>) mixed_gemm_kernel(con
 }
 
 // Tiles of many independent transforms: item = (transform, im, p0 or j0, parity), list
-// sorted by decreasing cost. done[t] receives the %globaltimer value at which the last
-// tile of transform t was stored (the maximum over its tiles).
+// sorted by decreasing cost and claimed through the device counter queue (zero at launch).
+// done[t] receives the %globaltimer value at which the last tile of transform t was
+// stored (the maximum over its tiles).
 template <int MODE>
 struct GroupSrc {
+  static constexpr bool kDynamic = true;
   const Args* targs;
   const int4* items;
   int n;
   unsigned long long* done;
+  int* queue;
+  __device__ int* err() const { return targs[0].err; }
   __device__ const Args& args(int i) const { return targs[items[i].x]; }
   __device__ TileCoord coord(int i) const {
     const int4 it = items[i];
@@ -1032,16 +1104,24 @@ struct GroupSrc {
   }
 };
 
-// Persistent GEMM over the tiles of many transforms.
+// Persistent GEMM over the tiles of many transforms, claimed from the counter *queue.
 template <int MODE, int N>
 __global__ void __launch_bounds__(kThreads, kCtasPerSm<N>) mixed_gemm_group_kernel(const Args* __restrict__ targs,
                                                                                    const int4* __restrict__ items,
                                                                                    int nitems,
-                                                                                   unsigned long long* __restrict__ done) {
+                                                                                   unsigned long long* __restrict__ done,
+                                                                                   int* __restrict__ queue) {
   extern __shared__ __align__(1024) unsigned char sm[];
   const Bars B = gemm_bars<N>(sm);
+  if (threadIdx.x == 0) {   // made visible by the fence and barrier of gemm_cta_setup
+    const TileQueue Q = tile_queue<N>(sm);
+    for (int s = 0; s < Smem<N>::kQ; ++s) {
+      mbar_init(&Q.full[s], 1);
+      mbar_init(&Q.empty[s], kQueueConsumers<MODE>);
+    }
+  }
   const unsigned tmem = gemm_cta_setup<N>(B);
-  const GroupSrc<MODE> src{targs, items, nitems, done};
+  const GroupSrc<MODE> src{targs, items, nitems, done, queue};
   gemm_tiles<MODE, N>(src, sm, B, tmem);
   gemm_cta_teardown<N>(tmem);
 }
@@ -1339,26 +1419,26 @@ int mixed_group_ksteps(const shtb_plan* p, int mode, int im, int par) {
 
 int mixed_group_tile_rows() { return kM; }
 
-int launch_pack_group(const void* targs, const int2* items, int nitems, int grid, cudaStream_t st) {
+int launch_pack_group(const void* targs, const int2* items, int nitems, int grid, int* queue, cudaStream_t st) {
   if (nitems <= 0) return SHTB_OK;
-  mixed_pack_group_kernel<<<grid, kPack1Threads, 0, st>>>((const Args*)targs, items, nitems);
+  mixed_pack_group_kernel<<<grid, kPack1Threads, 0, st>>>((const Args*)targs, items, nitems, queue);
   count_launch();
   SHTB_TRY_CUDA(cudaGetLastError(), "group pack launch");
   return SHTB_OK;
 }
 
 int launch_gemm_group(int mode, const void* targs, const int4* items, int nitems, int grid, unsigned long long* done,
-                      cudaStream_t st) {
+                      int* queue, cudaStream_t st) {
   if (nitems <= 0) return SHTB_OK;
-  const int smem = Smem<16>::kBytes;
+  const int smem = Smem<16>::kBytesQ;
   if (mode == 0) {
     auto kern = mixed_gemm_group_kernel<0, 16>;
     SHTB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "group gemm smem attr");
-    kern<<<grid, kThreads, smem, st>>>((const Args*)targs, items, nitems, done);
+    kern<<<grid, kThreads, smem, st>>>((const Args*)targs, items, nitems, done, queue);
   } else {
     auto kern = mixed_gemm_group_kernel<1, 16>;
     SHTB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "group gemm smem attr");
-    kern<<<grid, kThreads, smem, st>>>((const Args*)targs, items, nitems, done);
+    kern<<<grid, kThreads, smem, st>>>((const Args*)targs, items, nitems, done, queue);
   }
   count_launch();
   SHTB_TRY_CUDA(cudaGetLastError(), "group gemm launch");

@@ -1,7 +1,7 @@
 """Uneven batches (``shtb_group_*``): members of different sizes run as persistent grouped
-launches replayed from a CUDA graph must reproduce the per-member mixed-precision
-transforms bit for bit, stay within the mixed-precision tolerance of the FP64 oracle,
-and keep doing so after autotuning changes the launch shape."""
+launches (work claimed from device counters) replayed from a CUDA graph must reproduce the
+per-member mixed-precision transforms bit for bit, stay within the mixed-precision
+tolerance of the FP64 oracle, and keep doing so after autotuning changes the launch shape."""
 import numpy as np
 import pytest
 import torch
@@ -15,6 +15,13 @@ from _util import rand_alm, rel_l2
 
 pytestmark = pytest.mark.gpu
 TOLMX = 1e-6
+
+
+def packed_pair_fft(cfg):
+    """The library's rule for the packed-pair FP32 FFT kernels (power-of-two nlon in
+    64..2048, nlat a multiple of 4); the group runs them in their own persistent kernel."""
+    n = cfg.nlon
+    return 64 <= n <= 2048 and (n & (n - 1)) == 0 and cfg.nlat % 4 == 0
 
 
 def members(lmaxes, nfs):
@@ -56,7 +63,10 @@ def test_group_matches_per_member_bitwise():
     launches0 = _lib.load().shtb_launch_count(0)
     b.roundtrip()
     torch.cuda.synchronize()
-    assert _lib.load().shtb_launch_count(0) - launches0 == 6
+    # start marker, packing, two GEMMs and one FFT kernel per direction and FFT kind
+    kinds = len({packed_pair_fft(c) for c in cfgs})
+    assert kinds == 2
+    assert _lib.load().shtb_launch_count(0) - launches0 == 4 + 2 * kinds
     b.status()
     grids, alms = per_member(b)
     assert_same(b, grids, alms)
