@@ -445,19 +445,23 @@ __device__ __forceinline__ bool loader_tile(const Args& a, const TileCoord& tc, 
   return true;
 }
 
-// Analysis splitters. The FFT writes B as FP32 tile images; image K-steps 2g and 2g + 1
-// of a chunk form f16 K-step g (K = 16), whose hi tile takes the place of FP32 tile 2g and
-// lo tile that of 2g + 1 (the table holds A in that form already). kTpr threads per row:
-// each row of the chunk is scaled by the power of two 2^e that brings its largest
-// magnitude into [2^14, 2^15), split into f16 hi + lo and written in place (the same
-// core-matrix byte order: 16-byte rows of 8 f16 values). The factor 2^-(e + s) that undoes
-// this and the table's scale 2^s goes to the chunk's entry of the scale ring. A missing odd
-// K-step at the end of a tile converts as zeros. The splitter warps form two groups that
-// take the chunks in turn (group gc % 2), so conversions of consecutive chunks overlap. A
-// group reaches chunk gc after its own chunk gc - 2, possibly before the loader has
-// refilled the stage; the copy barriers form a ring of 2 kSt (an even count), so the
-// previous phase of chunk gc's barrier belongs to chunk gc - 2 kSt, the group's own, whose
-// copies it saw land: its wait cannot match an older phase.
+// Analysis splitters. The FFT writes B as FP32 tile images; image K-steps 2g and 2g + 1 of
+// a chunk form f16 K-step g (K = 16), whose hi tile takes the place of FP32 tile 2g and lo
+// tile that of 2g + 1 (the table holds A in that form already). kTpr threads per row, each
+// owning whole FP32 K-steps st = v, v + kTpr, ...: each row of the chunk is scaled by the
+// power of two 2^e that brings its largest magnitude into [2^14, 2^15), split into f16 hi +
+// lo and written in place (the same core-matrix byte order: 16-byte rows of 8 f16 values),
+// one 16-byte store per K-step for hi and one for lo. Lane layout: the 8 lanes of a quarter
+// warp take 8 consecutive rows of one core-matrix group (so every 16-byte access of a
+// quarter warp covers one 128-byte run), and a row's kTpr threads sit 8 lanes apart
+// (partners by xor 8, 16). The factor 2^-(e + s) that undoes this and the table's scale 2^s
+// goes to the chunk's entry of the scale ring. A missing odd K-step at the end of a tile
+// converts as zeros. The splitter warps form two groups that take the chunks in turn (group
+// gc % 2), so conversions of consecutive chunks overlap. A group reaches chunk gc after its
+// own chunk gc - 2, possibly before the loader has refilled the stage; the copy barriers
+// form a ring of 2 kSt (an even count), so the previous phase of chunk gc's barrier belongs
+// to chunk gc - 2 kSt, the group's own, whose copies it saw land: its wait cannot match an
+// older phase.
 template <int MODE, int N>
 __device__ __forceinline__ bool splitter_tile(const Args& a, const TileInfo& T, unsigned char* sm, const Bars& B,
                                                   unsigned c0) {
@@ -465,13 +469,15 @@ __device__ __forceinline__ bool splitter_tile(const Args& a, const TileInfo& T, 
   constexpr int kSG = 2;                                                 // splitter groups
   static_assert(S::kLd % kSG == 0, "copy-barrier ring a multiple of the groups");
   constexpr int kGT = 32 * kSW / kSG;                                    // threads per group
-  constexpr int kTpr = (kGT >= 8 * N) ? 8 : (kGT >= N) ? kGT / N : 1;     // threads per B row
+  constexpr int kTpr = (kGT >= 4 * N) ? 4 : (kGT >= N) ? kGT / N : 1;     // threads per B row (1, 2 or 4)
   constexpr int kRpt = (kGT >= N) ? 1 : N / kGT;                         // B rows per thread
-  constexpr int kPieces = 2 * kChunk;                 // 16-byte pieces of a B row per chunk
-  constexpr int kPt = (kPieces + kTpr - 1) / kTpr;    // pieces per thread
+  constexpr int kSpt = kChunk / kTpr;                                    // FP32 K-steps per thread
+  constexpr int kRpw = 8 * (4 / kTpr);                                   // rows per warp
+  static_assert(kChunk % kTpr == 0 && (kTpr == 1 || kTpr == 2 || kTpr == 4), "splitter layout");
   const int tid = threadIdx.x % kGT, grp = threadIdx.x / kGT, lane = tid & 31;
+  const int slot = lane >> 3, v = slot % kTpr;
+  const int row_w = (tid >> 5) * kRpw + 8 * (slot / kTpr) + (lane & 7);   // this thread's row (first pass)
   const int nrows = min((int)(T.bbytes >> 5), N);     // B rows loaded (2 per field)
-  const int v = tid % kTpr;
   const int sa = f16_table_exp(a.P.lmax);
   for (int c = 0; c < T.nch; ++c) {
     const unsigned gc = c0 + c;
@@ -480,42 +486,48 @@ __device__ __forceinline__ bool splitter_tile(const Args& a, const TileInfo& T, 
     const bool ok = mbar_wait(&B.ldfull[gc % S::kLd], (gc / S::kLd) & 1, B.abort_flag, a.err, a.wait_ns);
     if (!__all_sync(0xffffffffu, ok)) return false;
     unsigned char* Bs = sm + (size_t)(gc % S::kSt) * S::kStage + S::kStageA;
+#pragma unroll
     for (int ri = 0; ri < kRpt; ++ri) {
-      const int r = tid / kTpr + ri * (kGT / kTpr);
+      const int r = row_w + ri * (kGT / kTpr);
       const bool rowok = r < nrows;
-      // B row r: piece u = 2 st + khalf of FP32 tile st holds k = 4 u .. 4 u + 3 of the chunk.
-      // The thread's pieces u = v, v + kTpr, ... go to registers, with the row's largest
-      // magnitude; all of the row's pieces are read before any is overwritten (a row's
-      // threads share a warp), then converted from the registers.
-      float4 xb[kPt];
+      // the thread's K-steps (both 16-byte halves) go to registers with the row's largest
+      // magnitude; all of the row's values are read before any is overwritten (a row's
+      // threads share a warp), then converted from the registers
+      float4 xa[kSpt], xb[kSpt];
       unsigned mx = 0;
 #pragma unroll
-      for (int j = 0; j < kPt; ++j) {
-        const int u = v + j * kTpr;
-        xb[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (rowok && u < kPieces && (u >> 1) < nk) {
-          xb[j] = *reinterpret_cast<const float4*>(Bs + (u >> 1) * T.bstr + tile_off(r, u & 1));
+      for (int j = 0; j < kSpt; ++j) {
+        const int st = v + j * kTpr;
+        xa[j] = xb[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (rowok && st < nk) {
+          const unsigned char* src = Bs + st * T.bstr + tile_off(r, 0);
+          xa[j] = *reinterpret_cast<const float4*>(src);
+          xb[j] = *reinterpret_cast<const float4*>(src + 128);
+          mx = max(mx, max(max(__float_as_uint(xa[j].x) & 0x7fffffffu, __float_as_uint(xa[j].y) & 0x7fffffffu),
+                           max(__float_as_uint(xa[j].z) & 0x7fffffffu, __float_as_uint(xa[j].w) & 0x7fffffffu)));
           mx = max(mx, max(max(__float_as_uint(xb[j].x) & 0x7fffffffu, __float_as_uint(xb[j].y) & 0x7fffffffu),
                            max(__float_as_uint(xb[j].z) & 0x7fffffffu, __float_as_uint(xb[j].w) & 0x7fffffffu)));
         }
       }
 #pragma unroll
-      for (int o = 1; o < kTpr; o <<= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      for (int o = 8; o < 8 * kTpr; o <<= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
       // max * 2^e in [2^14, 2^15) (e at most 100: rows below 2^-86 keep the f16 subnormal steps)
       const int e = min(141 - (int)(mx >> 23), 100);
       const float su = __int_as_float((e + 127) << 23);
       __syncwarp();
       if (rowok) {
 #pragma unroll
-        for (int j = 0; j < kPt; ++j) {
-          const int u = v + j * kTpr, st = u >> 1;
-          if (u < kPieces && st < 2 * nk2) {   // a missing odd K-step is written as zeros
-            unsigned h0, l0, h1, l1;
-            split_h2(xb[j].x * su, xb[j].y * su, h0, l0);
-            split_h2(xb[j].z * su, xb[j].w * su, h1, l1);
-            unsigned char* d = Bs + (st & ~1) * T.bstr + tile_off(r, st & 1) + (u & 1) * 8;
-            *reinterpret_cast<uint2*>(d) = make_uint2(h0, h1);
-            *reinterpret_cast<uint2*>(d + T.bstr) = make_uint2(l0, l1);
+        for (int j = 0; j < kSpt; ++j) {
+          const int st = v + j * kTpr;
+          if (st < 2 * nk2) {   // a missing odd K-step is written as zeros
+            uint4 hi, lo;
+            split_h2(xa[j].x * su, xa[j].y * su, hi.x, lo.x);
+            split_h2(xa[j].z * su, xa[j].w * su, hi.y, lo.y);
+            split_h2(xb[j].x * su, xb[j].y * su, hi.z, lo.z);
+            split_h2(xb[j].z * su, xb[j].w * su, hi.w, lo.w);
+            unsigned char* d = Bs + (st & ~1) * T.bstr + tile_off(r, st & 1);
+            *reinterpret_cast<uint4*>(d) = hi;
+            *reinterpret_cast<uint4*>(d + T.bstr) = lo;
           }
         }
       }
