@@ -448,10 +448,11 @@ __device__ __forceinline__ bool loader_tile(const Args& a, const TileCoord& tc, 
 // Analysis splitters. The FFT writes B as FP32 tile images; image K-steps 2g and 2g + 1 of
 // a chunk form f16 K-step g (K = 16), whose hi tile takes the place of FP32 tile 2g and lo
 // tile that of 2g + 1 (the table holds A in that form already). kTpr threads per row, each
-// owning whole FP32 K-steps st = v, v + kTpr, ...: each row of the chunk is scaled by the
-// power of two 2^e that brings its largest magnitude into [2^14, 2^15), split into f16 hi +
-// lo and written in place (the same core-matrix byte order: 16-byte rows of 8 f16 values),
-// one 16-byte store per K-step for hi and one for lo. Lane layout: the 8 lanes of a quarter
+// owning whole f16 K-steps g = v, v + kTpr, ...: each row of the chunk is scaled by the power
+// of two 2^e that brings its largest magnitude into [2^14, 2^15) (a first pass over the
+// thread's values finds the row maximum), split into f16 hi + lo and written in place (the
+// same core-matrix byte order: 16-byte rows of 8 f16 values), one 16-byte store per FP32
+// K-step half for hi and one for lo; a thread's writes land only in its own two FP32 tiles. Lane layout: the 8 lanes of a quarter
 // warp take 8 consecutive rows of one core-matrix group (so every 16-byte access of a
 // quarter warp covers one 128-byte run), and a row's kTpr threads sit 8 lanes apart
 // (partners by xor 8, 16). The factor 2^-(e + s) that undoes this and the table's scale 2^s
@@ -471,9 +472,9 @@ __device__ __forceinline__ bool splitter_tile(const Args& a, const TileInfo& T, 
   constexpr int kGT = 32 * kSW / kSG;                                    // threads per group
   constexpr int kTpr = (kGT >= 4 * N) ? 4 : (kGT >= N) ? kGT / N : 1;     // threads per B row (1, 2 or 4)
   constexpr int kRpt = (kGT >= N) ? 1 : N / kGT;                         // B rows per thread
-  constexpr int kSpt = kChunk / kTpr;                                    // FP32 K-steps per thread
+  constexpr int kGpt = kChunk / 2 / kTpr;                                // f16 K-steps per thread
   constexpr int kRpw = 8 * (4 / kTpr);                                   // rows per warp
-  static_assert(kChunk % kTpr == 0 && (kTpr == 1 || kTpr == 2 || kTpr == 4), "splitter layout");
+  static_assert((kChunk / 2) % kTpr == 0 && (kTpr == 1 || kTpr == 2 || kTpr == 4), "splitter layout");
   const int tid = threadIdx.x % kGT, grp = threadIdx.x / kGT, lane = tid & 31;
   const int slot = lane >> 3, v = slot % kTpr;
   const int row_w = (tid >> 5) * kRpw + 8 * (slot / kTpr) + (lane & 7);   // this thread's row (first pass)
@@ -493,20 +494,24 @@ __device__ __forceinline__ bool splitter_tile(const Args& a, const TileInfo& T, 
       // the thread's K-steps (both 16-byte halves) go to registers with the row's largest
       // magnitude; all of the row's values are read before any is overwritten (a row's
       // threads share a warp), then converted from the registers
-      float4 xa[kSpt], xb[kSpt];
+      // pass 1: the row's largest magnitude over the thread's f16 K-steps (FP32 K-steps 2g,
+      // 2g + 1 for g = v, v + kTpr, ...), reduced over the row's threads
       unsigned mx = 0;
 #pragma unroll
-      for (int j = 0; j < kSpt; ++j) {
-        const int st = v + j * kTpr;
-        xa[j] = xb[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (rowok && st < nk) {
-          const unsigned char* src = Bs + st * T.bstr + tile_off(r, 0);
-          xa[j] = *reinterpret_cast<const float4*>(src);
-          xb[j] = *reinterpret_cast<const float4*>(src + 128);
-          mx = max(mx, max(max(__float_as_uint(xa[j].x) & 0x7fffffffu, __float_as_uint(xa[j].y) & 0x7fffffffu),
-                           max(__float_as_uint(xa[j].z) & 0x7fffffffu, __float_as_uint(xa[j].w) & 0x7fffffffu)));
-          mx = max(mx, max(max(__float_as_uint(xb[j].x) & 0x7fffffffu, __float_as_uint(xb[j].y) & 0x7fffffffu),
-                           max(__float_as_uint(xb[j].z) & 0x7fffffffu, __float_as_uint(xb[j].w) & 0x7fffffffu)));
+      for (int j = 0; j < kGpt; ++j) {
+        const int g = v + j * kTpr;
+#pragma unroll
+        for (int w = 0; w < 2; ++w) {
+          const int st = 2 * g + w;
+          if (rowok && st < nk) {
+            const unsigned char* src = Bs + st * T.bstr + tile_off(r, 0);
+            const float4 x0 = *reinterpret_cast<const float4*>(src);
+            const float4 x1 = *reinterpret_cast<const float4*>(src + 128);
+            mx = max(mx, max(max(__float_as_uint(x0.x) & 0x7fffffffu, __float_as_uint(x0.y) & 0x7fffffffu),
+                             max(__float_as_uint(x0.z) & 0x7fffffffu, __float_as_uint(x0.w) & 0x7fffffffu)));
+            mx = max(mx, max(max(__float_as_uint(x1.x) & 0x7fffffffu, __float_as_uint(x1.y) & 0x7fffffffu),
+                             max(__float_as_uint(x1.z) & 0x7fffffffu, __float_as_uint(x1.w) & 0x7fffffffu)));
+          }
         }
       }
 #pragma unroll
@@ -514,20 +519,34 @@ __device__ __forceinline__ bool splitter_tile(const Args& a, const TileInfo& T, 
       // max * 2^e in [2^14, 2^15) (e at most 100: rows below 2^-86 keep the f16 subnormal steps)
       const int e = min(141 - (int)(mx >> 23), 100);
       const float su = __int_as_float((e + 127) << 23);
-      __syncwarp();
+      // pass 2: each f16 K-step g reads and writes only its own two FP32 tiles 2g, 2g + 1
+      // (hi of both into 2g, lo of both into 2g + 1), so it converts in place right after
+      // reading them
       if (rowok) {
 #pragma unroll
-        for (int j = 0; j < kSpt; ++j) {
-          const int st = v + j * kTpr;
-          if (st < 2 * nk2) {   // a missing odd K-step is written as zeros
-            uint4 hi, lo;
-            split_h2(xa[j].x * su, xa[j].y * su, hi.x, lo.x);
-            split_h2(xa[j].z * su, xa[j].w * su, hi.y, lo.y);
-            split_h2(xb[j].x * su, xb[j].y * su, hi.z, lo.z);
-            split_h2(xb[j].z * su, xb[j].w * su, hi.w, lo.w);
-            unsigned char* d = Bs + (st & ~1) * T.bstr + tile_off(r, st & 1);
-            *reinterpret_cast<uint4*>(d) = hi;
-            *reinterpret_cast<uint4*>(d + T.bstr) = lo;
+        for (int j = 0; j < kGpt; ++j) {
+          const int g = v + j * kTpr;
+          if (g < nk2) {
+            unsigned char* b0 = Bs + 2 * g * T.bstr + tile_off(r, 0);
+            float4 x[4];
+#pragma unroll
+            for (int w = 0; w < 2; ++w) {
+              const bool have = 2 * g + w < nk;   // a missing odd K-step converts as zeros
+              const unsigned char* src = b0 + w * T.bstr;
+              x[2 * w] = have ? *reinterpret_cast<const float4*>(src) : make_float4(0.f, 0.f, 0.f, 0.f);
+              x[2 * w + 1] = have ? *reinterpret_cast<const float4*>(src + 128) : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+#pragma unroll
+            for (int w = 0; w < 2; ++w) {
+              uint4 hi, lo;
+              split_h2(x[2 * w].x * su, x[2 * w].y * su, hi.x, lo.x);
+              split_h2(x[2 * w].z * su, x[2 * w].w * su, hi.y, lo.y);
+              split_h2(x[2 * w + 1].x * su, x[2 * w + 1].y * su, hi.z, lo.z);
+              split_h2(x[2 * w + 1].z * su, x[2 * w + 1].w * su, hi.w, lo.w);
+              // FP32 K-step 2g + w -> khalf w of the hi tile (2g) and of the lo tile (2g + 1)
+              *reinterpret_cast<uint4*>(b0 + w * 128) = hi;
+              *reinterpret_cast<uint4*>(b0 + T.bstr + w * 128) = lo;
+            }
           }
         }
       }
