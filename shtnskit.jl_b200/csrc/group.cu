@@ -43,7 +43,8 @@ __global__ void group_start_kernel(unsigned long long* done, int n, unsigned lon
 
 static size_t align256(size_t v) { return (v + 255) / 256 * 256; }
 
-constexpr int kGroupQueues = 7;   // pack, GEMM syn, FFT syn, FFT ana, GEMM ana, fft2 syn, fft2 ana
+// work counters: pack, GEMM syn, FFT syn, FFT ana, GEMM ana, fft2 syn, fft2 ana, FP64-pipe syn
+constexpr int kGroupQueues = 8;
 
 }  // namespace shtb
 
@@ -55,6 +56,12 @@ struct shtb_group {
   std::vector<int> nf;
   std::vector<size_t> woff;             // byte offset of member t's Fourier buffer
   std::vector<char> f2;                 // member runs the packed-pair FFTs (fft2_applicable)
+  std::vector<char> simt;               // member's Legendre synthesis runs on the FP64 pipes (simt_applicable)
+  size_t sargsz = 0;
+  unsigned char* d_sargs = nullptr;
+  int4* d_items_ssyn = nullptr;
+  int n_ssyn = 0, ssyn_ctas = 148;
+  size_t ssyn_smem = 0;
   size_t argsz = 0, jobsz = 0, job2sz = 0;
   // device memory: [args syn | args ana | jobs syn | jobs ana | done | t0 | gemm items | W]
   unsigned char* dmem = nullptr;
@@ -168,6 +175,30 @@ static int group_fft_stage(shtb_group* g, int syn, int* q_gen, int* q_f2, cudaSt
   return SHTB_OK;
 }
 
+// The Legendre synthesis stage: the FP64-pipe kernel of the one- and two-field members on the
+// aux stream, forked from and joined back into st, beside the packing and tensor-core GEMM of
+// the others on st.
+static int group_synthesis_stage(shtb_group* g, int* q, cudaStream_t st) {
+  int rc;
+  const bool fork = g->n_ssyn > 0 && g->n_syn > 0;
+  if (fork) {
+    SHTB_TRY_CUDA(cudaEventRecord(g->ev_fork, st), "group fork");
+    SHTB_TRY_CUDA(cudaStreamWaitEvent(g->aux, g->ev_fork, 0), "group fork");
+  }
+  if ((rc = launch_simt_group(g->d_sargs, g->d_items_ssyn, g->n_ssyn, g->ssyn_ctas, g->ssyn_smem, q + 7,
+                              fork ? g->aux : st)))
+    return rc;
+  if ((rc = launch_pack_group(g->d_args_syn, g->d_items_pack, g->n_pack, std::min(g->n_pack, 24 * g->nsm), q, st)))
+    return rc;
+  if ((rc = launch_gemm_group(0, g->d_args_syn, g->d_items_syn, g->n_syn, g->gemm_ctas_syn, nullptr, q + 1, st)))
+    return rc;
+  if (fork) {
+    SHTB_TRY_CUDA(cudaEventRecord(g->ev_join, g->aux), "group join");
+    SHTB_TRY_CUDA(cudaStreamWaitEvent(st, g->ev_join, 0), "group join");
+  }
+  return SHTB_OK;
+}
+
 static int group_launch_stages(shtb_group* g, int op, cudaStream_t st) {
   int rc;
   int* q = g->d_queue;
@@ -176,10 +207,7 @@ static int group_launch_stages(shtb_group* g, int op, cudaStream_t st) {
     group_start_kernel<<<1, 256, 0, st>>>(g->d_done, g->n, g->d_t0);
     count_launch();
     SHTB_TRY_CUDA(cudaGetLastError(), "group start marker");
-    if ((rc = launch_pack_group(g->d_args_syn, g->d_items_pack, g->n_pack, std::min(g->n_pack, 24 * g->nsm), q, st)))
-      return rc;
-    if ((rc = launch_gemm_group(0, g->d_args_syn, g->d_items_syn, g->n_syn, g->gemm_ctas_syn, nullptr, q + 1, st)))
-      return rc;
+    if ((rc = group_synthesis_stage(g, q, st))) return rc;
     if ((rc = group_fft_stage(g, 1, q + 2, q + 5, st))) return rc;
   }
   if (op != SHTB_OP_SYNTHESIS) {
@@ -223,8 +251,10 @@ extern "C" int shtb_group_create(shtb_group** out, const shtb_plan* const* plans
     return rc;
   };
   g->f2.resize(n);
+  g->simt.resize(n);
   for (int t = 0; t < n; ++t) {
-    int rc = mixed_prepare(plans[t], 0);
+    g->simt[t] = simt_applicable(plans[t], nfields[t]) ? 1 : 0;
+    int rc = mixed_prepare(plans[t], 0);   // the analysis GEMM reads the plan's P table
     if (rc) return fail(rc);
     g->f2[t] = fft2_applicable(plans[t]) ? 1 : 0;
     if (!g->f2[t]) g->generic = g->generic || fft_plan_generic(plans[t]);
@@ -256,12 +286,26 @@ extern "C" int shtb_group_create(shtb_group** out, const shtb_plan* const* plans
   const int TM = mixed_group_tile_rows();
   std::vector<int4> syn, ana;
   std::vector<int> csyn, cana;
+  // FP64-pipe synthesis items of the one- and two-field members, most work first
+  std::vector<int4> ssyn;
+  std::vector<int> cssyn;
+  for (int t = 0; t < n; ++t) {
+    if (!g->simt[t]) continue;
+    const shtb_plan* p = plans[t];
+    const int mlim = std::min(p->mmax, p->lmax);
+    g->ssyn_smem = std::max(g->ssyn_smem, simt_group_syn_smem(p));
+    for (int im = 0; im <= mlim; ++im)
+      for (int pb = 0; pb < simt_syn_pair_blocks(p); ++pb) {
+        ssyn.push_back(make_int4(t, im, pb, 0));
+        cssyn.push_back(p->lmax - im + 1);
+      }
+  }
   for (int t = 0; t < n; ++t) {
     const shtb_plan* p = plans[t];
     const int mlim = std::min(p->mmax, p->lmax);
     for (int im = 0; im <= mlim; ++im) {
       for (int par = 0; par < 2; ++par) {
-        for (int p0 = 0; p0 < p->npair; p0 += TM) {
+        for (int p0 = 0; !g->simt[t] && p0 < p->npair; p0 += TM) {
           syn.push_back(make_int4(t, im, p0, par));
           csyn.push_back(mixed_group_ksteps(p, 0, im, par));
         }
@@ -283,12 +327,13 @@ extern "C" int shtb_group_create(shtb_group** out, const shtb_plan* const* plans
   };
   sort_items(syn, csyn);
   sort_items(ana, cana);
+  sort_items(ssyn, cssyn);
   std::vector<int2> pack;   // (member, order) for the synthesis B packing, most degrees first
   {
     std::vector<int4> tmp;
     std::vector<int> cost;
     for (int t = 0; t < n; ++t)
-      for (int im = 0; im <= std::min(plans[t]->mmax, plans[t]->lmax); ++im) {
+      for (int im = 0; !g->simt[t] && im <= std::min(plans[t]->mmax, plans[t]->lmax); ++im) {
         tmp.push_back(make_int4(t, im, 0, 0));
         cost.push_back(plans[t]->lmax - im);
       }
@@ -301,6 +346,9 @@ extern "C" int shtb_group_create(shtb_group** out, const shtb_plan* const* plans
   // two GEMM CTAs of 16 columns fit on an SM
   g->gemm_ctas_syn = std::max(1, std::min(2 * g->nsm, g->n_syn));
   g->gemm_ctas_ana = std::max(1, std::min(2 * g->nsm, g->n_ana));
+  g->n_ssyn = (int)ssyn.size();
+  g->ssyn_ctas = std::max(1, std::min(8 * g->nsm, g->n_ssyn));   // 128-thread CTAs, several per SM
+  g->sargsz = simt_args_bytes();
   // one device allocation
   g->argsz = mixed_args_bytes();
   g->jobsz = fft_job_bytes_f32();
@@ -313,6 +361,7 @@ extern "C" int shtb_group_create(shtb_group** out, const shtb_plan* const* plans
   const size_t o_done = take(n * 8), o_t0 = take(8), o_q = take(kGroupQueues * sizeof(int)),
                o_is = take(syn.size() * sizeof(int4)),
                o_ia = take(ana.size() * sizeof(int4)), o_ip = take(pack.size() * sizeof(int2));
+  const size_t o_sas = take(n * g->sargsz), o_iss = take(ssyn.size() * sizeof(int4));
   g->woff.resize(n);
   size_t wbytes = 0;
   for (int t = 0; t < n; ++t) {
@@ -336,10 +385,13 @@ extern "C" int shtb_group_create(shtb_group** out, const shtb_plan* const* plans
   g->d_items_syn = (int4*)(g->dmem + o_is);
   g->d_items_ana = (int4*)(g->dmem + o_ia);
   g->d_items_pack = (int2*)(g->dmem + o_ip);
+  g->d_sargs = g->dmem + o_sas;
+  g->d_items_ssyn = (int4*)(g->dmem + o_iss);
   g->d_w = g->dmem + o_w;
   e = cudaMemcpy(g->d_items_syn, syn.data(), syn.size() * sizeof(int4), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(g->d_items_ana, ana.data(), ana.size() * sizeof(int4), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(g->d_items_pack, pack.data(), pack.size() * sizeof(int2), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(g->d_items_ssyn, ssyn.data(), ssyn.size() * sizeof(int4), cudaMemcpyHostToDevice);
   if (e == cudaSuccess && !f2items.empty())
     e = cudaMemcpy(g->d_items_fft2, f2items.data(), f2items.size() * sizeof(int4), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemset(g->d_done, 0, n * 8);
@@ -371,7 +423,7 @@ extern "C" int shtb_group_bind(shtb_group* g, void* const* alm_in, void* const* 
   int rc = check_device(g);
   if (rc) return rc;
   std::vector<unsigned char> as(g->n * g->argsz), aa(g->n * g->argsz), js(g->n * g->jobsz), ja(g->n * g->jobsz),
-      j2s(g->n * g->job2sz), j2a(g->n * g->job2sz);
+      j2s(g->n * g->job2sz), j2a(g->n * g->job2sz), sas(g->n * g->sargsz);
   for (int t = 0; t < g->n; ++t) {
     if (!alm_in[t] || !grid[t] || !alm_out[t])
       return set_error(SHTB_ERR_BAD_ARG, "NULL buffer for member " + std::to_string(t));
@@ -387,6 +439,7 @@ extern "C" int shtb_group_bind(shtb_group* g, void* const* alm_in, void* const* 
       fft2_fill_job(p, 1, W, grid[t], g->nf[t], j2s.data() + t * g->job2sz);
       fft2_fill_job(p, 0, W, grid[t], g->nf[t], j2a.data() + t * g->job2sz);
     }
+    if (g->simt[t]) simt_fill_args(p, alm_in[t], W, g->nf[t], sas.data() + t * g->sargsz);
   }
   SHTB_TRY_CUDA(cudaMemcpy(g->d_args_syn, as.data(), as.size(), cudaMemcpyHostToDevice), "group bind");
   SHTB_TRY_CUDA(cudaMemcpy(g->d_args_ana, aa.data(), aa.size(), cudaMemcpyHostToDevice), "group bind");
@@ -394,6 +447,7 @@ extern "C" int shtb_group_bind(shtb_group* g, void* const* alm_in, void* const* 
   SHTB_TRY_CUDA(cudaMemcpy(g->d_jobs_ana, ja.data(), ja.size(), cudaMemcpyHostToDevice), "group bind");
   SHTB_TRY_CUDA(cudaMemcpy(g->d_jobs2_syn, j2s.data(), j2s.size(), cudaMemcpyHostToDevice), "group bind");
   SHTB_TRY_CUDA(cudaMemcpy(g->d_jobs2_ana, j2a.data(), j2a.size(), cudaMemcpyHostToDevice), "group bind");
+  SHTB_TRY_CUDA(cudaMemcpy(g->d_sargs, sas.data(), sas.size(), cudaMemcpyHostToDevice), "group bind");
   g->bound = true;
   drop_graph(g);
   return SHTB_OK;
@@ -493,6 +547,7 @@ extern "C" int shtb_group_autotune(shtb_group* g, void* stream) {
   for (int which = 0; which < 2 && !rc; ++which) {
     int& ctas = which == 0 ? g->gemm_ctas_syn : g->gemm_ctas_ana;
     const int nitems = which == 0 ? g->n_syn : g->n_ana;
+    if (nitems == 0) continue;
     int keep = ctas;
     for (int mult : {1, 2}) {
       const int c = std::max(1, std::min(mult * g->nsm, nitems));

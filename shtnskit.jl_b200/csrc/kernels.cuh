@@ -84,6 +84,17 @@ size_t fft_group_smem_f32(const shtb_plan* p, int h);
 bool fft_plan_generic(const shtb_plan* p);
 int launch_fft_group_f32(int syn, int h, bool generic, const void* jobs, const int4* items, int nitems, int grid,
                          size_t smem, int* queue, cudaStream_t st);
+// Mixed-precision Legendre synthesis on the FP64 pipes for one or two fields (simt.cu):
+// coefficients (dense or packed LM) -> Fourier buffer.
+bool simt_applicable(const shtb_plan* p, int nf);
+int launch_simt_syn(const shtb_plan* p, const void* alm, void* W, int nf, int ltr, int mlim, int packed,
+                    cudaStream_t st);
+size_t simt_args_bytes();
+void simt_fill_args(const shtb_plan* p, const void* alm, void* W, int nf, void* host_args);
+int simt_syn_pair_blocks(const shtb_plan* p);
+size_t simt_group_syn_smem(const shtb_plan* p);
+int launch_simt_group(const void* targs, const int4* items, int nitems, int grid, size_t smem, int* queue,
+                      cudaStream_t st);
 // the packed-pair FP32 FFTs of fft2_applicable members (2 HP latitude pairs per item)
 size_t fft2_job_bytes();
 int fft2_group_pairs();

@@ -1333,9 +1333,13 @@ static Args base_args(const shtb_plan* p) {
 
 int mixed_synthesis(const shtb_plan* p, const void* alm, void* f, int nf, int ltr, void* work, cudaStream_t st,
                     int packed) {
-  int rc = ensure_table(p, st);
-  if (rc) return rc;
   const int mlim = std::min(p->mmax, ltr);
+  int rc;
+  if (simt_applicable(p, nf)) {   // one or two fields: recurrence on the FP64 pipes, no table
+    if ((rc = launch_simt_syn(p, alm, work, nf, ltr, mlim, packed, st))) return rc;
+    return launch_fft_syn<float, float>(p, work, (float*)f, nullptr, 1, nf, mlim, p->phi_inv_scale / p->nlon, 0, 0, st);
+  }
+  if ((rc = ensure_table(p, st))) return rc;
   Args a = base_args(p);
   a.cin = (const float2*)alm;
   if (packed) {
@@ -1364,9 +1368,9 @@ size_t mixed_workspace_bytes(const shtb_plan* p, int op, int nf) {
 
 int mixed_analysis(const shtb_plan* p, const void* f, void* alm, int nf, int ltr, void* work, cudaStream_t st,
                    int packed) {
-  int rc = ensure_table(p, st);
-  if (rc) return rc;
   const int mlim = std::min(p->mmax, ltr);
+  int rc;
+  if ((rc = ensure_table(p, st))) return rc;
   const long long nlm = lm_count(p->lmax, p->mmax, p->mres);
   if (packed && ltr < p->lmax)   // degrees above ltr are no tile's output
     SHTB_TRY_CUDA(cudaMemsetAsync(alm, 0, (size_t)nlm * nf * sizeof(float2), st), "packed output clear");

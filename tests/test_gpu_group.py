@@ -24,6 +24,12 @@ def packed_pair_fft(cfg):
     return 64 <= n <= 2048 and (n & (n - 1)) == 0 and cfg.nlat % 4 == 0
 
 
+def fp64_pipe_synthesis(nf):
+    """The library's rule for the FP64-pipe Legendre synthesis of the mixed path (one or two
+    fields); other members run the packing and the tensor-core synthesis GEMM."""
+    return nf <= 2
+
+
 def members(lmaxes, nfs):
     cfgs = [sht.create_gauss_config(l, l + 1, nlon=smooth_nlon(l)) for l in lmaxes]
     return cfgs, list(nfs)
@@ -63,10 +69,12 @@ def test_group_matches_per_member_bitwise():
     launches0 = _lib.load().shtb_launch_count(0)
     b.roundtrip()
     torch.cuda.synchronize()
-    # start marker, packing, two GEMMs and one FFT kernel per direction and FFT kind
+    # start marker; FP64-pipe synthesis (one- and two-field members); packing and synthesis
+    # GEMM (the others); one FFT kernel per direction and FFT kind; analysis GEMM (all)
     kinds = len({packed_pair_fft(c) for c in cfgs})
-    assert kinds == 2
-    assert _lib.load().shtb_launch_count(0) - launches0 == 4 + 2 * kinds
+    synth = {fp64_pipe_synthesis(k) for k in nfs}
+    assert kinds == 2 and synth == {True, False}
+    assert _lib.load().shtb_launch_count(0) - launches0 == 1 + 1 + 2 + 2 * kinds + 1
     b.status()
     grids, alms = per_member(b)
     assert_same(b, grids, alms)
