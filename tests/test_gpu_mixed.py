@@ -1,4 +1,5 @@
-"""GPU parity of the mixed-precision (tensor-core fp16x3) path.
+"""GPU parity of the mixed-precision path (tensor-core fp16x3 GEMMs; one- and two-field
+syntheses on the FP64 pipes).
 
 Inputs are rounded to FP32 (the path's I/O type); the FP64 oracle runs on the same
 rounded inputs. Bar: relative L2 <= 1e-6 against the FP64 result.
@@ -32,7 +33,7 @@ def host(t):
 
 
 @pytest.mark.parametrize("case", CASES, ids=lambda c: "-".join(f"{k}{v}" for k, v in c.items()))
-@pytest.mark.parametrize("nf", [1, 9, 20, 64])
+@pytest.mark.parametrize("nf", [1, 2, 9, 20, 64])
 def test_mixed_vs_fp64_oracle(case, nf):
     c = dict(case)
     lmax, nlat = c.pop("lmax"), c.pop("nlat")
@@ -51,18 +52,29 @@ def test_mixed_vs_fp64_oracle(case, nf):
     cfg.plan(0).status()
 
 
-def test_mixed_lcap():
+@pytest.mark.parametrize("nf", [1, 3])
+def test_mixed_lcap(nf):
     cfg = sht.create_gauss_config(40, 42, nlon=81)
     ocfg = so.create_gauss_config(40, 42, nlon=81)
-    a = rand_alm(40, 40, 3, seed=5).astype(np.complex64).astype(np.complex128)
+    a = rand_alm(40, 40, nf, seed=5).astype(np.complex64).astype(np.complex128)
     for ltr in (3, 17, 40):
         f = host(sht.synthesis_batch(cfg, a.astype(np.complex64), lcap=ltr, precision="mixed"))
-        ref = np.stack([so.synthesis(ocfg, a[:, :, k], ltr=ltr) for k in range(3)], axis=2)
+        ref = np.stack([so.synthesis(ocfg, a[:, :, k], ltr=ltr) for k in range(nf)], axis=2)
         assert rel_l2(f, ref) <= TOLMX
-        g = np.random.default_rng(6).standard_normal((42, 81, 3)).astype(np.float32)
+        g = np.random.default_rng(6).standard_normal((42, 81, nf)).astype(np.float32)
         b = host(sht.analysis_batch(cfg, g, lcap=ltr, precision="mixed"))
-        bref = np.stack([so.analysis(ocfg, g[:, :, k].astype(np.float64), ltr=ltr) for k in range(3)], axis=2)
+        bref = np.stack([so.analysis(ocfg, g[:, :, k].astype(np.float64), ltr=ltr) for k in range(nf)], axis=2)
         assert rel_l2(b, bref) <= TOLMX
+
+
+def test_mixed_one_field_high_degree():
+    """One field at lmax 511 (FP64-pipe synthesis from the extended-range start records at
+    high orders) against the oracle."""
+    cfg = sht.create_gauss_config(511, 512, nlon=1024)
+    ocfg = so.create_gauss_config(511, 512, nlon=1024)
+    a = rand_alm(511, 511, seed=13).astype(np.complex64).astype(np.complex128)
+    f = host(sht.synthesis(cfg, a.astype(np.complex64), precision="mixed"))
+    assert rel_l2(f, so.synthesis(ocfg, a)) <= TOLMX
 
 
 def test_mixed_config3_size():
