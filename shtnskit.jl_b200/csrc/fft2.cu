@@ -274,26 +274,37 @@ __device__ __forceinline__ void ana_body(const Job& J, int k, int p0, float4* X,
   }
   // epilogue: E = w (X_N + X_S), O = w (X_N - X_S) with X_N = (Z_m + conj Z_{N-m}) / 2 and
   // X_S = -i (Z_m - conj Z_{N-m}) / 2, for both pairs of a pair-pair, into the B images
-  const int nmu = J.mlim / P.mres + 1;
-  const int fl = k & 63;
-  for (int idx = threadIdx.x; idx < nmu * HP; idx += blockDim.x) {
-    const int hp = idx % HP, im = idx / HP, m = im * P.mres;
+  // Lanes 2j and 2j + 1 hold pair-pairs hp and hp + 1 (4 consecutive pairs) of one order:
+  // after one exchange the even lane stores the 4 pairs of the real row and the odd lane
+  // those of the imaginary row, two adjacent 16-byte core-matrix rows, so every store of a
+  // warp fills whole 32-byte sectors. Pairs past npair carry zero weights and store zeros
+  // into the padding of their K-step.
+  static_assert(HP % 2 == 0, "pair-pairs go in lane pairs");
+  const int nmu = J.mlim / P.mres + 1, nitem = nmu * HP;
+  const int fl = k & 63, lane = threadIdx.x & 31;
+  const bool odd = lane & 1;
+  for (int base = threadIdx.x - lane; base < nitem; base += blockDim.x) {
+    const int idx = base + lane;
+    const bool valid = idx < nitem;
+    const int hp = idx % HP, im = valid ? idx / HP : 0, m = im * P.mres;
     const int pa = p0 + 2 * hp;
-    if (pa >= npair) continue;
     const C2 zm = ldc(X, sidx<HP>(J.perm[m], hp));
     const C2 zc = ldc(X, sidx<HP>(J.perm[m == 0 ? 0 : N - m], hp));
     const u64 sre = add2(zm.re, zc.re), sim = sub2(zm.im, zc.im);   // Z_m + conj Z_c
     const u64 dre = sub2(zm.re, zc.re), dim = add2(zm.im, zc.im);   // Z_m - conj Z_c
     const u64 hw = pk(make_float2(0.5f * wfac[2 * hp], 0.5f * wfac[2 * hp + 1]));
-    const float2 Ere = up(mul2(hw, add2(sre, dim))), Eim = up(mul2(hw, sub2(sim, dre)));
-    const float2 Ore = up(mul2(hw, sub2(sre, dim))), Oim = up(mul2(hw, add2(sim, dre)));
-    const int kk = pa & 7;
-    float* d0 = J.Wout + f2_btile_base(im, 0, pa, k, npair, J.nf);
-    float* d1 = J.Wout + f2_btile_base(im, 1, pa, k, npair, J.nf);
-    *reinterpret_cast<float2*>(d0 + btile_off(2 * fl, kk)) = Ere;
-    *reinterpret_cast<float2*>(d0 + btile_off(2 * fl + 1, kk)) = Eim;
-    *reinterpret_cast<float2*>(d1 + btile_off(2 * fl, kk)) = Ore;
-    *reinterpret_cast<float2*>(d1 + btile_off(2 * fl + 1, kk)) = Oim;
+    const u64 Ere = mul2(hw, add2(sre, dim)), Eim = mul2(hw, sub2(sim, dre));
+    const u64 Ore = mul2(hw, sub2(sre, dim)), Oim = mul2(hw, add2(sim, dre));
+    // the even lane keeps its real parts and takes its partner's; the odd lane the reverse
+    const u64 eo = __shfl_xor_sync(0xffffffffu, odd ? Ere : Eim, 1);
+    const u64 oo = __shfl_xor_sync(0xffffffffu, odd ? Ore : Oim, 1);
+    if (!valid) continue;
+    const float2 e0 = up(odd ? eo : Ere), e1 = up(odd ? Eim : eo);
+    const float2 o0 = up(odd ? oo : Ore), o1 = up(odd ? Oim : oo);
+    const int pe = pa - (odd ? 2 : 0);     // first of the 4 pairs, a multiple of 4
+    const int off = btile_off(2 * fl + (odd ? 1 : 0), pe & 7);
+    *reinterpret_cast<float4*>(J.Wout + f2_btile_base(im, 0, pe, k, npair, J.nf) + off) = make_float4(e0.x, e0.y, e1.x, e1.y);
+    *reinterpret_cast<float4*>(J.Wout + f2_btile_base(im, 1, pe, k, npair, J.nf) + off) = make_float4(o0.x, o0.y, o1.x, o1.y);
   }
   if (p0 <= npair - 1 && npair - 1 < p0 + 2 * HP) {
     // the CTA holding the last pair also zeroes the padding pairs npair .. npair8-1

@@ -23,12 +23,14 @@
 // analysis B images (Fourier coefficients) arrive in FP32 from the FFT and are split in
 // shared memory.
 //
-// CTA organisation (576 threads, one parity class per CTA): one thread of warp 17 fills a
-// shared-memory ring of chunk stages (8 image K-steps of A and B each) with bulk copies;
-// in the analysis, warps 0-7 split each chunk's B tiles in place; one thread of warp 8
-// (which allocates TMEM) issues the MMAs from shared memory, 12 per chunk, into one of 4
-// TMEM accumulators and commits once per chunk; warps 9-16 drain each finished chunk with
-// tcgen05.ld into round-to-nearest FP32 register sums. Long accumulation chains inside
+// CTA organisation (one parity class per CTA; at N = 128: 27 warps, 864 threads): one
+// thread of the loader warp (25) fills a shared-memory ring of chunk stages (8 image
+// K-steps of A and B each) with bulk copies; in the analysis, warps 0-7 split each
+// chunk's B tiles in place; one thread of warp 8 (which allocates TMEM) issues the MMAs
+// from shared memory, 12 per chunk, into one of 4 TMEM accumulators and commits once per
+// chunk; warps 9-24 drain each finished chunk with tcgen05.ld into round-to-nearest FP32
+// register sums and store the tile; warp 26 writes the analysis output's structural
+// zeros (degrees below m and above lcap). Long accumulation chains inside
 // the tensor core round toward zero and would bias sums of many terms; short chunks keep
 // that bias below 1e-6 relative at any lmax.
 // Every mbarrier wait is bounded (2 s of %globaltimer); a timeout sets the
@@ -50,10 +52,21 @@ constexpr unsigned long long kWaitNs = 2000000000ull;
 constexpr int kChunk = 8;        // image K-steps (4 f16 K-steps, 12 MMAs) accumulated before promotion
 constexpr int kScR = 16;         // ring of per-chunk B column scales
 constexpr int kSegRows = 16;     // table segment padding (degrees): one f16 K-step
-// Warp roles: splitters [0, kSW), MMA issuer kSW, promotion [kSW + 1, kSW + 9), loader kSW + 9.
+// Warp roles: splitters [0, kSW), MMA issuer kSW, promotion [kSW + 1, kSW + 1 + kPW), loader
+// kSW + 1 + kPW, and at N >= 64 a clearing warp after it. The promotion warps (kPW of them,
+// four per TMEM lane quadrant) each drain and store a quarter (kPW = 16, N >= 64) or a half
+// (kPW = 8) of a tile's columns; the clearing warp writes the analysis output's structural
+// zeros (l < m, l > lcap), which the promotion warps do themselves below N = 64.
 constexpr int kSW = 8;
-constexpr int kMmaWarp = kSW, kPromo0 = kSW + 1, kLoaderWarp = kSW + 9;
-constexpr int kThreads = 32 * (kSW + 10);
+constexpr int kMmaWarp = kSW, kPromo0 = kSW + 1;
+template <int N>
+constexpr int kPW = (N >= 64) ? 16 : 8;
+template <int N>
+constexpr int kLoaderWarp = kPromo0 + kPW<N>;
+template <int N>
+constexpr int kZW = (N >= 64) ? 1 : 0;
+template <int N>
+constexpr int kThreads = 32 * (kLoaderWarp<N> + 1 + kZW<N>);
 constexpr int kAcc = 4;          // TMEM chunk accumulators
 
 struct Args {
@@ -330,7 +343,7 @@ __device__ __forceinline__ unsigned gemm_cta_setup(const Bars& B) {
     for (int s = 0; s < Smem<N>::kFull; ++s) mbar_init(&B.full[s], 2 * kSW);
     for (int s = 0; s < Smem<N>::kLd; ++s) mbar_init(&B.ldfull[s], 1);
     for (int s = 0; s < Smem<N>::kRel; ++s) mbar_init(&B.rel[s], 1);
-    for (int b = 0; b < kAcc; ++b) mbar_init(&B.acce[b], 8);   // one arrival per promotion warp
+    for (int b = 0; b < kAcc; ++b) mbar_init(&B.acce[b], kPW<N>);   // one arrival per promotion warp
     *B.abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -600,6 +613,25 @@ __device__ __forceinline__ bool mma_tile(const Args& a, const TileInfo& T, unsig
   return true;
 }
 
+// The first analysis tile of each order also clears that order's degrees l < m and
+// lcap < l <= lmax (dense layout; a packed output is cleared before the call); the two
+// parity tiles take half of the fields each. Threads t = t0, t0 + nt, ... of the clearing role.
+template <int N>
+__device__ __forceinline__ void clear_tile(const Args& a, const TileCoord& tc, int t0, int nt) {
+  if (tc.j0 != 0 || a.cpacked) return;
+  const PlanDev& P = a.P;
+  const int m = tc.im * P.mres, kb = tc.kb, par = tc.par;
+  const int nfl = min(N / 2, a.nf - kb), hf = (nfl + 1) / 2;
+  const int f0 = par ? hf : 0, f1 = par ? nfl : hf;
+  const int lcap = a.lcap, ntail = P.lmax - lcap, per = m + ntail;
+  const long long ld = a.ld_k;
+  float2* col0 = a.cout + (long long)m * (P.lmax + 1);
+  for (int fi = f0; fi < f1; ++fi) {
+    float2* col = col0 + (long long)(kb + fi) * ld;
+    for (int r = t0; r < per; r += nt) col[r < m ? r : lcap + 1 + (r - m)] = make_float2(0.f, 0.f);
+  }
+}
+
 // Promotion warps: drain each chunk into round-to-nearest FP32 sums, then store the tile
 // (the analysis also clears l < m and l > lcap in the first tile of an order). The
 // analysis undoes its per-chunk B scales chunk by chunk; the synthesis sums in units of
@@ -611,13 +643,14 @@ __device__ __forceinline__ bool promo_tile(const Args& a, const TileCoord& tc, c
   const PlanDev& P = a.P;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int q = warp & 3;                        // TMEM lane quadrant this warp may access
-  const int h = (warp - kPromo0) >> 2;           // column half
+  const int h = (warp - kPromo0) >> 2;           // column group of kCols columns
   const int row = 32 * q + lane;
   const unsigned lane_base = (unsigned)(32 * q) << 16;
-  constexpr int kLd = (N / 2 < 16) ? N / 2 : 16;   // columns per TMEM load
-  float acc[N / 2];
+  constexpr int kCols = N / (kPW<N> / 4);          // columns of this thread's TMEM lane
+  constexpr int kLd = (kCols < 16) ? kCols : 16;  // columns per TMEM load
+  float acc[kCols];
 #pragma unroll
-  for (int i = 0; i < N / 2; ++i) acc[i] = 0.f;
+  for (int i = 0; i < kCols; ++i) acc[i] = 0.f;
   bool ok = true;
   for (int c = 0; c < T.nch; ++c) {
     const unsigned gc = c0 + c;
@@ -629,10 +662,10 @@ __device__ __forceinline__ bool promo_tile(const Args& a, const TileCoord& tc, c
     ok = __all_sync(0xffffffffu, ok);   // warp-uniform: the TMEM loads are warp-collective
     if (!ok) return false;              // the chunk's MMAs may not have run: leave TMEM alone
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const unsigned dH = tmem + lane_base + bb * N + h * (N / 2);
-    const float4* fs = reinterpret_cast<const float4*>(B.fsc + (gc % kScR) * N + h * (N / 2));
+    const unsigned dH = tmem + lane_base + bb * N + h * kCols;
+    const float4* fs = reinterpret_cast<const float4*>(B.fsc + (gc % kScR) * N + h * kCols);
 #pragma unroll
-    for (int i = 0; i < N / 2; i += kLd) {
+    for (int i = 0; i < kCols; i += kLd) {
       float v[kLd];
       tmem_ld<kLd>(dH + i, v);
       if constexpr (MODE == 1) {
@@ -656,8 +689,8 @@ __device__ __forceinline__ bool promo_tile(const Args& a, const TileCoord& tc, c
   // Every Args field and the scale factor are read before the first store: the stores
   // go through generic pointers, after which the compiler would reload them.
   const int npair = P.npair, im = tc.im, par = tc.par, m = T.m, kb = tc.kb;
-  const int nf = a.nf, kf0 = kb + h * (N / 4);
-  const int nq = min(N / 4, nf - kf0);
+  const int nf = a.nf, kf0 = kb + h * (kCols / 2);
+  const int nq = min(kCols / 2, nf - kf0);
   if (MODE == 0) {
     const int pr = tc.p0 + row;
     if (pr < npair) {
@@ -665,7 +698,7 @@ __device__ __forceinline__ bool promo_tile(const Args& a, const TileCoord& tc, c
       const float2* fsc = reinterpret_cast<const float2*>(a.bsc + (2 * im + par) * 2 * btile_nfp(nf)) + kf0;
       float2* w = a.Wout + (((size_t)kf0 * P.nm + im) * 2 + par) * npair + pr;
 #pragma unroll
-      for (int qq = 0; qq < N / 4; ++qq)
+      for (int qq = 0; qq < kCols / 2; ++qq)
         if (qq < nq) {
           const float2 f = fsc[qq];
           w[qq * fstride] = make_float2(acc[2 * qq] * f.x, acc[2 * qq + 1] * f.y);
@@ -678,25 +711,11 @@ __device__ __forceinline__ bool promo_tile(const Args& a, const TileCoord& tc, c
       const long long ld = a.ld_k;
       float2* c = a.cout + (long long)kf0 * ld + coef_col(a, m) + l;
 #pragma unroll
-      for (int qq = 0; qq < N / 4; ++qq)
+      for (int qq = 0; qq < kCols / 2; ++qq)
         if (qq < nq) c[qq * ld] = make_float2(acc[2 * qq] * s, acc[2 * qq + 1] * s);
     }
   }
-  if (MODE == 1 && tc.j0 == 0 && !a.cpacked) {
-    // The first tile of each order also clears that order's degrees l < m and
-    // lcap < l <= lmax (dense layout; a packed output is cleared before the call); the
-    // two parity tiles take half of the fields each.
-    const int pt = tid - kPromo0 * 32;
-    const int nfl = min(N / 2, nf - kb), hf = (nfl + 1) / 2;
-    const int f0 = par ? hf : 0, f1 = par ? nfl : hf;
-    const int lcap = a.lcap, ntail = P.lmax - lcap, per = m + ntail;
-    const long long ld = a.ld_k;
-    float2* col0 = a.cout + (long long)m * (P.lmax + 1);
-    for (int fi = f0; fi < f1; ++fi) {
-      float2* col = col0 + (long long)(kb + fi) * ld;
-      for (int r = pt; r < per; r += 256) col[r < m ? r : lcap + 1 + (r - m)] = make_float2(0.f, 0.f);
-    }
-  }
+  if (MODE == 1 && kZW<N> == 0) clear_tile<N>(a, tc, tid - kPromo0 * 32, 32 * kPW<N>);
   return true;
 }
 
@@ -719,8 +738,8 @@ __device__ __forceinline__ TileQueue tile_queue(unsigned char* sm) {
   Q.ids = reinterpret_cast<volatile int*>(Q.empty + S::kQ);
   return Q;
 }
-template <int MODE>
-constexpr unsigned kQueueConsumers = (MODE == 1 ? kSW : 0) + 1 + 8;
+template <int MODE, int N>
+constexpr unsigned kQueueConsumers = (MODE == 1 ? kSW + kZW<N> : 0) + 1 + kPW<N>;
 
 // Runs the tiles of src (args(i), coord(i), n): i = blockIdx.x, blockIdx.x + gridDim.x, ...
 // for a static source; for a dynamic one (Src::kDynamic, the grouped kernels) the tiles
@@ -729,9 +748,10 @@ template <int MODE, int N, class Src>
 __device__ __forceinline__ void gemm_tiles(const Src& src, unsigned char* sm, const Bars& B, unsigned tmem) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // the synthesis B images arrive converted: its splitter warps have no work
-  const bool loader = (warp == kLoaderWarp && lane == 0), splitter = (MODE == 1 && warp < kSW),
-             mma = (warp == kMmaWarp && lane == 0), promo = (warp >= kPromo0 && warp < kPromo0 + 8);
-  const bool role = loader || splitter || mma || promo;
+  const bool loader = (warp == kLoaderWarp<N> && lane == 0), splitter = (MODE == 1 && warp < kSW),
+             mma = (warp == kMmaWarp && lane == 0), promo = (warp >= kPromo0 && warp < kPromo0 + kPW<N>),
+             clear = (MODE == 1 && kZW<N> == 1 && warp == kLoaderWarp<N> + 1);
+  const bool role = loader || splitter || mma || promo || clear;
   unsigned c0 = 0;
   unsigned issued = 0;   // loader: chunks 0 .. issued-1 had their copies issued (all but a skipped one)
   int committed = -1;    // MMA issuer: last chunk committed
@@ -773,6 +793,8 @@ __device__ __forceinline__ void gemm_tiles(const Src& src, unsigned char* sm, co
       ok = splitter_tile<MODE, N>(a, T, sm, B, c0);
     else if (mma)
       ok = mma_tile<MODE, N>(a, T, sm, B, tmem, c0, committed);
+    else if (clear)
+      clear_tile<N>(a, tc, lane, 32), ok = true;
     else
       ok = promo_tile<MODE, N>(a, tc, T, B, tmem, c0);
     if (!ok) break;
@@ -1093,7 +1115,7 @@ struct SingleSrc {
 
 // ntiles: synthesis nmu * nz * ntp * 2, analysis ntiles_list * nz * 2.
 template <int MODE, int N>
-__global__ void __launch_bounds__(kThreads, kCtasPerSm<N>) mixed_gemm_kernel(const __grid_constant__ Args a, int ntiles,
+__global__ void __launch_bounds__(kThreads<N>, kCtasPerSm<N>) mixed_gemm_kernel(const __grid_constant__ Args a, int ntiles,
                                                                              int nz, int ntp) {
   extern __shared__ __align__(1024) unsigned char sm[];
   const Bars B = gemm_bars<N>(sm);
@@ -1137,7 +1159,7 @@ struct GroupSrc {
 
 // Persistent GEMM over the tiles of many transforms, claimed from the counter *queue.
 template <int MODE, int N>
-__global__ void __launch_bounds__(kThreads, kCtasPerSm<N>) mixed_gemm_group_kernel(const Args* __restrict__ targs,
+__global__ void __launch_bounds__(kThreads<N>, kCtasPerSm<N>) mixed_gemm_group_kernel(const Args* __restrict__ targs,
                                                                                    const int4* __restrict__ items,
                                                                                    int nitems,
                                                                                    unsigned long long* __restrict__ done,
@@ -1148,7 +1170,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm<N>) mixed_gemm_group_kern
     const TileQueue Q = tile_queue<N>(sm);
     for (int s = 0; s < Smem<N>::kQ; ++s) {
       mbar_init(&Q.full[s], 1);
-      mbar_init(&Q.empty[s], kQueueConsumers<MODE>);
+      mbar_init(&Q.empty[s], kQueueConsumers<MODE, N>);
     }
   }
   const unsigned tmem = gemm_cta_setup<N>(B);
@@ -1292,7 +1314,7 @@ static int launch_gemm(const shtb_plan* p, const Args& a, int ntiles, int nz, in
   const int total = ntiles * nz;
   const int grid = std::max(1, std::min(total, sm_count() * kCtasPerSm<N>));
   prof_begin(st);
-  kern<<<grid, kThreads, smem, st>>>(a, total, nz, ntp);
+  kern<<<grid, kThreads<N>, smem, st>>>(a, total, nz, ntp);
   SHTB_LAUNCHED(MODE == 0 ? "tc gemm synthesis kernel" : "tc gemm analysis kernel");
   return SHTB_OK;
 }
@@ -1469,11 +1491,11 @@ int launch_gemm_group(int mode, const void* targs, const int4* items, int nitems
   if (mode == 0) {
     auto kern = mixed_gemm_group_kernel<0, 16>;
     SHTB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "group gemm smem attr");
-    kern<<<grid, kThreads, smem, st>>>((const Args*)targs, items, nitems, done, queue);
+    kern<<<grid, kThreads<16>, smem, st>>>((const Args*)targs, items, nitems, done, queue);
   } else {
     auto kern = mixed_gemm_group_kernel<1, 16>;
     SHTB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "group gemm smem attr");
-    kern<<<grid, kThreads, smem, st>>>((const Args*)targs, items, nitems, done, queue);
+    kern<<<grid, kThreads<16>, smem, st>>>((const Args*)targs, items, nitems, done, queue);
   }
   count_launch();
   SHTB_TRY_CUDA(cudaGetLastError(), "group gemm launch");
