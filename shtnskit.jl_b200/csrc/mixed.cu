@@ -462,25 +462,30 @@ __device__ __forceinline__ bool loader_tile(const Args& a, const TileCoord& tc, 
 // a chunk form f16 K-step g (K = 16), whose hi tile takes the place of FP32 tile 2g and lo
 // tile that of 2g + 1 (the table holds A in that form already). kTpr threads per row, each
 // owning whole f16 K-steps g = v, v + kTpr, ...: each row of the chunk is scaled by the power
-// of two 2^e that brings its largest magnitude into [2^14, 2^15) (a first pass over the
-// thread's values finds the row maximum), split into f16 hi + lo and written in place (the
-// same core-matrix byte order: 16-byte rows of 8 f16 values), one 16-byte store per FP32
-// K-step half for hi and one for lo; a thread's writes land only in its own two FP32 tiles. Lane layout: the 8 lanes of a quarter
-// warp take 8 consecutive rows of one core-matrix group (so every 16-byte access of a
-// quarter warp covers one 128-byte run), and a row's kTpr threads sit 8 lanes apart
-// (partners by xor 8, 16). The factor 2^-(e + s) that undoes this and the table's scale 2^s
-// goes to the chunk's entry of the scale ring. A missing odd K-step at the end of a tile
-// converts as zeros. The splitter warps form two groups that take the chunks in turn (group
-// gc % 2), so conversions of consecutive chunks overlap. A group reaches chunk gc after its
-// own chunk gc - 2, possibly before the loader has refilled the stage; the copy barriers
-// form a ring of 2 kSt (an even count), so the previous phase of chunk gc's barrier belongs
-// to chunk gc - 2 kSt, the group's own, whose copies it saw land: its wait cannot match an
-// older phase.
+// of two 2^e that brings its largest magnitude into [2^14, 2^15), split into f16 hi + lo and
+// written in place (the same core-matrix byte order: 16-byte rows of 8 f16 values), one
+// 16-byte store per FP32 K-step half for hi and one for lo; a thread's writes land only in
+// its own two FP32 tiles. A thread with at most 32 values keeps them in registers between
+// the row maximum and the conversion; with more it reads them twice (maximum, then
+// conversion). Lane layout: the 8 lanes of a quarter warp take 8 consecutive rows of one
+// core-matrix group (so every 16-byte access of a quarter warp covers one 128-byte run),
+// and a row's kTpr threads sit 8 lanes apart (partners by xor 8, 16). The factor
+// 2^-(e + s) that undoes this and the table's scale 2^s goes to the chunk's entry of the
+// scale ring. A missing odd K-step at the end of a tile converts as zeros. Below N = 128
+// the splitter warps form two groups that take the chunks in turn (group gc % 2), so
+// conversions of consecutive chunks overlap; at N = 128 all eight convert every chunk
+// (2 threads per row), which halves a conversion's latency. A group reaches chunk gc after
+// its own previous chunk, possibly before the loader has refilled the stage; the copy
+// barriers form a ring of 2 kSt (a multiple of the group count), so the previous phase of
+// chunk gc's barrier belongs to chunk gc - 2 kSt, the group's own, whose copies it saw
+// land: its wait cannot match an older phase.
 template <int MODE, int N>
 __device__ __forceinline__ bool splitter_tile(const Args& a, const TileInfo& T, unsigned char* sm, const Bars& B,
                                                   unsigned c0) {
   using S = Smem<N>;
-  constexpr int kSG = 2;                                                 // splitter groups
+  // splitter groups: one at N = 128 (2 threads per row, 32 values each, converted in one
+  // pass from registers), two otherwise
+  constexpr int kSG = (N == 128) ? 1 : 2;
   static_assert(S::kLd % kSG == 0, "copy-barrier ring a multiple of the groups");
   constexpr int kGT = 32 * kSW / kSG;                                    // threads per group
   constexpr int kTpr = (kGT >= 4 * N) ? 4 : (kGT >= N) ? kGT / N : 1;     // threads per B row (1, 2 or 4)
@@ -504,61 +509,106 @@ __device__ __forceinline__ bool splitter_tile(const Args& a, const TileInfo& T, 
     for (int ri = 0; ri < kRpt; ++ri) {
       const int r = row_w + ri * (kGT / kTpr);
       const bool rowok = r < nrows;
-      // the thread's K-steps (both 16-byte halves) go to registers with the row's largest
-      // magnitude; all of the row's values are read before any is overwritten (a row's
-      // threads share a warp), then converted from the registers
-      // pass 1: the row's largest magnitude over the thread's f16 K-steps (FP32 K-steps 2g,
-      // 2g + 1 for g = v, v + kTpr, ...), reduced over the row's threads
-      unsigned mx = 0;
-#pragma unroll
-      for (int j = 0; j < kGpt; ++j) {
-        const int g = v + j * kTpr;
-#pragma unroll
-        for (int w = 0; w < 2; ++w) {
-          const int st = 2 * g + w;
-          if (rowok && st < nk) {
-            const unsigned char* src = Bs + st * T.bstr + tile_off(r, 0);
-            const float4 x0 = *reinterpret_cast<const float4*>(src);
-            const float4 x1 = *reinterpret_cast<const float4*>(src + 128);
-            mx = max(mx, max(max(__float_as_uint(x0.x) & 0x7fffffffu, __float_as_uint(x0.y) & 0x7fffffffu),
-                             max(__float_as_uint(x0.z) & 0x7fffffffu, __float_as_uint(x0.w) & 0x7fffffffu)));
-            mx = max(mx, max(max(__float_as_uint(x1.x) & 0x7fffffffu, __float_as_uint(x1.y) & 0x7fffffffu),
-                             max(__float_as_uint(x1.z) & 0x7fffffffu, __float_as_uint(x1.w) & 0x7fffffffu)));
-          }
-        }
-      }
-#pragma unroll
-      for (int o = 8; o < 8 * kTpr; o <<= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-      // max * 2^e in [2^14, 2^15) (e at most 100: rows below 2^-86 keep the f16 subnormal steps)
-      const int e = min(141 - (int)(mx >> 23), 100);
-      const float su = __int_as_float((e + 127) << 23);
-      // pass 2: each f16 K-step g reads and writes only its own two FP32 tiles 2g, 2g + 1
-      // (hi of both into 2g, lo of both into 2g + 1), so it converts in place right after
-      // reading them
-      if (rowok) {
+      int e;
+      if constexpr (kGpt * 16 <= 32) {
+        // one pass: the thread's values (kGpt f16 K-steps, both FP32 tiles 2g, 2g + 1, two
+        // 16-byte halves each) stay in registers between the row maximum and the conversion
+        float4 x[kGpt][4];
+        unsigned mx = 0;
 #pragma unroll
         for (int j = 0; j < kGpt; ++j) {
           const int g = v + j * kTpr;
-          if (g < nk2) {
-            unsigned char* b0 = Bs + 2 * g * T.bstr + tile_off(r, 0);
-            float4 x[4];
 #pragma unroll
-            for (int w = 0; w < 2; ++w) {
-              const bool have = 2 * g + w < nk;   // a missing odd K-step converts as zeros
-              const unsigned char* src = b0 + w * T.bstr;
-              x[2 * w] = have ? *reinterpret_cast<const float4*>(src) : make_float4(0.f, 0.f, 0.f, 0.f);
-              x[2 * w + 1] = have ? *reinterpret_cast<const float4*>(src + 128) : make_float4(0.f, 0.f, 0.f, 0.f);
+          for (int w = 0; w < 2; ++w) {
+            const bool have = rowok && 2 * g + w < nk;   // a missing odd K-step converts as zeros
+            const unsigned char* src = Bs + (2 * g + w) * T.bstr + tile_off(r, 0);
+            x[j][2 * w] = have ? *reinterpret_cast<const float4*>(src) : make_float4(0.f, 0.f, 0.f, 0.f);
+            x[j][2 * w + 1] = have ? *reinterpret_cast<const float4*>(src + 128) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+            for (int hh = 0; hh < 2; ++hh) {
+              const float4 y = x[j][2 * w + hh];
+              mx = max(mx, max(max(__float_as_uint(y.x) & 0x7fffffffu, __float_as_uint(y.y) & 0x7fffffffu),
+                               max(__float_as_uint(y.z) & 0x7fffffffu, __float_as_uint(y.w) & 0x7fffffffu)));
             }
+          }
+        }
 #pragma unroll
-            for (int w = 0; w < 2; ++w) {
-              uint4 hi, lo;
-              split_h2(x[2 * w].x * su, x[2 * w].y * su, hi.x, lo.x);
-              split_h2(x[2 * w].z * su, x[2 * w].w * su, hi.y, lo.y);
-              split_h2(x[2 * w + 1].x * su, x[2 * w + 1].y * su, hi.z, lo.z);
-              split_h2(x[2 * w + 1].z * su, x[2 * w + 1].w * su, hi.w, lo.w);
-              // FP32 K-step 2g + w -> khalf w of the hi tile (2g) and of the lo tile (2g + 1)
-              *reinterpret_cast<uint4*>(b0 + w * 128) = hi;
-              *reinterpret_cast<uint4*>(b0 + T.bstr + w * 128) = lo;
+        for (int o = 8; o < 8 * kTpr; o <<= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        e = min(141 - (int)(mx >> 23), 100);
+        const float su = __int_as_float((e + 127) << 23);
+        if (rowok) {
+#pragma unroll
+          for (int j = 0; j < kGpt; ++j) {
+            const int g = v + j * kTpr;
+            if (g < nk2) {
+              unsigned char* b0 = Bs + 2 * g * T.bstr + tile_off(r, 0);
+#pragma unroll
+              for (int w = 0; w < 2; ++w) {
+                uint4 hi, lo;
+                split_h2(x[j][2 * w].x * su, x[j][2 * w].y * su, hi.x, lo.x);
+                split_h2(x[j][2 * w].z * su, x[j][2 * w].w * su, hi.y, lo.y);
+                split_h2(x[j][2 * w + 1].x * su, x[j][2 * w + 1].y * su, hi.z, lo.z);
+                split_h2(x[j][2 * w + 1].z * su, x[j][2 * w + 1].w * su, hi.w, lo.w);
+                *reinterpret_cast<uint4*>(b0 + w * 128) = hi;
+                *reinterpret_cast<uint4*>(b0 + T.bstr + w * 128) = lo;
+              }
+            }
+          }
+        }
+      } else {
+        // two passes (more values than registers). pass 1: the row's largest magnitude over the thread's f16 K-steps (FP32 K-steps 2g,
+        // 2g + 1 for g = v, v + kTpr, ...), reduced over the row's threads
+        unsigned mx = 0;
+#pragma unroll
+        for (int j = 0; j < kGpt; ++j) {
+          const int g = v + j * kTpr;
+#pragma unroll
+          for (int w = 0; w < 2; ++w) {
+            const int st = 2 * g + w;
+            if (rowok && st < nk) {
+              const unsigned char* src = Bs + st * T.bstr + tile_off(r, 0);
+              const float4 x0 = *reinterpret_cast<const float4*>(src);
+              const float4 x1 = *reinterpret_cast<const float4*>(src + 128);
+              mx = max(mx, max(max(__float_as_uint(x0.x) & 0x7fffffffu, __float_as_uint(x0.y) & 0x7fffffffu),
+                               max(__float_as_uint(x0.z) & 0x7fffffffu, __float_as_uint(x0.w) & 0x7fffffffu)));
+              mx = max(mx, max(max(__float_as_uint(x1.x) & 0x7fffffffu, __float_as_uint(x1.y) & 0x7fffffffu),
+                               max(__float_as_uint(x1.z) & 0x7fffffffu, __float_as_uint(x1.w) & 0x7fffffffu)));
+            }
+          }
+        }
+#pragma unroll
+        for (int o = 8; o < 8 * kTpr; o <<= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        // max * 2^e in [2^14, 2^15) (e at most 100: rows below 2^-86 keep the f16 subnormal steps)
+        e = min(141 - (int)(mx >> 23), 100);
+        const float su = __int_as_float((e + 127) << 23);
+        // pass 2: each f16 K-step g reads and writes only its own two FP32 tiles 2g, 2g + 1
+        // (hi of both into 2g, lo of both into 2g + 1), so it converts in place right after
+        // reading them
+        if (rowok) {
+#pragma unroll
+          for (int j = 0; j < kGpt; ++j) {
+            const int g = v + j * kTpr;
+            if (g < nk2) {
+              unsigned char* b0 = Bs + 2 * g * T.bstr + tile_off(r, 0);
+              float4 x[4];
+#pragma unroll
+              for (int w = 0; w < 2; ++w) {
+                const bool have = 2 * g + w < nk;   // a missing odd K-step converts as zeros
+                const unsigned char* src = b0 + w * T.bstr;
+                x[2 * w] = have ? *reinterpret_cast<const float4*>(src) : make_float4(0.f, 0.f, 0.f, 0.f);
+                x[2 * w + 1] = have ? *reinterpret_cast<const float4*>(src + 128) : make_float4(0.f, 0.f, 0.f, 0.f);
+              }
+#pragma unroll
+              for (int w = 0; w < 2; ++w) {
+                uint4 hi, lo;
+                split_h2(x[2 * w].x * su, x[2 * w].y * su, hi.x, lo.x);
+                split_h2(x[2 * w].z * su, x[2 * w].w * su, hi.y, lo.y);
+                split_h2(x[2 * w + 1].x * su, x[2 * w + 1].y * su, hi.z, lo.z);
+                split_h2(x[2 * w + 1].z * su, x[2 * w + 1].w * su, hi.w, lo.w);
+                // FP32 K-step 2g + w -> khalf w of the hi tile (2g) and of the lo tile (2g + 1)
+                *reinterpret_cast<uint4*>(b0 + w * 128) = hi;
+                *reinterpret_cast<uint4*>(b0 + T.bstr + w * 128) = lo;
+              }
             }
           }
         }
