@@ -150,10 +150,18 @@ struct shtb_plan {
   float* d_tab = nullptr;                 // synthesis tile images (start of the table allocation)
   float* d_tab_ana = nullptr;             // analysis tile images
   const long long* d_tab_seg = nullptr;
+  // per-tile live-chunk masks of the GEMMs (chunks whose P image is all zero are skipped):
+  // synthesis [2 nm][npp / 128], analysis [2 nm][tab_njt]
+  const unsigned long long* d_tab_msk_s = nullptr;
+  const unsigned long long* d_tab_msk_a = nullptr;
+  int tab_njt = 0;
   size_t tab_bytes = 0;
   int npp = 0;
   std::vector<long long> htab_seg;
-  std::vector<int2> hmx_tiles;
-  int mx_tiles_key = -1;
+  std::vector<unsigned long long> hmsk_s, hmsk_a;   // host copies of the live-chunk masks
+  // GEMM tile lists (analysis: (im, j0); synthesis: (im, p0)) for truncation degree key
+  std::vector<int2> hmx_tiles, hmx_stiles;
+  int mx_tiles_key = -1, mx_stiles_key = -1;
   int2* d_mx_tiles = nullptr;
+  int2* d_mx_stiles = nullptr;
 };

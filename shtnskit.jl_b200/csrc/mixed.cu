@@ -74,6 +74,12 @@ struct Args {
   const float* tab;          // tile images of this direction (synthesis or analysis)
   const long long* seg;      // [2*nm+1] first table row of segment (im, parity); rows hold npp pairs
   int npp;
+  // live-chunk masks of the tiles (bit c: chunk c's A image has a nonzero value; chunks
+  // from 64 on always run), or null (every chunk runs): synthesis [2 nm][npp / 128] by pair
+  // tile, analysis [2 nm][njt] by degree tile
+  const unsigned long long* mskS;
+  const unsigned long long* mskA;
+  int njt;
   const float2* cin;         // synthesis: coefficients (input of the B packing)
   float* bimg;               // B tile images: synthesis f16 hi/lo pairs written by the packing,
                              //   analysis FP32 written by the FFT (converted in shared memory)
@@ -86,7 +92,7 @@ struct Args {
   int sc_mode;               // 0 none, 1 multiply, 2 divide
   float mf0, mf1;
   int nf, lend, lcap;
-  const int2* tiles;         // analysis tiles (im, j0)
+  const int2* tiles;         // tiles (im, p0) of the synthesis, (im, j0) of the analysis
   int* err;
   int cpacked;               // coefficients in the packed LM layout (field stride ld_k = nlm)
   unsigned long long wait_ns;  // limit of every bounded mbarrier wait (kWaitNs unless a test shortens it)
@@ -387,21 +393,37 @@ __device__ __forceinline__ void gemm_cta_teardown(unsigned tmem) {
 // it for chunk gc + kAcc. The ring sizes keep every waiter from seeing a barrier two
 // phases ahead.
 struct TileInfo {
-  int m, nks, nch;
+  int m, nks, nch;          // K-steps; chunks with a nonzero A block (the ones every role runs)
+  int nall;                 // chunks of the tile's K range
+  unsigned long long live;  // chunk c < 64 runs iff bit c is set (chunks from 64 on always run)
   long long sg, ln;   // table segment start and rows of (im, par)
   int arows;          // rows of the A tile image (128, fewer in the last analysis tile)
   unsigned bstr;      // bytes from one K-step's B tile to the next in a stage
   unsigned bbytes;    // bytes of one K-step's B tile image (this CTA's fields)
 };
 
+__device__ __forceinline__ bool chunk_live(const TileInfo& T, int c) { return c >= 64 || ((T.live >> c) & 1ull); }
+
+// The live-chunk mask of a tile (all ones without masks).
 template <int MODE>
-__device__ __forceinline__ TileInfo tile_info(const Args& a, const TileCoord& tc) {
+__device__ __forceinline__ unsigned long long tile_live(const Args& a, const TileCoord& tc) {
+  if (MODE == 0)
+    return a.mskS ? a.mskS[(long long)(2 * tc.im + tc.par) * (a.npp / kM) + tc.p0 / kM] : ~0ull;
+  return a.mskA ? a.mskA[(long long)(2 * tc.im + tc.par) * a.njt + tc.j0 / kM] : ~0ull;
+}
+
+template <int MODE>
+__device__ __forceinline__ TileInfo tile_info(const Args& a, const TileCoord& tc, unsigned long long live) {
   TileInfo T;
   T.m = tc.im * a.P.mres;
   T.sg = a.seg[2 * tc.im + tc.par];
   T.ln = a.seg[2 * tc.im + tc.par + 1] - T.sg;
   T.nks = tile_ksteps<MODE>(a, tc);
-  T.nch = (T.nks + kChunk - 1) / kChunk;
+  T.nall = (T.nks + kChunk - 1) / kChunk;
+  // A chunk (64 degree rows x 128 pairs in the synthesis, 128 degree rows x 64 pairs in the
+  // analysis) whose P image is all zero adds exact zeros: no role runs it.
+  T.live = live;
+  T.nch = __popcll(T.nall >= 64 ? T.live : T.live & ((1ull << T.nall) - 1)) + max(T.nall - 64, 0);
   T.arows = (MODE == 0) ? kM : min(kM, (int)T.ln - tc.j0);
   // B images of consecutive K-steps are contiguous when all fields fit one 64-field block
   const int nfp = btile_nfp(a.nf);
@@ -431,8 +453,9 @@ __device__ __forceinline__ bool loader_tile(const Args& a, const TileCoord& tc, 
   const unsigned bbytes = T.bbytes;
   const bool bcontig = nfp <= 64;
   int* err = a.err;
-  for (int c = 0; c < T.nch; ++c) {
-    const unsigned gc = c0 + c;
+  for (int c = 0, q = 0; c < T.nall; ++c) {
+    if (!chunk_live(T, c)) continue;
+    const unsigned gc = c0 + q++;
     const int st = gc % S::kSt;
     if (gc >= S::kSt) {
       const unsigned q = gc - S::kSt;   // the chunk that last used this stage
@@ -498,8 +521,9 @@ __device__ __forceinline__ bool splitter_tile(const Args& a, const TileInfo& T, 
   const int row_w = (tid >> 5) * kRpw + 8 * (slot / kTpr) + (lane & 7);   // this thread's row (first pass)
   const int nrows = min((int)(T.bbytes >> 5), N);     // B rows loaded (2 per field)
   const int sa = f16_table_exp(a.P.lmax);
-  for (int c = 0; c < T.nch; ++c) {
-    const unsigned gc = c0 + c;
+  for (int c = 0, q = 0; c < T.nall; ++c) {
+    if (!chunk_live(T, c)) continue;
+    const unsigned gc = c0 + q++;
     if ((int)(gc % kSG) != grp) continue;
     const int nk = min(kChunk, T.nks - c * kChunk), nk2 = (nk + 1) >> 1;
     const bool ok = mbar_wait(&B.ldfull[gc % S::kLd], (gc / S::kLd) & 1, B.abort_flag, a.err, a.wait_ns);
@@ -634,8 +658,9 @@ __device__ __forceinline__ bool mma_tile(const Args& a, const TileInfo& T, unsig
   const unsigned long long a0 = sdesc(sm), b0 = sdesc(sm + S::kStageA);
   const unsigned long long akDesc = ((unsigned)T.arows * kK * 4) >> 4;   // per image K-step: A
   const unsigned long long bkDesc = T.bstr >> 4;                         // and B
-  for (int c = 0; c < T.nch; ++c) {
-    const unsigned gc = c0 + c;
+  for (int c = 0, q = 0; c < T.nall; ++c) {
+    if (!chunk_live(T, c)) continue;
+    const unsigned gc = c0 + q++;
     const int bb = gc % kAcc;
     if (gc >= kAcc && !mbar_wait(&B.acce[bb], ((gc / kAcc) - 1) & 1, B.abort_flag, a.err, a.wait_ns)) return false;
     const int k0 = c * kChunk, k1 = min(T.nks, k0 + kChunk);
@@ -807,6 +832,10 @@ __device__ __forceinline__ void gemm_tiles(const Src& src, unsigned char* sm, co
   int committed = -1;    // MMA issuer: last chunk committed
   int skip = -1;
   int i = blockIdx.x;
+  unsigned long long live_next = ~0ull;
+  if constexpr (!Src::kDynamic) {
+    if (i < src.n) live_next = tile_live<MODE>(src.args(i), src.coord(i));
+  }
   for (unsigned t = 0; role; ++t) {
     if constexpr (Src::kDynamic) {
       using S = Smem<N>;
@@ -834,7 +863,14 @@ __device__ __forceinline__ void gemm_tiles(const Src& src, unsigned char* sm, co
     }
     const Args& a = src.args(i);
     const TileCoord tc = src.coord(i);
-    const TileInfo T = tile_info<MODE>(a, tc);
+    unsigned long long live = ~0ull;
+    if constexpr (!Src::kDynamic) {
+      // this tile's mask was loaded one tile ahead; start the next tile's load now
+      live = live_next;
+      const int in = i + (int)gridDim.x;
+      if (in < src.n) live_next = tile_live<MODE>(src.args(in), src.coord(in));
+    }
+    const TileInfo T = tile_info<MODE>(a, tc, live);
     if (blockIdx.x == 0) skip = a.skip_chunk;
     bool ok;
     if (loader)
@@ -1131,46 +1167,37 @@ __global__ void __launch_bounds__(kPack1Threads) mixed_pack_group_kernel(const A
   }
 }
 
-// Tiles of one transform, in order of decreasing work: synthesis tile i = ((im * nz + z)
-// * ntp + ptile) * 2 + par (lower orders have more degrees); analysis tile i = (list
-// index * nz + z) * 2 + par over the (im, j0) list. z = block of N/2 fields.
+// Tiles of one transform: tile i = (list index * nz + z) * 2 + par over the tile list
+// (synthesis (im, p0), analysis (im, j0), in order of decreasing work), z = block of N/2
+// fields.
 template <int MODE, int N>
 struct SingleSrc {
   static constexpr bool kDynamic = false;
   const Args& a;
-  int n, nz, ntp;
+  int n, nz;
   __device__ const Args& args(int) const { return a; }
   __device__ void tile_done(int) const {}
   __device__ TileCoord coord(int i) const {
     TileCoord tc;
     tc.par = i & 1;
     int r = i >> 1;
-    if (MODE == 0) {
-      const int pt = r % ntp;
-      r /= ntp;
-      tc.kb = (r % nz) * (N / 2);
-      tc.im = r / nz;
-      tc.p0 = pt * kM;
-      tc.j0 = 0;
-    } else {
-      tc.kb = (r % nz) * (N / 2);
-      const int2 t = a.tiles[r / nz];
-      tc.im = t.x;
-      tc.j0 = t.y;
-      tc.p0 = 0;
-    }
+    tc.kb = (r % nz) * (N / 2);
+    const int2 t = a.tiles[r / nz];   // (im, first pair) or (im, first degree row)
+    tc.im = t.x;
+    tc.p0 = (MODE == 0) ? t.y : 0;
+    tc.j0 = (MODE == 0) ? 0 : t.y;
     return tc;
   }
 };
 
-// ntiles: synthesis nmu * nz * ntp * 2, analysis ntiles_list * nz * 2.
+// ntiles: tile list length * nz * 2.
 template <int MODE, int N>
 __global__ void __launch_bounds__(kThreads<N>, kCtasPerSm<N>) mixed_gemm_kernel(const __grid_constant__ Args a, int ntiles,
-                                                                             int nz, int ntp) {
+                                                                             int nz) {
   extern __shared__ __align__(1024) unsigned char sm[];
   const Bars B = gemm_bars<N>(sm);
   const unsigned tmem = gemm_cta_setup<N>(B);
-  const SingleSrc<MODE, N> src{a, ntiles, nz, ntp};
+  const SingleSrc<MODE, N> src{a, ntiles, nz};
   gemm_tiles<MODE, N>(src, sm, B, tmem);
   gemm_cta_teardown<N>(tmem);
 }
@@ -1232,7 +1259,8 @@ __global__ void __launch_bounds__(kThreads<N>, kCtasPerSm<N>) mixed_gemm_group_k
 // Table: P_l^m(x_pair) as FP32, degree row j = (l-m)/2 of segment (im, (l-m)%2), written
 // into both tile images (layout described at the top of this file).
 __global__ void mixed_table_kernel(PlanDev P, float* __restrict__ tabS, float* __restrict__ tabA,
-                                   const long long* __restrict__ seg, int npp) {
+                                   const long long* __restrict__ seg, int npp, unsigned char* __restrict__ nzb, int nrb,
+                                   int npb) {
   const int pair = blockIdx.x * blockDim.x + threadIdx.x;
   const int im = blockIdx.y;
   if (pair >= P.npair) return;
@@ -1244,6 +1272,8 @@ __global__ void mixed_table_kernel(PlanDev P, float* __restrict__ tabS, float* _
   const int pt = pair / kM, pr = pair % kM;
   const float asc = (float)(1 << f16_table_exp(P.lmax));   // exact scaling
   double ra = 0.0, rb = 0.0;
+  unsigned long long nzm[2] = {0ull, 0ull};   // 64-row blocks of each parity with a nonzero value
+  unsigned char* nzf = nzb + (long long)(2 * im) * nrb * npb + pair / 64;
   for (int l = m; l <= P.lrec; ++l) {
     double r;
     if (l == l0)
@@ -1273,6 +1303,39 @@ __global__ void mixed_table_kernel(PlanDev P, float* __restrict__ tabS, float* _
     *reinterpret_cast<__half*>(ds + kTileBytesA) = lo;
     *reinterpret_cast<__half*>(da) = h;
     *reinterpret_cast<__half*>(da + rows * kK * 4) = lo;
+    if ((__half_as_ushort(h) | __half_as_ushort(lo)) & 0x7fffu) {
+      const int b = j / 64;
+      if (b < 64)
+        nzm[par] |= 1ull << b;
+      else
+        nzf[((long long)par * nrb + b) * npb] = 1;
+    }
+  }
+  for (int par = 0; par < 2; ++par)
+    for (unsigned long long bits = nzm[par]; bits; bits &= bits - 1)
+      nzf[((long long)par * nrb + __ffsll((long long)bits) - 1) * npb] = 1;
+}
+
+// Live-chunk masks from the block flags: synthesis tile (im, par, pair tile pt) chunk c =
+// degree rows 64 c.. of pair blocks 2 pt, 2 pt + 1; analysis tile (im, par, degree tile jt)
+// chunk c = pairs 64 c.. of row blocks 2 jt, 2 jt + 1. One thread per (segment, tile).
+__global__ void mixed_mask_kernel(const unsigned char* __restrict__ nzb, int nseg, int nrb, int npb, int njt,
+                                  unsigned long long* __restrict__ mskS, unsigned long long* __restrict__ mskA) {
+  const int ntp = npb / 2;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nseg * (ntp + njt)) return;
+  const int sgi = i / (ntp + njt), r = i - sgi * (ntp + njt);
+  const unsigned char* f = nzb + (long long)sgi * nrb * npb;
+  unsigned long long live = 0ull;
+  if (r < ntp) {
+    for (int c = 0; c < 64 && c < nrb; ++c)
+      if (f[c * npb + 2 * r] | f[c * npb + 2 * r + 1]) live |= 1ull << c;
+    mskS[(long long)sgi * ntp + r] = live;
+  } else {
+    const int jt = r - ntp;
+    for (int c = 0; c < 64 && c < npb; ++c)
+      if (f[(2 * jt) * npb + c] | f[(2 * jt + 1) * npb + c]) live |= 1ull << c;
+    mskA[(long long)sgi * njt + jt] = live;
   }
 }
 
@@ -1320,20 +1383,34 @@ static int ensure_table(const shtb_plan* cp, cudaStream_t st) {
   p->npp = (p->npair + kM - 1) / kM * kM;
   const long long rows = table_segments(p, &p->htab_seg);
   const size_t tb = (size_t)rows * p->npp * 4;   // one image
+  long long rmax = 0;
+  for (int s = 0; s < 2 * nm; ++s) rmax = std::max(rmax, p->htab_seg[s + 1] - p->htab_seg[s]);
+  const int njt = (int)((rmax + kM - 1) / kM), nrb = 2 * njt + 1, npb = p->npp / 64;
+  const size_t nzbytes = (size_t)2 * nm * nrb * npb;
+  const size_t segoff = (2 * tb + 255) / 256 * 256, nzoff = (segoff + (2 * nm + 1) * 8 + 255) / 256 * 256;
+  const size_t msoff = (nzoff + nzbytes + 255) / 256 * 256, ntp = p->npp / kM;
+  const size_t maoff = msoff + (size_t)2 * nm * ntp * 8, mend = maoff + (size_t)2 * nm * njt * 8;
   void* mem = nullptr;
-  cudaError_t e = cudaMalloc(&mem, 2 * tb + (2 * nm + 1) * 8 + 256);
+  cudaError_t e = cudaMalloc(&mem, mend);
   if (e != cudaSuccess) return set_error(SHTB_ERR_OOM, std::string("mixed table: ") + cudaGetErrorString(e));
   float* tab = (float*)mem;
   float* taba = (float*)((char*)mem + tb);
-  long long* dseg = (long long*)((char*)mem + (2 * tb + 255) / 256 * 256);
+  long long* dseg = (long long*)((char*)mem + segoff);
+  unsigned char* dnz = (unsigned char*)mem + nzoff;
   e = cudaMemcpyAsync(dseg, p->htab_seg.data(), (2 * nm + 1) * 8, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(tab, 0, 2 * tb, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(dnz, 0, nzbytes, st);
   if (e != cudaSuccess) {
     cudaFree(mem);
     return set_error(SHTB_ERR_CUDA, std::string("mixed table init: ") + cudaGetErrorString(e));
   }
   dim3 grid((p->npair + 127) / 128, nm);
-  mixed_table_kernel<<<grid, 128, 0, st>>>(p->dev, tab, taba, dseg, p->npp);
+  mixed_table_kernel<<<grid, 128, 0, st>>>(p->dev, tab, taba, dseg, p->npp, dnz, nrb, npb);
+  count_launch();
+  unsigned long long* msk_s = (unsigned long long*)((char*)mem + msoff);
+  unsigned long long* msk_a = (unsigned long long*)((char*)mem + maoff);
+  const int nmask = 2 * nm * (int)(ntp + njt);
+  mixed_mask_kernel<<<(nmask + 127) / 128, 128, 0, st>>>(dnz, 2 * nm, nrb, npb, njt, msk_s, msk_a);
   count_launch();
   e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -1344,7 +1421,18 @@ static int ensure_table(const shtb_plan* cp, cudaStream_t st) {
   p->d_tab = tab;
   p->d_tab_ana = taba;
   p->d_tab_seg = dseg;
-  p->tab_bytes = 2 * tb;
+  p->hmsk_s.resize((size_t)2 * nm * ntp);
+  p->hmsk_a.resize((size_t)2 * nm * njt);
+  e = cudaMemcpy(p->hmsk_s.data(), msk_s, p->hmsk_s.size() * 8, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(p->hmsk_a.data(), msk_a, p->hmsk_a.size() * 8, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) {
+    cudaFree(mem);
+    return set_error(SHTB_ERR_CUDA, std::string("mixed table masks: ") + cudaGetErrorString(e));
+  }
+  p->d_tab_msk_s = msk_s;
+  p->d_tab_msk_a = msk_a;
+  p->tab_njt = njt;
+  p->tab_bytes = mend;
   return SHTB_OK;
 }
 
@@ -1357,26 +1445,25 @@ static int sm_count() {
 
 // ntiles tiles per block of N/2 fields; persistent CTAs, at most the resident number.
 template <int MODE, int N>
-static int launch_gemm(const shtb_plan* p, const Args& a, int ntiles, int nz, int ntp, cudaStream_t st) {
+static int launch_gemm(const shtb_plan* p, const Args& a, int ntiles, int nz, cudaStream_t st) {
   auto kern = mixed_gemm_kernel<MODE, N>;
   const int smem = Smem<N>::kBytes;
   SHTB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "mixed smem attr");
   const int total = ntiles * nz;
   const int grid = std::max(1, std::min(total, sm_count() * kCtasPerSm<N>));
   prof_begin(st);
-  kern<<<grid, kThreads<N>, smem, st>>>(a, total, nz, ntp);
+  kern<<<grid, kThreads<N>, smem, st>>>(a, total, nz);
   SHTB_LAUNCHED(MODE == 0 ? "tc gemm synthesis kernel" : "tc gemm analysis kernel");
   return SHTB_OK;
 }
 
-// ntiles: tiles per block of fields (synthesis: orders x pair tiles x 2, analysis:
-// degree tiles x 2); ntp: pair tiles per order (synthesis).
+// ntiles: tiles per block of fields (tile list length x 2 parities).
 template <int MODE>
-static int dispatch_gemm(const shtb_plan* p, const Args& a, int nf, int ntiles, int ntp, cudaStream_t st) {
-  if (nf > 32) return launch_gemm<MODE, 128>(p, a, ntiles, (nf + 63) / 64, ntp, st);
-  if (nf > 16) return launch_gemm<MODE, 64>(p, a, ntiles, 1, ntp, st);
-  if (nf > 8) return launch_gemm<MODE, 32>(p, a, ntiles, 1, ntp, st);
-  return launch_gemm<MODE, 16>(p, a, ntiles, 1, ntp, st);
+static int dispatch_gemm(const shtb_plan* p, const Args& a, int nf, int ntiles, cudaStream_t st) {
+  if (nf > 32) return launch_gemm<MODE, 128>(p, a, ntiles, (nf + 63) / 64, st);
+  if (nf > 16) return launch_gemm<MODE, 64>(p, a, ntiles, 1, st);
+  if (nf > 8) return launch_gemm<MODE, 32>(p, a, ntiles, 1, st);
+  return launch_gemm<MODE, 16>(p, a, ntiles, 1, st);
 }
 
 // Clears whole order columns the analysis GEMM does not visit (m not a multiple of
@@ -1394,6 +1481,9 @@ static Args base_args(const shtb_plan* p) {
   a.tab = p->d_tab;
   a.seg = p->d_tab_seg;
   a.npp = p->npp;
+  a.mskS = p->d_tab_msk_s;
+  a.mskA = p->d_tab_msk_a;
+  a.njt = p->tab_njt;
   a.ld_k = (long long)(p->lmax + 1) * (p->mmax + 1);
   a.sc = p->d_scale;
   a.err = p->d_err;
@@ -1401,6 +1491,62 @@ static Args base_args(const shtb_plan* p) {
   a.wait_ns = p->dbg_wait_ns ? p->dbg_wait_ns : kWaitNs;
   a.skip_chunk = p->dbg_skip_chunk;
   return a;
+}
+
+// GEMM tile list of one direction for truncation degree ltr, cached on the plan: synthesis
+// (im, first pair), analysis (im, first degree row), ordered by decreasing count of live
+// chunks over both parities (the persistent CTAs take tiles blockIdx.x, + gridDim.x, ...,
+// so every round holds tiles of similar cost).
+static int gemm_tiles_list(const shtb_plan* cp, int mode, int ltr, int mlim, cudaStream_t st, int* count) {
+  shtb_plan* p = const_cast<shtb_plan*>(cp);
+  std::vector<int2>& tl = mode ? p->hmx_tiles : p->hmx_stiles;
+  int& key = mode ? p->mx_tiles_key : p->mx_stiles_key;
+  int2*& dev = mode ? p->d_mx_tiles : p->d_mx_stiles;
+  if (key != ltr) {
+    tl.clear();
+    std::vector<int> cost;
+    const int ntp = p->npp / kM, njt = p->tab_njt;
+    auto live = [](unsigned long long msk, int nall) {
+      return __builtin_popcountll(nall >= 64 ? msk : msk & ((1ull << nall) - 1)) + std::max(nall - 64, 0);
+    };
+    for (int im = 0; im * p->mres <= mlim; ++im) {
+      const int m = im * p->mres;
+      if (mode == 0) {
+        for (int pt = 0; pt * kM < p->npair; ++pt) {
+          int c = 0;
+          for (int par = 0; par < 2; ++par) {
+            const int J = (ltr >= m + par) ? (ltr - m - par) / 2 + 1 : 0;
+            c += live(p->hmsk_s[(size_t)(2 * im + par) * ntp + pt], ((J + kK - 1) / kK + kChunk - 1) / kChunk);
+          }
+          tl.push_back(make_int2(im, pt * kM));
+          cost.push_back(c);
+        }
+      } else {
+        const int JE = (ltr - m) / 2 + 1;
+        const int nall = ((p->npair + kK - 1) / kK + kChunk - 1) / kChunk;
+        for (int j0 = 0; j0 < JE; j0 += kM) {
+          int c = 0;
+          for (int par = 0; par < 2; ++par) c += live(p->hmsk_a[(size_t)(2 * im + par) * njt + j0 / kM], nall);
+          tl.push_back(make_int2(im, j0));
+          cost.push_back(c);
+        }
+      }
+    }
+    std::vector<int> ord(tl.size());
+    for (size_t i = 0; i < ord.size(); ++i) ord[i] = (int)i;
+    std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return cost[x] > cost[y]; });
+    std::vector<int2> sorted(tl.size());
+    for (size_t i = 0; i < ord.size(); ++i) sorted[i] = tl[ord[i]];
+    tl.swap(sorted);
+    if (dev) cudaFree(dev);
+    dev = nullptr;
+    SHTB_TRY_CUDA(cudaMalloc(&dev, tl.size() * sizeof(int2)), "mixed tiles");
+    SHTB_TRY_CUDA(cudaMemcpyAsync(dev, tl.data(), tl.size() * sizeof(int2), cudaMemcpyHostToDevice, st),
+                  "mixed tiles upload");
+    key = ltr;
+  }
+  *count = (int)tl.size();
+  return SHTB_OK;
 }
 
 int mixed_synthesis(const shtb_plan* p, const void* alm, void* f, int nf, int ltr, void* work, cudaStream_t st,
@@ -1428,8 +1574,10 @@ int mixed_synthesis(const shtb_plan* p, const void* alm, void* f, int nf, int lt
   prof_begin(st);
   mixed_pack_kernel<<<dim3(mlim / p->mres + 1, (nf + kPackFields - 1) / kPackFields), kPackThreads, 0, st>>>(a);
   SHTB_LAUNCHED("tc gemm B packing kernel");
-  const int ntp = (p->npair + kM - 1) / kM;
-  if ((rc = dispatch_gemm<0>(p, a, nf, 2 * ntp * (mlim / p->mres + 1), ntp, st))) return rc;
+  int ntl = 0;
+  if ((rc = gemm_tiles_list(p, 0, ltr, mlim, st, &ntl))) return rc;
+  a.tiles = p->d_mx_stiles;
+  if ((rc = dispatch_gemm<0>(p, a, nf, 2 * ntl, st))) return rc;
   return launch_fft_syn<float, float>(p, work, (float*)f, nullptr, 1, nf, mlim, p->phi_inv_scale / p->nlon, 0, 0, st);
 }
 
@@ -1449,23 +1597,8 @@ int mixed_analysis(const shtb_plan* p, const void* f, void* alm, int nf, int ltr
   if ((rc = launch_fft_ana<float, float>(p, (const float*)f, nullptr, 1, work, nf, mlim, p->ana_scale, 1, 0, st, 1)))
     return rc;
   // analysis tiles: 128 degrees of each parity per tile
-  std::vector<int2>& tl = const_cast<shtb_plan*>(p)->hmx_tiles;
-  const int key = ltr;
-  if (p->mx_tiles_key != key) {
-    tl.clear();
-    for (int im = 0; im * p->mres <= mlim; ++im) {
-      const int m = im * p->mres;
-      const int JE = (ltr - m) / 2 + 1;
-      for (int j0 = 0; j0 < JE; j0 += kM) tl.push_back(make_int2(im, j0));
-    }
-    shtb_plan* pm = const_cast<shtb_plan*>(p);
-    if (pm->d_mx_tiles) cudaFree(pm->d_mx_tiles);
-    pm->d_mx_tiles = nullptr;
-    SHTB_TRY_CUDA(cudaMalloc(&pm->d_mx_tiles, tl.size() * sizeof(int2)), "mixed tiles");
-    SHTB_TRY_CUDA(cudaMemcpyAsync(pm->d_mx_tiles, tl.data(), tl.size() * sizeof(int2), cudaMemcpyHostToDevice, st),
-                  "mixed tiles upload");
-    pm->mx_tiles_key = key;
-  }
+  int ntl = 0;
+  if ((rc = gemm_tiles_list(p, 1, ltr, mlim, st, &ntl))) return rc;
   Args a = base_args(p);
   a.tab = p->d_tab_ana;
   a.bimg = (float*)work;
@@ -1479,7 +1612,7 @@ int mixed_analysis(const shtb_plan* p, const void* f, void* alm, int nf, int ltr
     a.cpacked = 1;
     a.ld_k = nlm;
   }
-  if ((rc = dispatch_gemm<1>(p, a, nf, 2 * (int)tl.size(), 0, st))) return rc;
+  if ((rc = dispatch_gemm<1>(p, a, nf, 2 * ntl, st))) return rc;
   if (!packed && (p->mres > 1 || mlim < p->mmax)) {
     dim3 zg(p->mmax + 1, nf);
     prof_begin(st);

@@ -468,6 +468,7 @@ extern "C" int shtb_plan_destroy(shtb_plan* p) {
   cudaError_t e = cudaFree(p->dmem);
   if (p->d_tab) cudaFree(p->d_tab);
   if (p->d_mx_tiles) cudaFree(p->d_mx_tiles);
+  if (p->d_mx_stiles) cudaFree(p->d_mx_stiles);
   if (dev >= 0 && dev != p->device) cudaSetDevice(dev);
   delete p;
   return check_cuda(e, "plan destroy");
