@@ -164,4 +164,6 @@ struct shtb_plan {
   int mx_tiles_key = -1, mx_stiles_key = -1;
   int2* d_mx_tiles = nullptr;
   int2* d_mx_stiles = nullptr;
+  unsigned long long* d_mx_tmask = nullptr;    // live-chunk masks of the lists' entries
+  unsigned long long* d_mx_stmask = nullptr;
 };

@@ -74,12 +74,9 @@ struct Args {
   const float* tab;          // tile images of this direction (synthesis or analysis)
   const long long* seg;      // [2*nm+1] first table row of segment (im, parity); rows hold npp pairs
   int npp;
-  // live-chunk masks of the tiles (bit c: chunk c's A image has a nonzero value; chunks
-  // from 64 on always run), or null (every chunk runs): synthesis [2 nm][npp / 128] by pair
-  // tile, analysis [2 nm][njt] by degree tile
-  const unsigned long long* mskS;
-  const unsigned long long* mskA;
-  int njt;
+  // live-chunk masks of the tile list's entries ([entry][parity]; bit c: chunk c's A image
+  // has a nonzero value; chunks from 64 on always run), or null (every chunk runs)
+  const unsigned long long* tmask;
   const float2* cin;         // synthesis: coefficients (input of the B packing)
   float* bimg;               // B tile images: synthesis f16 hi/lo pairs written by the packing,
                              //   analysis FP32 written by the FFT (converted in shared memory)
@@ -403,14 +400,6 @@ struct TileInfo {
 };
 
 __device__ __forceinline__ bool chunk_live(const TileInfo& T, int c) { return c >= 64 || ((T.live >> c) & 1ull); }
-
-// The live-chunk mask of a tile (all ones without masks).
-template <int MODE>
-__device__ __forceinline__ unsigned long long tile_live(const Args& a, const TileCoord& tc) {
-  if (MODE == 0)
-    return a.mskS ? a.mskS[(long long)(2 * tc.im + tc.par) * (a.npp / kM) + tc.p0 / kM] : ~0ull;
-  return a.mskA ? a.mskA[(long long)(2 * tc.im + tc.par) * a.njt + tc.j0 / kM] : ~0ull;
-}
 
 template <int MODE>
 __device__ __forceinline__ TileInfo tile_info(const Args& a, const TileCoord& tc, unsigned long long live) {
@@ -832,9 +821,13 @@ __device__ __forceinline__ void gemm_tiles(const Src& src, unsigned char* sm, co
   int committed = -1;    // MMA issuer: last chunk committed
   int skip = -1;
   int i = blockIdx.x;
+  TileCoord tc_next{};
   unsigned long long live_next = ~0ull;
   if constexpr (!Src::kDynamic) {
-    if (i < src.n) live_next = tile_live<MODE>(src.args(i), src.coord(i));
+    if (i < src.n) {
+      tc_next = src.coord(i);
+      live_next = src.live(i);
+    }
   }
   for (unsigned t = 0; role; ++t) {
     if constexpr (Src::kDynamic) {
@@ -862,13 +855,20 @@ __device__ __forceinline__ void gemm_tiles(const Src& src, unsigned char* sm, co
       if (i >= src.n) break;
     }
     const Args& a = src.args(i);
-    const TileCoord tc = src.coord(i);
+    TileCoord tc;
     unsigned long long live = ~0ull;
     if constexpr (!Src::kDynamic) {
-      // this tile's mask was loaded one tile ahead; start the next tile's load now
+      // this tile's list entry and mask were loaded one tile ahead; start the next tile's
+      // loads now, so no role waits for them at a tile boundary
+      tc = tc_next;
       live = live_next;
       const int in = i + (int)gridDim.x;
-      if (in < src.n) live_next = tile_live<MODE>(src.args(in), src.coord(in));
+      if (in < src.n) {
+        tc_next = src.coord(in);
+        live_next = src.live(in);
+      }
+    } else {
+      tc = src.coord(i);
     }
     const TileInfo T = tile_info<MODE>(a, tc, live);
     if (blockIdx.x == 0) skip = a.skip_chunk;
@@ -1177,6 +1177,7 @@ struct SingleSrc {
   int n, nz;
   __device__ const Args& args(int) const { return a; }
   __device__ void tile_done(int) const {}
+  __device__ unsigned long long live(int i) const { return a.tmask ? a.tmask[((i >> 1) / nz) * 2 + (i & 1)] : ~0ull; }
   __device__ TileCoord coord(int i) const {
     TileCoord tc;
     tc.par = i & 1;
@@ -1481,9 +1482,7 @@ static Args base_args(const shtb_plan* p) {
   a.tab = p->d_tab;
   a.seg = p->d_tab_seg;
   a.npp = p->npp;
-  a.mskS = p->d_tab_msk_s;
-  a.mskA = p->d_tab_msk_a;
-  a.njt = p->tab_njt;
+
   a.ld_k = (long long)(p->lmax + 1) * (p->mmax + 1);
   a.sc = p->d_scale;
   a.err = p->d_err;
@@ -1502,9 +1501,11 @@ static int gemm_tiles_list(const shtb_plan* cp, int mode, int ltr, int mlim, cud
   std::vector<int2>& tl = mode ? p->hmx_tiles : p->hmx_stiles;
   int& key = mode ? p->mx_tiles_key : p->mx_stiles_key;
   int2*& dev = mode ? p->d_mx_tiles : p->d_mx_stiles;
+  unsigned long long*& dmask = mode ? p->d_mx_tmask : p->d_mx_stmask;
   if (key != ltr) {
     tl.clear();
     std::vector<int> cost;
+    std::vector<unsigned long long> msk;   // [entry][parity]
     const int ntp = p->npp / kM, njt = p->tab_njt;
     auto live = [](unsigned long long msk, int nall) {
       return __builtin_popcountll(nall >= 64 ? msk : msk & ((1ull << nall) - 1)) + std::max(nall - 64, 0);
@@ -1516,7 +1517,9 @@ static int gemm_tiles_list(const shtb_plan* cp, int mode, int ltr, int mlim, cud
           int c = 0;
           for (int par = 0; par < 2; ++par) {
             const int J = (ltr >= m + par) ? (ltr - m - par) / 2 + 1 : 0;
-            c += live(p->hmsk_s[(size_t)(2 * im + par) * ntp + pt], ((J + kK - 1) / kK + kChunk - 1) / kChunk);
+            const unsigned long long mk = p->hmsk_s[(size_t)(2 * im + par) * ntp + pt];
+            c += live(mk, ((J + kK - 1) / kK + kChunk - 1) / kChunk);
+            msk.push_back(mk);
           }
           tl.push_back(make_int2(im, pt * kM));
           cost.push_back(c);
@@ -1526,7 +1529,11 @@ static int gemm_tiles_list(const shtb_plan* cp, int mode, int ltr, int mlim, cud
         const int nall = ((p->npair + kK - 1) / kK + kChunk - 1) / kChunk;
         for (int j0 = 0; j0 < JE; j0 += kM) {
           int c = 0;
-          for (int par = 0; par < 2; ++par) c += live(p->hmsk_a[(size_t)(2 * im + par) * njt + j0 / kM], nall);
+          for (int par = 0; par < 2; ++par) {
+            const unsigned long long mk = p->hmsk_a[(size_t)(2 * im + par) * njt + j0 / kM];
+            c += live(mk, nall);
+            msk.push_back(mk);
+          }
           tl.push_back(make_int2(im, j0));
           cost.push_back(c);
         }
@@ -1536,13 +1543,25 @@ static int gemm_tiles_list(const shtb_plan* cp, int mode, int ltr, int mlim, cud
     for (size_t i = 0; i < ord.size(); ++i) ord[i] = (int)i;
     std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return cost[x] > cost[y]; });
     std::vector<int2> sorted(tl.size());
-    for (size_t i = 0; i < ord.size(); ++i) sorted[i] = tl[ord[i]];
+    std::vector<unsigned long long> smsk(msk.size());
+    for (size_t i = 0; i < ord.size(); ++i) {
+      sorted[i] = tl[ord[i]];
+      smsk[2 * i] = msk[2 * ord[i]];
+      smsk[2 * i + 1] = msk[2 * ord[i] + 1];
+    }
     tl.swap(sorted);
     if (dev) cudaFree(dev);
+    if (dmask) cudaFree(dmask);
     dev = nullptr;
+    dmask = nullptr;
+    key = -1;
     SHTB_TRY_CUDA(cudaMalloc(&dev, tl.size() * sizeof(int2)), "mixed tiles");
+    SHTB_TRY_CUDA(cudaMalloc(&dmask, smsk.size() * 8), "mixed tile masks");
     SHTB_TRY_CUDA(cudaMemcpyAsync(dev, tl.data(), tl.size() * sizeof(int2), cudaMemcpyHostToDevice, st),
                   "mixed tiles upload");
+    // pageable source: the copy is complete when the call returns
+    SHTB_TRY_CUDA(cudaMemcpyAsync(dmask, smsk.data(), smsk.size() * 8, cudaMemcpyHostToDevice, st),
+                  "mixed tile masks upload");
     key = ltr;
   }
   *count = (int)tl.size();
@@ -1577,6 +1596,7 @@ int mixed_synthesis(const shtb_plan* p, const void* alm, void* f, int nf, int lt
   int ntl = 0;
   if ((rc = gemm_tiles_list(p, 0, ltr, mlim, st, &ntl))) return rc;
   a.tiles = p->d_mx_stiles;
+  a.tmask = p->d_mx_stmask;
   if ((rc = dispatch_gemm<0>(p, a, nf, 2 * ntl, st))) return rc;
   return launch_fft_syn<float, float>(p, work, (float*)f, nullptr, 1, nf, mlim, p->phi_inv_scale / p->nlon, 0, 0, st);
 }
@@ -1608,6 +1628,7 @@ int mixed_analysis(const shtb_plan* p, const void* f, void* alm, int nf, int ltr
   a.lend = ltr;
   a.lcap = ltr;
   a.tiles = p->d_mx_tiles;
+  a.tmask = p->d_mx_tmask;
   if (packed) {
     a.cpacked = 1;
     a.ld_k = nlm;
