@@ -73,6 +73,7 @@ struct shtb_group {
   unsigned long long *d_done = nullptr, *d_t0 = nullptr;
   int* d_queue = nullptr;               // work counters (kGroupQueues)
   int4 *d_items_syn = nullptr, *d_items_ana = nullptr;
+  unsigned long long *d_masks_syn = nullptr, *d_masks_ana = nullptr;   // live-chunk mask per GEMM item
   int2* d_items_pack = nullptr;
   int n_syn = 0, n_ana = 0, n_pack = 0;
   unsigned char* d_w = nullptr;
@@ -190,7 +191,7 @@ static int group_synthesis_stage(shtb_group* g, int* q, cudaStream_t st) {
     return rc;
   if ((rc = launch_pack_group(g->d_args_syn, g->d_items_pack, g->n_pack, std::min(g->n_pack, 24 * g->nsm), q, st)))
     return rc;
-  if ((rc = launch_gemm_group(0, g->d_args_syn, g->d_items_syn, g->n_syn, g->gemm_ctas_syn, nullptr, q + 1, st)))
+  if ((rc = launch_gemm_group(0, g->d_args_syn, g->d_items_syn, g->d_masks_syn, g->n_syn, g->gemm_ctas_syn, nullptr, q + 1, st)))
     return rc;
   if (fork) {
     SHTB_TRY_CUDA(cudaEventRecord(g->ev_join, g->aux), "group join");
@@ -212,7 +213,7 @@ static int group_launch_stages(shtb_group* g, int op, cudaStream_t st) {
   }
   if (op != SHTB_OP_SYNTHESIS) {
     if ((rc = group_fft_stage(g, 0, q + 3, q + 6, st))) return rc;
-    if ((rc = launch_gemm_group(1, g->d_args_ana, g->d_items_ana, g->n_ana, g->gemm_ctas_ana, g->d_done, q + 4, st)))
+    if ((rc = launch_gemm_group(1, g->d_args_ana, g->d_items_ana, g->d_masks_ana, g->n_ana, g->gemm_ctas_ana, g->d_done, q + 4, st)))
       return rc;
   }
   return SHTB_OK;
@@ -282,9 +283,10 @@ extern "C" int shtb_group_create(shtb_group** out, const shtb_plan* const* plans
   }
   g->n_fft2 = (int)f2items.size();
   g->fft2_ctas = std::max(1, std::min(g->nsm, g->n_fft2));
-  // GEMM tiles, most K-steps first
+  // GEMM tiles with their live-chunk masks, most live K-steps first
   const int TM = mixed_group_tile_rows();
   std::vector<int4> syn, ana;
+  std::vector<unsigned long long> msyn, mana;
   std::vector<int> csyn, cana;
   // FP64-pipe synthesis items of the one- and two-field members, most work first
   std::vector<int4> ssyn;
@@ -306,13 +308,17 @@ extern "C" int shtb_group_create(shtb_group** out, const shtb_plan* const* plans
     for (int im = 0; im <= mlim; ++im) {
       for (int par = 0; par < 2; ++par) {
         for (int p0 = 0; !g->simt[t] && p0 < p->npair; p0 += TM) {
+          int c = 0;
+          msyn.push_back(mixed_group_tile(p, 0, im, p0, par, &c));
           syn.push_back(make_int4(t, im, p0, par));
-          csyn.push_back(mixed_group_ksteps(p, 0, im, par));
+          csyn.push_back(c);
         }
         const int JE = (p->lmax - im) / 2 + 1;
         for (int j0 = 0; j0 < JE; j0 += TM) {
+          int c = 0;
+          mana.push_back(mixed_group_tile(p, 1, im, j0, par, &c));
           ana.push_back(make_int4(t, im, j0, par));
-          cana.push_back(mixed_group_ksteps(p, 1, im, par));
+          cana.push_back(c);
         }
       }
     }
@@ -325,8 +331,21 @@ extern "C" int shtb_group_create(shtb_group** out, const shtb_plan* const* plans
     for (size_t i = 0; i < ord.size(); ++i) s[i] = it[ord[i]];
     it.swap(s);
   };
-  sort_items(syn, csyn);
-  sort_items(ana, cana);
+  auto sort_masked = [](std::vector<int4>& it, std::vector<unsigned long long>& mk, const std::vector<int>& cost) {
+    std::vector<int> ord(it.size());
+    std::iota(ord.begin(), ord.end(), 0);
+    std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    std::vector<int4> s(it.size());
+    std::vector<unsigned long long> sm(mk.size());
+    for (size_t i = 0; i < ord.size(); ++i) {
+      s[i] = it[ord[i]];
+      sm[i] = mk[ord[i]];
+    }
+    it.swap(s);
+    mk.swap(sm);
+  };
+  sort_masked(syn, msyn, csyn);
+  sort_masked(ana, mana, cana);
   sort_items(ssyn, cssyn);
   std::vector<int2> pack;   // (member, order) for the synthesis B packing, most degrees first
   {
@@ -360,7 +379,8 @@ extern "C" int shtb_group_create(shtb_group** out, const shtb_plan* const* plans
                o_i2 = take(std::max<size_t>(1, f2items.size()) * sizeof(int4));
   const size_t o_done = take(n * 8), o_t0 = take(8), o_q = take(kGroupQueues * sizeof(int)),
                o_is = take(syn.size() * sizeof(int4)),
-               o_ia = take(ana.size() * sizeof(int4)), o_ip = take(pack.size() * sizeof(int2));
+               o_ia = take(ana.size() * sizeof(int4)), o_ip = take(pack.size() * sizeof(int2)),
+               o_ms = take(msyn.size() * 8), o_ma = take(mana.size() * 8);
   const size_t o_sas = take(n * g->sargsz), o_iss = take(ssyn.size() * sizeof(int4));
   g->woff.resize(n);
   size_t wbytes = 0;
@@ -384,12 +404,16 @@ extern "C" int shtb_group_create(shtb_group** out, const shtb_plan* const* plans
   g->d_queue = (int*)(g->dmem + o_q);
   g->d_items_syn = (int4*)(g->dmem + o_is);
   g->d_items_ana = (int4*)(g->dmem + o_ia);
+  g->d_masks_syn = (unsigned long long*)(g->dmem + o_ms);
+  g->d_masks_ana = (unsigned long long*)(g->dmem + o_ma);
   g->d_items_pack = (int2*)(g->dmem + o_ip);
   g->d_sargs = g->dmem + o_sas;
   g->d_items_ssyn = (int4*)(g->dmem + o_iss);
   g->d_w = g->dmem + o_w;
   e = cudaMemcpy(g->d_items_syn, syn.data(), syn.size() * sizeof(int4), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(g->d_items_ana, ana.data(), ana.size() * sizeof(int4), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && !msyn.empty()) e = cudaMemcpy(g->d_masks_syn, msyn.data(), msyn.size() * 8, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && !mana.empty()) e = cudaMemcpy(g->d_masks_ana, mana.data(), mana.size() * 8, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(g->d_items_pack, pack.data(), pack.size() * sizeof(int2), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(g->d_items_ssyn, ssyn.data(), ssyn.size() * sizeof(int4), cudaMemcpyHostToDevice);
   if (e == cudaSuccess && !f2items.empty())

@@ -73,10 +73,12 @@ size_t mixed_workspace_bytes(const shtb_plan* p, int op, int nf);
 int mixed_prepare(const shtb_plan* p, cudaStream_t st);
 size_t mixed_args_bytes();
 void mixed_fill_args(const shtb_plan* p, int mode, const void* in, void* out, int nf, void* host_args);
-int mixed_group_ksteps(const shtb_plan* p, int mode, int im, int par);
+// Live-chunk mask of GEMM tile (mode, im, first pair or degree row t0, par) of a prepared
+// plan, with the K-steps its live chunks hold (the tile's cost).
+unsigned long long mixed_group_tile(const shtb_plan* p, int mode, int im, int t0, int par, int* ksteps);
 int mixed_group_tile_rows();
-int launch_gemm_group(int mode, const void* targs, const int4* items, int nitems, int grid, unsigned long long* done,
-                      int* queue, cudaStream_t st);
+int launch_gemm_group(int mode, const void* targs, const int4* items, const unsigned long long* masks, int nitems,
+                      int grid, unsigned long long* done, int* queue, cudaStream_t st);
 int launch_pack_group(const void* targs, const int2* items, int nitems, int grid, int* queue, cudaStream_t st);
 size_t fft_job_bytes_f32();
 void fft_fill_job_f32(const shtb_plan* p, int syn, const void* W, void* grid, int nf, void* host_job);

@@ -869,6 +869,7 @@ __device__ __forceinline__ void gemm_tiles(const Src& src, unsigned char* sm, co
       }
     } else {
       tc = src.coord(i);
+      live = src.live(i);
     }
     const TileInfo T = tile_info<MODE>(a, tc, live);
     if (blockIdx.x == 0) skip = a.skip_chunk;
@@ -1212,11 +1213,13 @@ struct GroupSrc {
   static constexpr bool kDynamic = true;
   const Args* targs;
   const int4* items;
+  const unsigned long long* masks;   // live-chunk mask of each item, or null
   int n;
   unsigned long long* done;
   int* queue;
   __device__ int* err() const { return targs[0].err; }
   __device__ const Args& args(int i) const { return targs[items[i].x]; }
+  __device__ unsigned long long live(int i) const { return masks ? masks[i] : ~0ull; }
   __device__ TileCoord coord(int i) const {
     const int4 it = items[i];
     TileCoord tc;
@@ -1239,6 +1242,7 @@ struct GroupSrc {
 template <int MODE, int N>
 __global__ void __launch_bounds__(kThreads<N>, kCtasPerSm<N>) mixed_gemm_group_kernel(const Args* __restrict__ targs,
                                                                                    const int4* __restrict__ items,
+                                                                                   const unsigned long long* __restrict__ masks,
                                                                                    int nitems,
                                                                                    unsigned long long* __restrict__ done,
                                                                                    int* __restrict__ queue) {
@@ -1252,7 +1256,7 @@ __global__ void __launch_bounds__(kThreads<N>, kCtasPerSm<N>) mixed_gemm_group_k
     }
   }
   const unsigned tmem = gemm_cta_setup<N>(B);
-  const GroupSrc<MODE> src{targs, items, nitems, done, queue};
+  const GroupSrc<MODE> src{targs, items, masks, nitems, done, queue};
   gemm_tiles<MODE, N>(src, sm, B, tmem);
   gemm_cta_teardown<N>(tmem);
 }
@@ -1672,10 +1676,16 @@ void mixed_fill_args(const shtb_plan* p, int mode, const void* in, void* out, in
   std::memcpy(host_args, &a, sizeof(Args));
 }
 
-int mixed_group_ksteps(const shtb_plan* p, int mode, int im, int par) {
+unsigned long long mixed_group_tile(const shtb_plan* p, int mode, int im, int t0, int par, int* ksteps) {
   const int m = im * p->mres;
   const int J = (p->lmax >= m + par) ? (p->lmax - m - par) / 2 + 1 : 0;
-  return mode == 0 ? (J + kK - 1) / kK : (p->npair + kK - 1) / kK;
+  const int nks = mode == 0 ? (J + kK - 1) / kK : (p->npair + kK - 1) / kK, nall = (nks + kChunk - 1) / kChunk;
+  unsigned long long mk = ~0ull;
+  if (mode == 0 && !p->hmsk_s.empty()) mk = p->hmsk_s[(size_t)(2 * im + par) * (p->npp / kM) + t0 / kM];
+  if (mode == 1 && !p->hmsk_a.empty()) mk = p->hmsk_a[(size_t)(2 * im + par) * p->tab_njt + t0 / kM];
+  const int live = __builtin_popcountll(nall >= 64 ? mk : mk & ((1ull << nall) - 1)) + std::max(nall - 64, 0);
+  *ksteps = std::min(nks, live * kChunk);
+  return mk;
 }
 
 int mixed_group_tile_rows() { return kM; }
@@ -1688,18 +1698,18 @@ int launch_pack_group(const void* targs, const int2* items, int nitems, int grid
   return SHTB_OK;
 }
 
-int launch_gemm_group(int mode, const void* targs, const int4* items, int nitems, int grid, unsigned long long* done,
-                      int* queue, cudaStream_t st) {
+int launch_gemm_group(int mode, const void* targs, const int4* items, const unsigned long long* masks, int nitems,
+                      int grid, unsigned long long* done, int* queue, cudaStream_t st) {
   if (nitems <= 0) return SHTB_OK;
   const int smem = Smem<16>::kBytesQ;
   if (mode == 0) {
     auto kern = mixed_gemm_group_kernel<0, 16>;
     SHTB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "group gemm smem attr");
-    kern<<<grid, kThreads<16>, smem, st>>>((const Args*)targs, items, nitems, done, queue);
+    kern<<<grid, kThreads<16>, smem, st>>>((const Args*)targs, items, masks, nitems, done, queue);
   } else {
     auto kern = mixed_gemm_group_kernel<1, 16>;
     SHTB_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "group gemm smem attr");
-    kern<<<grid, kThreads<16>, smem, st>>>((const Args*)targs, items, nitems, done, queue);
+    kern<<<grid, kThreads<16>, smem, st>>>((const Args*)targs, items, masks, nitems, done, queue);
   }
   count_launch();
   SHTB_TRY_CUDA(cudaGetLastError(), "group gemm launch");
