@@ -75,10 +75,11 @@ __device__ __forceinline__ C2 crot(C2 a) {
 __device__ __forceinline__ C2 cmulc(C2 a, u64 c, u64 s) {
   return C2{fma2(a.im, neg2(s), mul2(a.re, c)), fma2(a.re, s, mul2(a.im, c))};
 }
-// a * w^(DIR < 0 ? 1 : -1) for the table twiddle w = (c, c, s, s) = exp(-2 pi i e / Ns)
+// a * w^(DIR < 0 ? 1 : -1) for the table twiddle w = (c, s) = exp(-2 pi i e / Ns), broadcast
+// to both sequences
 template <int DIR>
-__device__ __forceinline__ C2 ctw(C2 a, float4 w) {
-  const u64 c = pk(make_float2(w.x, w.y)), s = pk(make_float2(w.z, w.w));
+__device__ __forceinline__ C2 ctw(C2 a, float2 w) {
+  const u64 c = pk(make_float2(w.x, w.x)), s = pk(make_float2(w.y, w.y));
   return DIR < 0 ? C2{fma2(a.im, neg2(s), mul2(a.re, c)), fma2(a.re, s, mul2(a.im, c))}
                  : C2{fma2(a.im, s, mul2(a.re, c)), fma2(a.re, neg2(s), mul2(a.im, c))};
 }
@@ -167,7 +168,7 @@ __device__ __forceinline__ void stc(float4* X, int i, C2 c) {
 
 // One in-shared-memory DIF pass of radix R over span S (twiddled unless S == 1).
 template <int HP, int R, int DIR>
-__device__ __forceinline__ void pass_smem(float4* X, int N, int S, const float4* __restrict__ tw) {
+__device__ __forceinline__ void pass_smem(float4* X, int N, int S, const float2* __restrict__ tw) {
   const int ngrp = HP * (N / R);
   for (int gi = threadIdx.x; gi < ngrp; gi += blockDim.x) {
     const int hp = gi % HP, grp = gi / HP;
@@ -186,7 +187,7 @@ __device__ __forceinline__ void pass_smem(float4* X, int N, int S, const float4*
 }
 
 template <int HP, int DIR>
-__device__ __forceinline__ void run_pass(float4* X, int N, int R, int S, const float4* tw) {
+__device__ __forceinline__ void run_pass(float4* X, int N, int R, int S, const float2* tw) {
   switch (R) {
     case 16: pass_smem<HP, 16, DIR>(X, N, S, tw); break;
     case 8: pass_smem<HP, 8, DIR>(X, N, S, tw); break;
@@ -199,7 +200,7 @@ struct Job {
   PlanDev P;
   FFTDesc fd;
   const int* perm;          // rev (analysis) or rinv (synthesis)
-  const float4* tw;         // per-pass twiddles (c, c, s, s), layout of FFTDesc::twoff
+  const float2* tw;         // per-pass twiddles (c, s), layout of FFTDesc::twoff
   const float2* Win;        // synthesis: Fourier buffer
   float* Wout;              // analysis: B tile images of the mixed analysis GEMM
   float* grid;
@@ -211,7 +212,7 @@ struct Job {
 template <int HP, int R0>
 __device__ __forceinline__ void first_from_grid(float4* X, const Job& J, const float* __restrict__ in, int p0) {
   const int N = J.fd.n, S = N / R0, nlat = J.P.nlat, npair = J.P.npair;
-  const float4* tw = J.tw + J.fd.twoff[0];
+  const float2* tw = J.tw + J.fd.twoff[0];
   const int ngrp = HP * S;
   for (int gi = threadIdx.x; gi < ngrp; gi += blockDim.x) {
     const int hp = gi % HP, j = gi / HP;
@@ -480,7 +481,7 @@ bool fft2_applicable(const shtb_plan* p) {
   if (fd.n < 64 || fd.n > 2048 || (fd.n & (fd.n - 1))) return false;
   for (int s = 0; s < fd.nrad; ++s)
     if (!(fd.rad[s] == 2 || fd.rad[s] == 4 || fd.rad[s] == 8 || fd.rad[s] == 16)) return false;
-  return p->d_twp32x4 != nullptr;
+  return p->d_twp32 != nullptr;
 }
 
 static f2::Job fft2_job(const shtb_plan* p, const int* perm, double scale, int nf, int mlim) {
@@ -488,7 +489,7 @@ static f2::Job fft2_job(const shtb_plan* p, const int* perm, double scale, int n
   J.P = p->dev;
   J.fd = p->fft;
   J.perm = perm;
-  J.tw = (const float4*)p->d_twp32x4;
+  J.tw = p->d_twp32;
   J.Win = nullptr;
   J.Wout = nullptr;
   J.grid = nullptr;

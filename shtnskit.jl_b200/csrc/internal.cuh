@@ -134,7 +134,6 @@ struct shtb_plan {
   const int* d_rinv = nullptr;            // natural index stored at FFT position q (inverse of d_rev)
   const double2* d_twp64 = nullptr;       // per-pass twiddles: pass s, factor q (1..r-1), index j < span:
   const float2* d_twp32 = nullptr;        //   entry twoff[s] + (q-1)*span + j = exp(-2 pi i j q / Ns)
-  const float4* d_twp32x4 = nullptr;      // the same as (re, re, im, im) for the packed-pair FFTs
   const double* d_dcoef = nullptr;        // packed d(l,m) = sqrt((l^2-m^2)/(4l^2-1)), l in [m, lrec]
   int* d_err = nullptr;                   // device status word (bounded waits that gave up)
   // device address of the allocation-free synthesis's static scratch array on this

@@ -359,8 +359,6 @@ extern "C" int shtb_plan_create(shtb_plan** out, int lmax, int mmax, int mres, i
   const int ntwp = fft_pass_twiddles(p->fft, twp);
   std::vector<float2> twp32(ntwp);
   for (int t = 0; t < ntwp; ++t) twp32[t] = make_float2((float)twp[t].x, (float)twp[t].y);
-  std::vector<float4> twp32x4(ntwp);
-  for (int t = 0; t < ntwp; ++t) twp32x4[t] = make_float4(twp32[t].x, twp32[t].x, twp32[t].y, twp32[t].y);
 
   // one device allocation for all tables
   size_t o = 0;
@@ -373,7 +371,7 @@ extern "C" int shtb_plan_create(shtb_plan** out, int lmax, int mmax, int mres, i
   const size_t o_scale = coeff_scale ? take((size_t)(lmax + 1) * (mmax + 1) * 8) : 0;
   const size_t o_tw = take((size_t)nlon * 16), o_tw32 = take((size_t)nlon * 8);
   const size_t o_seed = take((mmax + 2) * 8), o_rev = take((size_t)nlon * 4), o_rinv = take((size_t)nlon * 4);
-  const size_t o_twp = take((size_t)ntwp * 16), o_twp32 = take((size_t)ntwp * 8), o_twp32x4 = take((size_t)ntwp * 16);
+  const size_t o_twp = take((size_t)ntwp * 16), o_twp32 = take((size_t)ntwp * 8);
   const size_t o_err = take(16);
   p->dbytes = o;
   cudaError_t ce = cudaMalloc(&p->dmem, o);
@@ -403,7 +401,6 @@ extern "C" int shtb_plan_create(shtb_plan** out, int lmax, int mmax, int mres, i
   if (ce == cudaSuccess) ce = up(o_rinv, rinv.data(), (size_t)nlon * 4);
   if (ce == cudaSuccess) ce = up(o_twp, twp.data(), (size_t)ntwp * 16);
   if (ce == cudaSuccess) ce = up(o_twp32, twp32.data(), (size_t)ntwp * 8);
-  if (ce == cudaSuccess) ce = up(o_twp32x4, twp32x4.data(), (size_t)ntwp * 16);
   if (ce != cudaSuccess) {
     cudaFree(p->dmem);
     delete p;
@@ -433,7 +430,6 @@ extern "C" int shtb_plan_create(shtb_plan** out, int lmax, int mmax, int mres, i
   p->d_rinv = (const int*)(D + o_rinv);
   p->d_twp64 = (const double2*)(D + o_twp);
   p->d_twp32 = (const float2*)(D + o_twp32);
-  p->d_twp32x4 = (const float4*)(D + o_twp32x4);
   p->d_err = (int*)(D + o_err);
   if (ce == cudaSuccess) ce = cudaMemset(D + o_err, 0, 16);
 
