@@ -209,6 +209,14 @@ struct Job {
 };
 
 // ------------------------------------------------------------------------------ analysis
+// Fourier-buffer loads of the synthesis (read once) that leave no line in L1, which keeps the
+// twiddle and permutation tables there (FFT synthesis 0.409 -> 0.398 ms at nlon 2048 x 64
+// fields). The analysis's 8-byte grid loads are faster with L1 allocation (0.430 vs 0.588 ms).
+__device__ __forceinline__ float4 ld_once4(const float2* p) {
+  float4 v;
+  asm("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p));
+  return v;
+}
 template <int HP, int R0>
 __device__ __forceinline__ void first_from_grid(float4* X, const Job& J, const float* __restrict__ in, int p0) {
   const int N = J.fd.n, S = N / R0, nlat = J.P.nlat, npair = J.P.npair;
@@ -392,8 +400,8 @@ __device__ __forceinline__ void syn_body(const Job& J, int k, int p0, float4* X,
         const int pa = p0 + 2 * hp;
         const size_t base = ((size_t)k * P.nm + im) * 2 * npair + pa;
         if (pa + 1 < npair) {
-          ev[u] = *reinterpret_cast<const float4*>(J.Win + base);
-          ov[u] = *reinterpret_cast<const float4*>(J.Win + base + npair);
+          ev[u] = ld_once4(J.Win + base);
+          ov[u] = ld_once4(J.Win + base + npair);
         } else if (pa < npair) {
           const float2 e = J.Win[base], o = J.Win[base + npair];
           ev[u].x = e.x; ev[u].y = e.y;
