@@ -141,6 +141,19 @@ __device__ __forceinline__ void dif_last_to_grid(const V* X, int S, int N, T* __
 }
 
 // Latitude pairs p0 .. p0+H-1 of field k.
+// Fourier-buffer loads of the synthesis (each value read once) that leave no line in L1, so
+// the twiddle and permutation tables stay there.
+__device__ __forceinline__ float2 ld_once(const float2* p) {
+  float2 v;
+  asm("ld.global.nc.L1::no_allocate.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ double2 ld_once(const double2* p) {
+  double2 v;
+  asm("ld.global.nc.L1::no_allocate.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+  return v;
+}
+
 template <typename T, int H, bool GENERIC>
 __device__ __forceinline__ void fft_syn_body(const FFTJob<T>& J, int p0, int k, unsigned char* smem_raw) {
   const PlanDev& P = J.P;
@@ -190,8 +203,8 @@ __device__ __forceinline__ void fft_syn_body(const FFTJob<T>& J, int p0, int k, 
         const int im = idx / H, h = idx - im * H;
         if (h < hv) {
           const size_t base = ((size_t)k * P.nm + im) * 2 * npair + p0 + h;
-          Ev[u] = W[base];
-          Ov[u] = W[base + npair];
+          Ev[u] = ld_once(W + base);
+          Ov[u] = ld_once(W + base + npair);
         }
       }
     }
