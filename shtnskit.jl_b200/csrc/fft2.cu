@@ -148,13 +148,30 @@ __device__ __forceinline__ void dft(C2* u) {
   }
 }
 
-// Shared-memory index of point n of pair-pair hp (HP pair-pairs per CTA): HP point-pairs
-// of 16 bytes per n, and HP more after every 8 n, which keeps every pass's quarter-warp
-// accesses (8 lanes: the HP pair-pairs of 8 / HP consecutive groups) on distinct banks.
-template <int HP>
-__device__ __forceinline__ int sidx(int n, int hp) { return (n + (n >> 3)) * HP + hp; }
+// Shared-memory index of point n of pair-pair hp (HP pair-pairs per CTA, 16 bytes each).
+// Synthesis (SW false): HP point-pairs per n and HP more after every 8 n, which keeps every
+// pass's quarter-warp accesses (8 lanes: the HP pair-pairs of 8 / HP consecutive groups) on
+// distinct banks. Analysis (SW true, HP = 4): no padding; a 128-byte row holds points 2r and
+// 2r + 1 in the halves given by the parity of n ^ (n >> 3) ^ (n >> 7), so a quarter warp
+// covers all 8 slots of a row pair when its two points differ by 1 from an even point (the
+// first pass and the span-8 pass), by 8 from a multiple of 16 (the span-1 pass) or by 128
+// without a carry into bit 7 (bins at digit-reversed positions, which the padded layout
+// puts on the same banks). The smaller tile leaves the L1 more room beside it (FFT
+// analysis 0.429 -> 0.420 ms at nlon 2048 x 64; the synthesis measured slower with it).
+template <int HP, bool SW>
+__device__ __forceinline__ int sidx(int n, int hp) {
+  if constexpr (SW) {
+    static_assert(HP == 4, "row layout of four pair-pairs");
+    return (((n >> 1) << 1) | ((n ^ (n >> 3) ^ (n >> 7)) & 1)) * HP + hp;
+  } else {
+    return (n + (n >> 3)) * HP + hp;
+  }
+}
+// Elements of the larger (synthesis) layout; the analysis uses the first N HP of them.
 template <int HP>
 __host__ __device__ inline int smem_elems(int N) { return (N + (N >> 3)) * HP; }
+template <int HP>
+__host__ __device__ inline int smem_elems_ana(int N) { return N * HP; }
 
 __device__ __forceinline__ float4 ld4(const float4* X, int i) { return X[i]; }
 __device__ __forceinline__ C2 ldc(const float4* X, int i) {
@@ -175,14 +192,14 @@ __device__ __forceinline__ void pass_smem(float4* X, int N, int S, const float2*
     const int j = grp & (S - 1), base = (grp - j) * R + j;
     C2 u[R];
 #pragma unroll
-    for (int q = 0; q < R; ++q) u[q] = ldc(X, sidx<HP>(base + q * S, hp));
+    for (int q = 0; q < R; ++q) u[q] = ldc(X, sidx<HP, (DIR < 0)>(base + q * S, hp));
     dft<R, DIR>(u);
     if (j != 0) {
 #pragma unroll
       for (int q = 1; q < R; ++q) u[q] = ctw<DIR>(u[q], tw[(q - 1) * S + j]);
     }
 #pragma unroll
-    for (int q = 0; q < R; ++q) stc(X, sidx<HP>(base + q * S, hp), u[q]);
+    for (int q = 0; q < R; ++q) stc(X, sidx<HP, (DIR < 0)>(base + q * S, hp), u[q]);
   }
 }
 
@@ -247,7 +264,7 @@ __device__ __forceinline__ void first_from_grid(float4* X, const Job& J, const f
       for (int q = 1; q < R0; ++q) u[q] = ctw<-1>(u[q], tw[(q - 1) * S + j]);
     }
 #pragma unroll
-    for (int q = 0; q < R0; ++q) stc(X, sidx<HP>(j + q * S, hp), u[q]);
+    for (int q = 0; q < R0; ++q) stc(X, sidx<HP, true>(j + q * S, hp), u[q]);
   }
 }
 
@@ -297,8 +314,8 @@ __device__ __forceinline__ void ana_body(const Job& J, int k, int p0, float4* X,
     const bool valid = idx < nitem;
     const int hp = idx % HP, im = valid ? idx / HP : 0, m = im * P.mres;
     const int pa = p0 + 2 * hp;
-    const C2 zm = ldc(X, sidx<HP>(J.perm[m], hp));
-    const C2 zc = ldc(X, sidx<HP>(J.perm[m == 0 ? 0 : N - m], hp));
+    const C2 zm = ldc(X, sidx<HP, true>(J.perm[m], hp));
+    const C2 zc = ldc(X, sidx<HP, true>(J.perm[m == 0 ? 0 : N - m], hp));
     const u64 sre = add2(zm.re, zc.re), sim = sub2(zm.im, zc.im);   // Z_m + conj Z_c
     const u64 dre = sub2(zm.re, zc.re), dim = add2(zm.im, zc.im);   // Z_m - conj Z_c
     const u64 hw = pk(make_float2(0.5f * wfac[2 * hp], 0.5f * wfac[2 * hp + 1]));
@@ -347,7 +364,7 @@ __device__ __forceinline__ void last_to_grid(const float4* X, const Job& J, floa
     const int hp = gi % HP, blk = gi / HP;
     C2 u[RL];
 #pragma unroll
-    for (int q = 0; q < RL; ++q) u[q] = ldc(X, sidx<HP>(blk * RL + q, hp));
+    for (int q = 0; q < RL; ++q) u[q] = ldc(X, sidx<HP, false>(blk * RL + q, hp));
     dft<RL, +1>(u);
     const int pa = p0 + 2 * hp;
     if (pa >= npair) continue;
@@ -380,7 +397,7 @@ __device__ __forceinline__ void syn_body(const Job& J, int k, int p0, float4* X,
     const int zlo = (P.mres == 1) ? mlim + 1 : 0, zhi = (P.mres == 1) ? N - mlim : N;
     const int zn = zhi - zlo;
     for (int idx = threadIdx.x; idx < zn * HP; idx += blockDim.x)
-      X[sidx<HP>(zlo + idx / HP, idx % HP)] = make_float4(0.f, 0.f, 0.f, 0.f);
+      X[sidx<HP, false>(zlo + idx / HP, idx % HP)] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
   for (int h = threadIdx.x; h < 2 * HP; h += blockDim.x) gfac[h] = (float)J.scale;
   __syncthreads();
@@ -420,10 +437,10 @@ __device__ __forceinline__ void syn_body(const Job& J, int k, int p0, float4* X,
       const u64 sre = sub2(ere, ore), sim = sub2(eim, oim);   // X_S
       if (m == 0) {
         const float2 a = up(nre), b = up(sre);
-        X[sidx<HP>(0, hp)] = make_float4(a.x, a.y, b.x, b.y);
+        X[sidx<HP, false>(0, hp)] = make_float4(a.x, a.y, b.x, b.y);
       } else {
-        stc(X, sidx<HP>(m, hp), C2{sub2(nre, sim), add2(nim, sre)});
-        stc(X, sidx<HP>(N - m, hp), C2{add2(nre, sim), sub2(sre, nim)});
+        stc(X, sidx<HP, false>(m, hp), C2{sub2(nre, sim), add2(nim, sre)});
+        stc(X, sidx<HP, false>(N - m, hp), C2{add2(nre, sim), sub2(sre, nim)});
       }
     }
   }
@@ -514,7 +531,7 @@ constexpr int kFft2HP = 4;
 
 int launch_fft2_ana(const shtb_plan* p, const float* grid, void* W, int nf, int mlim, double wscale, cudaStream_t st) {
   constexpr int HP = kFft2HP;
-  const size_t smem = (size_t)f2::smem_elems<HP>(p->fft.n) * 16;
+  const size_t smem = (size_t)f2::smem_elems_ana<HP>(p->fft.n) * 16;
   SHTB_TRY_CUDA(cudaFuncSetAttribute(f2::ana_kernel<HP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                 "fft2 smem attr");
   f2::Job J = fft2_job(p, p->d_rev, wscale, nf, mlim);
