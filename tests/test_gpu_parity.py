@@ -245,3 +245,21 @@ def test_wide_batches_fp64_and_mixed(nf):
     assert rel_l2(f32, so.synthesis_batch(ocfg, a.astype(np.complex64).astype(np.complex128))) <= 1e-6
     b32 = host(sht.analysis_batch(cfg, g.astype(np.float32), precision="mixed"))
     assert rel_l2(b32, so.analysis_batch(ocfg, g.astype(np.float32).astype(np.float64))) <= 1e-6
+
+
+@pytest.mark.gpu
+def test_sharded_wrappers_single_process():
+    """synthesis/analysis_batch_sharded with no process group: the whole batch on this GPU,
+    bit for bit the plain batched calls, and against the oracle (the multi-rank split and
+    all-gather are covered on CPU ranks in test_multirank.py)."""
+    from shtb200.distributed import analysis_batch_sharded, synthesis_batch_sharded
+
+    cfg = sht.create_gauss_config(31, 32)
+    ocfg = so.create_gauss_config(31, 32)
+    a = rand_alm(31, 31, 5, seed=31)
+    f = synthesis_batch_sharded(cfg, a)
+    assert torch.equal(f, sht.synthesis_batch(cfg, a))
+    assert rel_l2(host(f), so.synthesis_batch(ocfg, a)) <= TOL64
+    b = analysis_batch_sharded(cfg, f)
+    assert torch.equal(b, sht.analysis_batch(cfg, f))
+    assert rel_l2(host(b), so.analysis_batch(ocfg, host(f))) <= TOL64
