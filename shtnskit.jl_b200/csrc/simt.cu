@@ -56,7 +56,7 @@ __host__ __device__ inline size_t syn_smem_bytes(int lmax, int nf) {
 }
 
 template <int NF>
-__device__ __forceinline__ void syn_body(const Args& a, int im, int pb, double* smem, int* sMin) {
+__device__ __forceinline__ void syn_body(const Args& a, int im, int pb, double* smem) {
   const PlanDev& P = a.P;
   const int m = im * P.mres;
   const int lend = a.lend, ndeg = lend - m + 1;
@@ -85,14 +85,13 @@ __device__ __forceinline__ void syn_body(const Args& a, int im, int pb, double* 
     s0 = v.x;
     s1 = v.y;
   }
+  // each warp starts at its own pairs' first significant degree (below it every value is
+  // zero) and a warp with no pair of the plan skips the degree loop
   int mn = l0;
   for (int o = 16; o > 0; o >>= 1) mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
-  if ((threadIdx.x & 31) == 0) sMin[threadIdx.x >> 5] = mn;
-  __syncthreads();
-  int lbeg = sMin[0];
-#pragma unroll
-  for (int w = 1; w < kSynThreads / 32; ++w) lbeg = min(lbeg, sMin[w]);
-  lbeg = max(lbeg, m);
+  __syncthreads();   // the staged alpha and coefficients
+  const int lbeg = max(mn, m);
+  const bool warp_live = pb * kSynThreads + (threadIdx.x & ~31) < npair;
   double2 accE[NF], accO[NF];
 #pragma unroll
   for (int k = 0; k < NF; ++k) accE[k] = accO[k] = make_double2(0.0, 0.0);
@@ -113,13 +112,15 @@ __device__ __forceinline__ void syn_body(const Args& a, int im, int pb, double* 
       acc[k].y = fma(r, c.y, acc[k].y);
     }
   };
-  int l = lbeg;
-  if (((l - m) & 1) && l <= lend) step(l++, accO);
-  for (; l + 1 <= lend; l += 2) {
-    step(l, accE);
-    step(l + 1, accO);
+  if (warp_live) {
+    int l = lbeg;
+    if (((l - m) & 1) && l <= lend) step(l++, accO);
+    for (; l + 1 <= lend; l += 2) {
+      step(l, accE);
+      step(l + 1, accO);
+    }
+    if (l <= lend) step(l, accE);
   }
-  if (l <= lend) step(l, accE);
   if (pair < npair) {
 #pragma unroll
     for (int k = 0; k < NF; ++k) {
@@ -136,8 +137,7 @@ __device__ __forceinline__ void syn_body(const Args& a, int im, int pb, double* 
 template <int NF>
 __global__ void __launch_bounds__(kSynThreads) syn_kernel(const __grid_constant__ Args a) {
   extern __shared__ __align__(16) double smem[];
-  __shared__ int sMin[kSynThreads / 32];
-  syn_body<NF>(a, blockIdx.y, blockIdx.x, smem, sMin);
+  syn_body<NF>(a, blockIdx.y, blockIdx.x, smem);
 }
 
 // Persistent kernel over the items of many transforms (uneven batches): item = (transform,
@@ -147,7 +147,6 @@ __global__ void __launch_bounds__(kSynThreads) syn_group_kernel(const Args* __re
                                                                 const int4* __restrict__ items, int nitems,
                                                                 int* __restrict__ queue) {
   extern __shared__ __align__(16) double smem[];
-  __shared__ int sMin[kSynThreads / 32];
   __shared__ Args sa;
   __shared__ int4 s_it;
   for (;;) {
@@ -160,9 +159,9 @@ __global__ void __launch_bounds__(kSynThreads) syn_group_kernel(const Args* __re
     const int4 it = s_it;
     if (it.x < 0) break;
     if (sa.nf == 1)
-      syn_body<1>(sa, it.y, it.z, smem, sMin);   // ends with a CTA barrier
+      syn_body<1>(sa, it.y, it.z, smem);   // ends with a CTA barrier
     else
-      syn_body<2>(sa, it.y, it.z, smem, sMin);
+      syn_body<2>(sa, it.y, it.z, smem);
   }
 }
 
