@@ -276,9 +276,9 @@ struct Smem {
   static constexpr int kFull = 16;   // per-chunk conversion barriers (analysis)
   static constexpr int kRel = 16;    // chunk-release barriers
   static constexpr int kBar = kSt * kStage;
-  // barriers: full[kFull], ldfull[kLd], rel[kRel], acce[kAcc]; then TMEM slot, abort flag,
-  // then the FP32 column scales of the last kScR chunks
-  static constexpr int kScOff = (kBar + (kFull + kLd + kRel + kAcc) * 8 + 16 + 15) & ~15;
+  // barriers: full[kFull], ldfull[kLd], ldb[kLd], rel[kRel], acce[kAcc]; then TMEM slot,
+  // abort flag, then the FP32 column scales of the last kScR chunks
+  static constexpr int kScOff = (kBar + (kFull + 2 * kLd + kRel + kAcc) * 8 + 16 + 15) & ~15;
   static constexpr int kBytes = kScOff + kScR * N * 4;
   // grouped kernels only: a ring of kQ claimed tile indices with its full/empty barriers
   static constexpr int kQ = 8;
@@ -309,7 +309,7 @@ struct TileCoord {
 
 // Shared-memory barriers of a GEMM CTA (initialised once per CTA).
 struct Bars {
-  unsigned long long *full, *ldfull, *rel, *acce;
+  unsigned long long *full, *ldfull, *ldb, *rel, *acce;
   unsigned* tmem_slot;
   volatile int* abort_flag;
   float* fsc;   // analysis: [kScR][N] factors 2^-(row scale + table scale) of chunk gc % kScR
@@ -320,8 +320,9 @@ __device__ __forceinline__ Bars gemm_bars(unsigned char* sm) {
   using S = Smem<N>;  // barriers follow the stage ring
   Bars B;
   B.full = reinterpret_cast<unsigned long long*>(sm + S::kBar);   // [kFull] chunk gc split (A in TMEM)
-  B.ldfull = B.full + S::kFull;   // [kLd] bulk copies of chunk q landed (q % kLd)
-  B.rel = B.ldfull + S::kLd;      // [kRel] MMAs of chunk q done (q % kRel)
+  B.ldfull = B.full + S::kFull;   // [kLd] bulk copies of chunk q landed (q % kLd; the analysis: its A)
+  B.ldb = B.ldfull + S::kLd;      // [kLd] analysis: the B copy of chunk q landed (q % kLd)
+  B.rel = B.ldb + S::kLd;         // [kRel] MMAs of chunk q done (q % kRel)
   B.acce = B.rel + S::kRel;       // [kAcc] TMEM chunk accumulator b drained by the promotion warps
   B.tmem_slot = reinterpret_cast<unsigned*>(B.acce + kAcc);
   B.abort_flag = reinterpret_cast<volatile int*>(B.tmem_slot + 1);
@@ -344,7 +345,10 @@ __device__ __forceinline__ unsigned gemm_cta_setup(const Bars& B) {
   if (tid == 0) {
     // two arrivals per splitter warp and chunk
     for (int s = 0; s < Smem<N>::kFull; ++s) mbar_init(&B.full[s], 2 * kSW);
-    for (int s = 0; s < Smem<N>::kLd; ++s) mbar_init(&B.ldfull[s], 1);
+    for (int s = 0; s < Smem<N>::kLd; ++s) {
+      mbar_init(&B.ldfull[s], 1);
+      mbar_init(&B.ldb[s], 1);
+    }
     for (int s = 0; s < Smem<N>::kRel; ++s) mbar_init(&B.rel[s], 1);
     for (int b = 0; b < kAcc; ++b) mbar_init(&B.acce[b], kPW<N>);   // one arrival per promotion warp
     *B.abort_flag = 0;
@@ -456,16 +460,24 @@ __device__ __forceinline__ bool loader_tile(const Args& a, const TileCoord& tc, 
     unsigned char* sa = sm + (size_t)st * S::kStage;
     unsigned char* sb = sa + S::kStageA;
     unsigned long long* bar = &B.ldfull[gc % S::kLd];
+    // the analysis's B copy goes first, on its own barrier, so that the splitters start
+    // converting while the A copy is still on its way
+    unsigned long long* barb = (MODE == 1) ? &B.ldb[gc % S::kLd] : bar;
     // A tiles come in hi/lo pairs, and so do the synthesis B tiles (the analysis loads its
     // FP32 B tiles and treats a missing last odd one as zeros)
     const int na = (nk + 1) & ~1, nb = (MODE == 0) ? na : nk;
-    mbar_expect_tx(bar, (unsigned)na * abytes + (unsigned)nb * bbytes);
-    bulk_g2s(sa, a0 + (long long)k0 * T.arows * kK, na * abytes, bar);
-    if (bcontig) {
-      bulk_g2s(sb, bsrc + (long long)k0 * nfp * 16, nb * bbytes, bar);
+    if (MODE == 1) {
+      mbar_expect_tx(barb, (unsigned)nb * bbytes);
+      mbar_expect_tx(bar, (unsigned)na * abytes);
     } else {
-      for (int s = 0; s < nb; ++s) bulk_g2s(sb + s * S::kTileB, bsrc + (long long)(k0 + s) * nfp * 16, bbytes, bar);
+      mbar_expect_tx(bar, (unsigned)na * abytes + (unsigned)nb * bbytes);
     }
+    if (bcontig) {
+      bulk_g2s(sb, bsrc + (long long)k0 * nfp * 16, nb * bbytes, barb);
+    } else {
+      for (int s = 0; s < nb; ++s) bulk_g2s(sb + s * S::kTileB, bsrc + (long long)(k0 + s) * nfp * 16, bbytes, barb);
+    }
+    bulk_g2s(sa, a0 + (long long)k0 * T.arows * kK, na * abytes, bar);
   }
   return true;
 }
@@ -515,7 +527,7 @@ __device__ __forceinline__ bool splitter_tile(const Args& a, const TileInfo& T, 
     const unsigned gc = c0 + q++;
     if ((int)(gc % kSG) != grp) continue;
     const int nk = min(kChunk, T.nks - c * kChunk), nk2 = (nk + 1) >> 1;
-    const bool ok = mbar_wait(&B.ldfull[gc % S::kLd], (gc / S::kLd) & 1, B.abort_flag, a.err, a.wait_ns);
+    const bool ok = mbar_wait(&B.ldb[gc % S::kLd], (gc / S::kLd) & 1, B.abort_flag, a.err, a.wait_ns);
     if (!__all_sync(0xffffffffu, ok)) return false;
     unsigned char* Bs = sm + (size_t)(gc % S::kSt) * S::kStage + S::kStageA;
 #pragma unroll
@@ -628,6 +640,9 @@ __device__ __forceinline__ bool splitter_tile(const Args& a, const TileInfo& T, 
       }
       if (rowok && v == 0) B.fsc[(gc % kScR) * N + r] = __int_as_float((127 - e - sa) << 23);
     }
+    // the chunk's A copy has landed too before the MMAs may run (they wait only on full)
+    const bool oka = mbar_wait(&B.ldfull[gc % S::kLd], (gc / S::kLd) & 1, B.abort_flag, a.err, a.wait_ns);
+    if (!__all_sync(0xffffffffu, oka)) return false;
     // the B tiles written here are read by the MMAs (async proxy)
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncwarp();
@@ -899,7 +914,10 @@ __device__ __forceinline__ void gemm_tiles(const Src& src, unsigned char* sm, co
   using S = Smem<N>;
   if (loader) {
     for (unsigned gc = issued > (unsigned)S::kSt ? issued - S::kSt : 0u; gc < issued; ++gc)
-      if ((int)gc != skip) mbar_wait_drain(&B.ldfull[gc % S::kLd], (gc / S::kLd) & 1);
+      if ((int)gc != skip) {
+        mbar_wait_drain(&B.ldfull[gc % S::kLd], (gc / S::kLd) & 1);
+        if (MODE == 1) mbar_wait_drain(&B.ldb[gc % S::kLd], (gc / S::kLd) & 1);
+      }
   } else if (mma && committed >= 0) {
     mbar_wait_drain(&B.rel[committed % S::kRel], (committed / S::kRel) & 1);
   }
