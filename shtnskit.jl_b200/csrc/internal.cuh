@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -159,10 +160,12 @@ struct shtb_plan {
   std::vector<long long> htab_seg;
   std::vector<unsigned long long> hmsk_s, hmsk_a;   // host copies of the live-chunk masks
   // GEMM tile lists (analysis: (im, j0); synthesis: (im, p0)) for truncation degree key
-  std::vector<int2> hmx_tiles, hmx_stiles;
-  int mx_tiles_key = -1, mx_stiles_key = -1;
-  int2* d_mx_tiles = nullptr;
-  int2* d_mx_stiles = nullptr;
-  unsigned long long* d_mx_tmask = nullptr;    // live-chunk masks of the lists' entries
-  unsigned long long* d_mx_stmask = nullptr;
+  // GEMM tile lists of the mixed path per direction (0 synthesis, 1 analysis) and truncation
+  // degree, kept until the plan is destroyed: device entries and live-chunk masks
+  struct MxTileList {
+    int2* tiles = nullptr;
+    unsigned long long* masks = nullptr;
+    int count = 0;
+  };
+  std::map<int, MxTileList> mx_lists[2];
 };

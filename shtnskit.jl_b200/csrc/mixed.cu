@@ -1514,79 +1514,84 @@ static Args base_args(const shtb_plan* p) {
   return a;
 }
 
-// GEMM tile list of one direction for truncation degree ltr, cached on the plan: synthesis
-// (im, first pair), analysis (im, first degree row), ordered by decreasing count of live
-// chunks over both parities (the persistent CTAs take tiles blockIdx.x, + gridDim.x, ...,
-// so every round holds tiles of similar cost).
-static int gemm_tiles_list(const shtb_plan* cp, int mode, int ltr, int mlim, cudaStream_t st, int* count) {
+// GEMM tile list of one direction for truncation degree ltr, built once per (direction, ltr)
+// and kept on the plan until it is destroyed, so a list handed to a kernel is never freed
+// under it (calls from several host threads share the cache under the plan's table mutex):
+// synthesis (im, first pair), analysis (im, first degree row), each entry with the
+// live-chunk masks of both parities, ordered by decreasing count of live chunks (the
+// persistent CTAs take tiles blockIdx.x, + gridDim.x, ..., so every round holds tiles of
+// similar cost).
+static int gemm_tiles_list(const shtb_plan* cp, int mode, int ltr, int mlim, cudaStream_t st,
+                           shtb_plan::MxTileList* out) {
   shtb_plan* p = const_cast<shtb_plan*>(cp);
-  std::vector<int2>& tl = mode ? p->hmx_tiles : p->hmx_stiles;
-  int& key = mode ? p->mx_tiles_key : p->mx_stiles_key;
-  int2*& dev = mode ? p->d_mx_tiles : p->d_mx_stiles;
-  unsigned long long*& dmask = mode ? p->d_mx_tmask : p->d_mx_stmask;
-  if (key != ltr) {
-    tl.clear();
-    std::vector<int> cost;
-    std::vector<unsigned long long> msk;   // [entry][parity]
-    const int ntp = p->npp / kM, njt = p->tab_njt;
-    auto live = [](unsigned long long msk, int nall) {
-      return __builtin_popcountll(nall >= 64 ? msk : msk & ((1ull << nall) - 1)) + std::max(nall - 64, 0);
-    };
-    for (int im = 0; im * p->mres <= mlim; ++im) {
-      const int m = im * p->mres;
-      if (mode == 0) {
-        for (int pt = 0; pt * kM < p->npair; ++pt) {
-          int c = 0;
-          for (int par = 0; par < 2; ++par) {
-            const int J = (ltr >= m + par) ? (ltr - m - par) / 2 + 1 : 0;
-            const unsigned long long mk = p->hmsk_s[(size_t)(2 * im + par) * ntp + pt];
-            c += live(mk, ((J + kK - 1) / kK + kChunk - 1) / kChunk);
-            msk.push_back(mk);
-          }
-          tl.push_back(make_int2(im, pt * kM));
-          cost.push_back(c);
+  std::lock_guard<std::mutex> lk(p->tab_mu);
+  auto it = p->mx_lists[mode].find(ltr);
+  if (it != p->mx_lists[mode].end()) {
+    *out = it->second;
+    return SHTB_OK;
+  }
+  std::vector<int2> tl;
+  std::vector<int> cost;
+  std::vector<unsigned long long> msk;   // [entry][parity]
+  const int ntp = p->npp / kM, njt = p->tab_njt;
+  auto live = [](unsigned long long mk, int nall) {
+    return __builtin_popcountll(nall >= 64 ? mk : mk & ((1ull << nall) - 1)) + std::max(nall - 64, 0);
+  };
+  for (int im = 0; im * p->mres <= mlim; ++im) {
+    const int m = im * p->mres;
+    if (mode == 0) {
+      for (int pt = 0; pt * kM < p->npair; ++pt) {
+        int c = 0;
+        for (int par = 0; par < 2; ++par) {
+          const int J = (ltr >= m + par) ? (ltr - m - par) / 2 + 1 : 0;
+          const unsigned long long mk = p->hmsk_s[(size_t)(2 * im + par) * ntp + pt];
+          c += live(mk, ((J + kK - 1) / kK + kChunk - 1) / kChunk);
+          msk.push_back(mk);
         }
-      } else {
-        const int JE = (ltr - m) / 2 + 1;
-        const int nall = ((p->npair + kK - 1) / kK + kChunk - 1) / kChunk;
-        for (int j0 = 0; j0 < JE; j0 += kM) {
-          int c = 0;
-          for (int par = 0; par < 2; ++par) {
-            const unsigned long long mk = p->hmsk_a[(size_t)(2 * im + par) * njt + j0 / kM];
-            c += live(mk, nall);
-            msk.push_back(mk);
-          }
-          tl.push_back(make_int2(im, j0));
-          cost.push_back(c);
+        tl.push_back(make_int2(im, pt * kM));
+        cost.push_back(c);
+      }
+    } else {
+      const int JE = (ltr - m) / 2 + 1;
+      const int nall = ((p->npair + kK - 1) / kK + kChunk - 1) / kChunk;
+      for (int j0 = 0; j0 < JE; j0 += kM) {
+        int c = 0;
+        for (int par = 0; par < 2; ++par) {
+          const unsigned long long mk = p->hmsk_a[(size_t)(2 * im + par) * njt + j0 / kM];
+          c += live(mk, nall);
+          msk.push_back(mk);
         }
+        tl.push_back(make_int2(im, j0));
+        cost.push_back(c);
       }
     }
-    std::vector<int> ord(tl.size());
-    for (size_t i = 0; i < ord.size(); ++i) ord[i] = (int)i;
-    std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return cost[x] > cost[y]; });
-    std::vector<int2> sorted(tl.size());
-    std::vector<unsigned long long> smsk(msk.size());
-    for (size_t i = 0; i < ord.size(); ++i) {
-      sorted[i] = tl[ord[i]];
-      smsk[2 * i] = msk[2 * ord[i]];
-      smsk[2 * i + 1] = msk[2 * ord[i] + 1];
-    }
-    tl.swap(sorted);
-    if (dev) cudaFree(dev);
-    if (dmask) cudaFree(dmask);
-    dev = nullptr;
-    dmask = nullptr;
-    key = -1;
-    SHTB_TRY_CUDA(cudaMalloc(&dev, tl.size() * sizeof(int2)), "mixed tiles");
-    SHTB_TRY_CUDA(cudaMalloc(&dmask, smsk.size() * 8), "mixed tile masks");
-    SHTB_TRY_CUDA(cudaMemcpyAsync(dev, tl.data(), tl.size() * sizeof(int2), cudaMemcpyHostToDevice, st),
-                  "mixed tiles upload");
-    // pageable source: the copy is complete when the call returns
-    SHTB_TRY_CUDA(cudaMemcpyAsync(dmask, smsk.data(), smsk.size() * 8, cudaMemcpyHostToDevice, st),
-                  "mixed tile masks upload");
-    key = ltr;
   }
-  *count = (int)tl.size();
+  std::vector<int> ord(tl.size());
+  for (size_t i = 0; i < ord.size(); ++i) ord[i] = (int)i;
+  std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return cost[x] > cost[y]; });
+  std::vector<int2> sorted(tl.size());
+  std::vector<unsigned long long> smsk(msk.size());
+  for (size_t i = 0; i < ord.size(); ++i) {
+    sorted[i] = tl[ord[i]];
+    smsk[2 * i] = msk[2 * ord[i]];
+    smsk[2 * i + 1] = msk[2 * ord[i] + 1];
+  }
+  shtb_plan::MxTileList L;
+  L.count = (int)sorted.size();
+  cudaError_t e = cudaMalloc(&L.tiles, std::max<size_t>(1, sorted.size()) * sizeof(int2));
+  if (e == cudaSuccess) e = cudaMalloc(&L.masks, std::max<size_t>(1, smsk.size()) * 8);
+  // pageable sources: each copy has read its source when the call returns
+  if (e == cudaSuccess && L.count)
+    e = cudaMemcpyAsync(L.tiles, sorted.data(), sorted.size() * sizeof(int2), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && L.count)
+    e = cudaMemcpyAsync(L.masks, smsk.data(), smsk.size() * 8, cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) {
+    if (L.tiles) cudaFree(L.tiles);
+    if (L.masks) cudaFree(L.masks);
+    return set_error(SHTB_ERR_CUDA, std::string("mixed tiles: ") + cudaGetErrorString(e));
+  }
+  p->mx_lists[mode][ltr] = L;
+  *out = L;
   return SHTB_OK;
 }
 
@@ -1615,11 +1620,11 @@ int mixed_synthesis(const shtb_plan* p, const void* alm, void* f, int nf, int lt
   prof_begin(st);
   mixed_pack_kernel<<<dim3(mlim / p->mres + 1, (nf + kPackFields - 1) / kPackFields), kPackThreads, 0, st>>>(a);
   SHTB_LAUNCHED("tc gemm B packing kernel");
-  int ntl = 0;
-  if ((rc = gemm_tiles_list(p, 0, ltr, mlim, st, &ntl))) return rc;
-  a.tiles = p->d_mx_stiles;
-  a.tmask = p->d_mx_stmask;
-  if ((rc = dispatch_gemm<0>(p, a, nf, 2 * ntl, st))) return rc;
+  shtb_plan::MxTileList tl;
+  if ((rc = gemm_tiles_list(p, 0, ltr, mlim, st, &tl))) return rc;
+  a.tiles = tl.tiles;
+  a.tmask = tl.masks;
+  if ((rc = dispatch_gemm<0>(p, a, nf, 2 * tl.count, st))) return rc;
   return launch_fft_syn<float, float>(p, work, (float*)f, nullptr, 1, nf, mlim, p->phi_inv_scale / p->nlon, 0, 0, st);
 }
 
@@ -1639,8 +1644,8 @@ int mixed_analysis(const shtb_plan* p, const void* f, void* alm, int nf, int ltr
   if ((rc = launch_fft_ana<float, float>(p, (const float*)f, nullptr, 1, work, nf, mlim, p->ana_scale, 1, 0, st, 1)))
     return rc;
   // analysis tiles: 128 degrees of each parity per tile
-  int ntl = 0;
-  if ((rc = gemm_tiles_list(p, 1, ltr, mlim, st, &ntl))) return rc;
+  shtb_plan::MxTileList tl;
+  if ((rc = gemm_tiles_list(p, 1, ltr, mlim, st, &tl))) return rc;
   Args a = base_args(p);
   a.tab = p->d_tab_ana;
   a.bimg = (float*)work;
@@ -1649,13 +1654,13 @@ int mixed_analysis(const shtb_plan* p, const void* f, void* alm, int nf, int ltr
   a.nf = nf;
   a.lend = ltr;
   a.lcap = ltr;
-  a.tiles = p->d_mx_tiles;
-  a.tmask = p->d_mx_tmask;
+  a.tiles = tl.tiles;
+  a.tmask = tl.masks;
   if (packed) {
     a.cpacked = 1;
     a.ld_k = nlm;
   }
-  if ((rc = dispatch_gemm<1>(p, a, nf, 2 * ntl, st))) return rc;
+  if ((rc = dispatch_gemm<1>(p, a, nf, 2 * tl.count, st))) return rc;
   if (!packed && (p->mres > 1 || mlim < p->mmax)) {
     dim3 zg(p->mmax + 1, nf);
     prof_begin(st);

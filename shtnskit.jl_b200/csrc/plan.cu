@@ -463,10 +463,11 @@ extern "C" int shtb_plan_destroy(shtb_plan* p) {
   if (dev != p->device) cudaSetDevice(p->device);
   cudaError_t e = cudaFree(p->dmem);
   if (p->d_tab) cudaFree(p->d_tab);
-  if (p->d_mx_tiles) cudaFree(p->d_mx_tiles);
-  if (p->d_mx_stiles) cudaFree(p->d_mx_stiles);
-  if (p->d_mx_tmask) cudaFree(p->d_mx_tmask);
-  if (p->d_mx_stmask) cudaFree(p->d_mx_stmask);
+  for (auto& lists : p->mx_lists)
+    for (auto& kv : lists) {
+      if (kv.second.tiles) cudaFree(kv.second.tiles);
+      if (kv.second.masks) cudaFree(kv.second.masks);
+    }
   if (dev >= 0 && dev != p->device) cudaSetDevice(dev);
   delete p;
   return check_cuda(e, "plan destroy");
