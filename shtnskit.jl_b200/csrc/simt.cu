@@ -140,28 +140,110 @@ __global__ void __launch_bounds__(kSynThreads) syn_kernel(const __grid_constant_
   syn_body<NF>(a, blockIdx.y, blockIdx.x, smem);
 }
 
-// Persistent kernel over the items of many transforms (uneven batches): item = (transform,
-// order index, pair block), list sorted by decreasing work and claimed from the device
-// counter *queue (zero at launch); the transform's Args are staged in shared memory per item.
-__global__ void __launch_bounds__(kSynThreads) syn_group_kernel(const Args* __restrict__ targs,
+// Persistent kernel over the items of many transforms (uneven batches), one item per warp:
+// item = (transform, order index, block of 32 latitude pairs), list sorted by decreasing
+// work and claimed by each warp from the device counter *queue (zero at launch). A warp
+// stages its order's recurrence coefficients and FP64 coefficients in its own shared-memory
+// slice, kGroupChunk degrees at a time, so warps never wait for one another (a CTA-wide item
+// ends with a barrier at which the warps nearer the poles, which start at higher degrees,
+// wait for the others). Per thread the arithmetic is that of syn_body, so the results are
+// the same bit for bit.
+constexpr int kGroupChunk = 128;
+constexpr size_t kGroupWarpDoubles = kGroupChunk + kGroupChunk * 2 * 2;   // alpha, then [degree][NF <= 2] double2
+
+template <int NF>
+__device__ __forceinline__ void syn_warp_item(const Args& a, int im, int pb, double* wsm) {
+  const PlanDev& P = a.P;
+  const int lane = threadIdx.x & 31;
+  const int m = im * P.mres;
+  const int lend = a.lend, ndeg = lend - m + 1;
+  const long long poff = P.off[im];
+  double* sAl = wsm;
+  double2* sC = reinterpret_cast<double2*>(wsm + kGroupChunk);
+  const int npair = P.npair, pair = pb * 32 + lane;
+  int l0 = INT_MAX / 2;
+  double x = 0.0, s0 = 0.0, s1 = 0.0;
+  if (pair < npair) {
+    x = P.x[pair];
+    l0 = P.l0[(size_t)im * npair + pair];
+    const double2 v = P.r01[(size_t)im * npair + pair];
+    s0 = v.x;
+    s1 = v.y;
+  }
+  int mn = l0;
+  for (int o = 16; o > 0; o >>= 1) mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+  const int dbeg = max(mn, m) - m;   // first degree (relative to m) with a nonzero value
+  const long long col = a.cpacked ? lm_base(P.lmax, P.mres, m) : (long long)m * (P.lmax + 1);
+  double2 accE[NF], accO[NF];
+#pragma unroll
+  for (int k = 0; k < NF; ++k) accE[k] = accO[k] = make_double2(0.0, 0.0);
+  double ra = 0.0, rb = 0.0;
+  for (int d0 = dbeg; d0 < ndeg; d0 += kGroupChunk) {
+    const int nd = min(kGroupChunk, ndeg - d0);
+    __syncwarp();   // the previous chunk's values are read
+    for (int d = lane; d < nd; d += 32) sAl[d] = P.alpha[poff + d0 + d];
+    for (int i = lane; i < nd * NF; i += 32) {
+      const int d = i / NF, k = i - d * NF, l = m + d0 + d;
+      double2 v = make_double2(0.0, 0.0);
+      if (k < a.nf) {
+        const float2 c = a.cin[(long long)k * a.ld_k + col + l];
+        const double f = P.cfac[poff + d0 + d] * coef_factor(a, l, m);
+        v = make_double2(c.x * f, c.y * f);
+      }
+      sC[i] = v;
+    }
+    __syncwarp();
+    auto step = [&](int l, double2 (&acc)[NF]) {
+      const int d = l - m - d0;
+      double r = fma(sAl[d] * x, ra, -rb);
+      r = (l == l0) ? s0 : r;
+      r = (l == l0 + 1) ? s1 : r;
+      rb = ra;
+      ra = r;
+#pragma unroll
+      for (int k = 0; k < NF; ++k) {
+        const double2 c = sC[d * NF + k];
+        acc[k].x = fma(r, c.x, acc[k].x);
+        acc[k].y = fma(r, c.y, acc[k].y);
+      }
+    };
+    int l = m + d0;
+    const int le = m + d0 + nd - 1;
+    if (((l - m) & 1) && l <= le) step(l++, accO);
+    for (; l + 1 <= le; l += 2) {
+      step(l, accE);
+      step(l + 1, accO);
+    }
+    if (l <= le) step(l, accE);
+  }
+  if (pair < npair) {
+#pragma unroll
+    for (int k = 0; k < NF; ++k) {
+      if (k >= a.nf) break;
+      float2* w = a.Wout + (((size_t)k * P.nm + im) * 2) * npair + pair;
+      w[0] = make_float2((float)accE[k].x, (float)accE[k].y);
+      w[npair] = make_float2((float)accO[k].x, (float)accO[k].y);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kSynThreads, 8) syn_group_kernel(const Args* __restrict__ targs,
                                                                 const int4* __restrict__ items, int nitems,
                                                                 int* __restrict__ queue) {
   extern __shared__ __align__(16) double smem[];
-  __shared__ Args sa;
-  __shared__ int4 s_it;
+  double* wsm = smem + (threadIdx.x >> 5) * kGroupWarpDoubles;
+  const int lane = threadIdx.x & 31;
   for (;;) {
-    if (threadIdx.x == 0) {
-      const int i = atomicAdd(queue, 1);
-      s_it = (i < nitems) ? items[i] : make_int4(-1, 0, 0, 0);
-      if (i < nitems) sa = targs[s_it.x];
-    }
-    __syncthreads();
-    const int4 it = s_it;
-    if (it.x < 0) break;
-    if (sa.nf == 1)
-      syn_body<1>(sa, it.y, it.z, smem);   // ends with a CTA barrier
+    int i = 0;
+    if (lane == 0) i = atomicAdd(queue, 1);
+    i = __shfl_sync(0xffffffffu, i, 0);
+    if (i >= nitems) break;
+    const int4 it = items[i];
+    const Args& a = targs[it.x];
+    if (a.nf == 1)
+      syn_warp_item<1>(a, it.y, it.z, wsm);
     else
-      syn_body<2>(sa, it.y, it.z, smem);
+      syn_warp_item<2>(a, it.y, it.z, wsm);
   }
 }
 
@@ -213,9 +295,9 @@ void simt_fill_args(const shtb_plan* p, const void* alm, void* W, int nf, void* 
   std::memcpy(host_args, &a, sizeof(a));
 }
 
-int simt_syn_pair_blocks(const shtb_plan* p) { return (p->npair + sx::kSynThreads - 1) / sx::kSynThreads; }
+int simt_syn_pair_blocks(const shtb_plan* p) { return (p->npair + 31) / 32; }   // per-warp items of the group kernel
 
-size_t simt_group_syn_smem(const shtb_plan* p) { return sx::syn_smem_bytes(p->lmax, 2); }
+size_t simt_group_syn_smem(const shtb_plan*) { return (sx::kSynThreads / 32) * sx::kGroupWarpDoubles * sizeof(double); }
 
 int launch_simt_group(const void* targs, const int4* items, int nitems, int grid, size_t smem, int* queue,
                       cudaStream_t st) {
