@@ -1,21 +1,23 @@
 // group.cu — uneven batches: many independent mixed-precision scalar transforms, each
-// with its own plan (lmax, Gauss grid, nlon) and 1..8 fields, run as four persistent
-// launches (B packing, order-GEMM synthesis, FFT synthesis, FFT analysis, order-GEMM
-// analysis).
+// with its own plan (lmax, Gauss grid, nlon) and 1..8 fields, run as persistent stage
+// launches: B packing and order-GEMM synthesis for members with three or more fields, the
+// FP64-pipe synthesis (simt.cu) for members with one or two, FFT synthesis, FFT analysis and
+// order-GEMM analysis.
 //
 // Every stage owns a list of work items over all members — GEMM tiles (member, order,
-// first latitude pair or degree, parity) and FFT tiles (member, first latitude pair,
-// field) — sorted by decreasing cost, and a device work counter (zeroed by a memset at
-// the start of every roundtrip). A stage launches min(items, SMs x CTAs per SM)
-// persistent CTAs; each claims the next item with an atomicAdd on the counter whenever
-// it has room for one, so the longest tiles start first and the short ones fill in
-// behind whichever CTA frees up first, and a batch of mixed sizes keeps every SM busy
-// without one launch per member. Members whose FFTs the packed-pair kernels take
-// (fft2_applicable) run them in a second persistent FFT kernel per direction, forked
-// beside the general one, so every member's results equal its single-plan calls bit for
-// bit. The memset and the six launches of a roundtrip (a start marker plus the five
-// stages; eight when both FFT kinds are present) are captured once into a CUDA graph and
-// replayed.
+// first latitude pair or degree, parity, with the tile's live-chunk mask: chunks whose P
+// image is all zero are skipped), FP64-pipe items (member, order, block of 32 latitude
+// pairs, one per warp) and FFT tiles (member, first latitude pair, field) — sorted by
+// decreasing cost, and a device work counter (zeroed by a memset at the start of every
+// roundtrip). A stage launches min(items, SMs x CTAs per SM) persistent CTAs; each claims
+// the next item with an atomicAdd on the counter whenever it has room for one, so the
+// longest tiles start first and the short ones fill in behind whichever CTA frees up first,
+// and a batch of mixed sizes keeps every SM busy without one launch per member. Members
+// whose FFTs the packed-pair kernels take (fft2_applicable) run them in a second persistent
+// FFT kernel per direction, forked beside the general one, and the FP64-pipe synthesis is
+// forked beside the packing and GEMM synthesis, so every member's results equal its
+// single-plan calls bit for bit. The memset and the launches of a roundtrip (a start marker
+// plus the stages) are captured once into a CUDA graph and replayed.
 //
 // Per-member latency: the start marker records %globaltimer; the analysis GEMM stores,
 // per member, the time its last tile finished.
