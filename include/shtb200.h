@@ -254,10 +254,11 @@ int shtb_synthesis_noalloc(const shtb_plan* plan, const void* alm, void* f, int 
  * Legendre stage) scalar transforms, each with its own plan (its own lmax, Gauss grid
  * and nlon) and 1..8 fields. No single counterpart in the reference, whose transforms
  * run one configuration per call (src/core_transforms.jl, src/batch_transforms.jl):
- * a group runs every member's tiles in one persistent launch per stage (B packing,
- * order-GEMM synthesis, FFT synthesis, FFT analysis, order-GEMM analysis), work items
- * sorted by cost and claimed by the CTAs from a device work counter, the stage launches
- * captured once in a CUDA graph and replayed.
+ * a group runs every member's tiles in one persistent launch per stage (B packing and
+ * order-GEMM synthesis for members of three or more fields, the FP64-pipe synthesis for
+ * one- or two-field members, FFT synthesis, FFT analysis, order-GEMM analysis), work items
+ * sorted by cost and claimed by the CTAs (or warps) from a device work counter, the stage
+ * launches captured once in a CUDA graph and replayed.
  * Members must use lcap = lmax and mres = 1. Buffers (device pointers, per member):
  * alm_in and alm_out are (lmax+1, mmax+1, nfields) complex FP32 (Julia column-major),
  * grid is (nlat, nlon, nfields) FP32. Results equal those of shtb_synthesis /
